@@ -1,0 +1,61 @@
+/*
+ * TensorBLAS.h — source-compatible replacement of the reference library's
+ * public header (Orgline/Tensor-BLAS include/TensorBLAS.h:135-171) for the
+ * B200 (sm_100a) implementation in libTensorBLAS.so.
+ *
+ * Same routine names, parameter lists and semantics as the reference:
+ * column-major FP32 (or FP64 for tc_ozimmu_*) device pointers, the FP16
+ * workspace argument of the plain routines, void return. Differences that a
+ * caller can observe are listed per routine. Status-returning C entry points
+ * with explicit flags and precision live in tb_capi.h.
+ *
+ * Handles: the cuBLAS and cuMpSGEMM handles are accepted only for source
+ * compatibility; nothing here calls cuBLAS or cuMpSGEMM. Work is queued on
+ * the stream set with tb_set_stream (default: the legacy default stream,
+ * which is also where the reference's handles run unless told otherwise).
+ *
+ * Workspace: the plain routines take the reference's FP16 workspace. When
+ * it is too small for this implementation's layout (row-padded FP16 copies)
+ * or NULL, a library-owned scratch buffer is used instead (grow-only, one per
+ * device; calls that overlap on different streams must pass their own).
+ */
+#ifndef TENSORBLAS_B200_H_
+#define TENSORBLAS_B200_H_
+
+#include <cuda_fp16.h>
+
+#include "tb_capi.h"
+
+/* Opaque handle types with the reference's spelling. */
+#ifndef CUBLAS_V2_H_
+struct cublasContext;
+typedef struct cublasContext* cublasHandle_t;
+#endif
+#ifndef TB_HAVE_CUMPSGEMM
+namespace cumpsgemm {
+struct handle;
+typedef handle* handle_t;
+}  // namespace cumpsgemm
+#endif
+
+/* include/TensorBLAS.h:139 — lower triangle of C = alpha A A^T + beta C,
+ * A n x k (lda). Ah: FP16 workspace of n*k halves. Unlike the reference the
+ * strict upper triangle of C is not written, odd n/k need no padding copies,
+ * and beta is honoured for every size (reference: BLAS/tc_syrk.cu:140). */
+TB_API void tc_syrk(cublasHandle_t handle, long int n, long int k, float alpha, float* A, long int lda, float beta,
+                    float* C, long int ldc, __half* Ah, long int nb);
+
+/* include/TensorBLAS.h:141 — FP32-accurate SYRK (split FP16 products). */
+TB_API void tc_cumpsgemm_syrk(cumpsgemm::handle_t cumpsgemm_handle, long int n, long int k, float alpha, float* A,
+                              long int lda, float beta, float* C, long int ldc, long int nb);
+
+/* include/TensorBLAS.h:147 — X A^T = B (right, lower, transpose, non-unit),
+ * B (m x n, ldb) overwritten; hwork: FP16 workspace. */
+TB_API void tc_trsm(cublasHandle_t handle, long int m, long int n, float* A, long int lda, float* B, long int ldb,
+                    __half* hwork, long int nb);
+
+/* include/TensorBLAS.h:149 — FP32-accurate TRSM (split FP16 products). */
+TB_API void tc_cumpsgemm_trsm(cublasHandle_t handle, cumpsgemm::handle_t cumpsgemm_handle, long int m, long int n,
+                              float* A, long int lda, float* B, long int ldb, long int nb);
+
+#endif /* TENSORBLAS_B200_H_ */

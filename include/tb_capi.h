@@ -1,0 +1,95 @@
+/*
+ * tb_capi.h — plain C ABI of the B200 TensorBLAS library (libTensorBLAS.so).
+ *
+ * Every entry point takes raw device pointers to column-major matrices and
+ * plain integers, returns a tb_status, and runs asynchronously on the stream
+ * set with tb_set_stream (default: the legacy default stream). No torch or
+ * cuBLAS types appear here; ctypes, cgo or any FFI can bind it directly.
+ *
+ * Each function names the reference interface it replaces
+ * (Orgline/Tensor-BLAS, paths relative to that project).
+ */
+#ifndef TB_CAPI_H_
+#define TB_CAPI_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TB_API __attribute__((visibility("default")))
+
+typedef enum {
+  TB_SUCCESS = 0,
+  TB_ERROR_INVALID_VALUE = 1, /* bad size, stride, flag or pointer */
+  TB_ERROR_ALLOC = 2,         /* device scratch could not be allocated */
+  TB_ERROR_CUDA = 3,          /* a CUDA runtime/driver call failed */
+  TB_ERROR_TIMEOUT = 4,       /* a bounded device-side wait gave up */
+  TB_ERROR_NOT_SUPPORTED = 5  /* no sm_100 device / unsupported option */
+} tb_status;
+
+typedef enum {
+  /* FP16 operands, FP32 accumulation: the reference's plain tc_* form. */
+  TB_PREC_PLAIN = 0,
+  /* FP16 hi + scaled-lo split of both operands, 3 tensor-core products with
+   * the correction in a separate FP32 accumulator: FP32-level accuracy (the
+   * role of the reference's tc_cumpsgemm_* / CUMPSGEMM_FP16TCEC). */
+  TB_PREC_SPLIT = 1
+} tb_precision;
+
+/* Library/stream control. `stream` is a cudaStream_t (NULL = default). */
+TB_API tb_status tb_set_stream(void* stream);
+TB_API void* tb_get_stream(void);
+TB_API const char* tb_status_string(tb_status s);
+/* Text of the last error recorded on the calling thread ("" if none). */
+TB_API const char* tb_last_error(void);
+/* Blocks until queued work finishes; returns TB_ERROR_TIMEOUT if a kernel
+ * reported a bounded-wait timeout, TB_ERROR_CUDA on a CUDA error. */
+TB_API tb_status tb_synchronize(void);
+TB_API int tb_version(void);
+
+/*
+ * GEMM: C = alpha * op(A) * op(B) + beta * C, op(A) m x k, op(B) k x n, all
+ * FP32 in memory, products on the tensor cores at `precision`.
+ * Replaces the cublasGemmEx(CUDA_R_16F in, CUDA_R_32F out) calls the
+ * reference builds every routine from (e.g. BLAS/tc_syrk.cu:106-118) and the
+ * FP16 GEMM of testing/testing_gemm.cu:62-130.
+ */
+TB_API tb_status tb_sgemm(char transa, char transb, long m, long n, long k, float alpha, const float* A, long lda,
+                          const float* B, long ldb, float beta, float* C, long ldc, int precision);
+
+/*
+ * SYRK: C = alpha * op(A) * op(A)^T + beta * C, lower triangle of C written
+ * (diagonal included); the strict upper triangle is left untouched.
+ *   trans 'N': A is n x k (lda >= n).   trans 'T': A is k x n (lda >= k).
+ * Replaces tc_syrk (BLAS/tc_syrk.cu:126-157, include/TensorBLAS.h:139) and,
+ * with TB_PREC_SPLIT, tc_cumpsgemm_syrk (BLAS/tc_cumpsgemm_syrk.cu:3-125).
+ * nb is the recursion block of the reference method (> 0).
+ */
+TB_API tb_status tb_ssyrk(char uplo, char trans, long n, long k, float alpha, const float* A, long lda, float beta,
+                          float* C, long ldc, long nb, int precision);
+
+/*
+ * TRSM with a lower-triangular, non-unit A, B overwritten by X:
+ *   side 'R': X * A^T = B,  A n x n, B m x n  (the reference's tc_trsm:
+ *             BLAS/tc_trsm.cu:139-174, right/lower/transpose/non-unit)
+ *   side 'L': A * X = B,    A m x m, B m x n  (left/lower/no-trans)
+ * Replaces tc_trsm (include/TensorBLAS.h:147) and, with TB_PREC_SPLIT,
+ * tc_cumpsgemm_trsm (BLAS/tc_cumpsgemm_trsm.cu:3-126).
+ */
+TB_API tb_status tb_strsm(char side, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
+                          int precision);
+
+/* Mirror lower -> upper of an n x n matrix (util/util.cu:148-157). */
+TB_API tb_status tb_ssymmetrize(long n, float* A, long lda);
+
+/* Reference C-ABI wrappers (include/TensorBLAS.h:135,137,145), same
+ * argument meaning and return convention (0 ok, 1 error). */
+TB_API int tc_syrk_wrapper(long n, long k, float* A, float* C, long nb);
+TB_API int tc_trsm_wrapper(long m, long n, float* A, float* B, long nb);
+TB_API void print_env(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TB_CAPI_H_ */

@@ -1,0 +1,203 @@
+// Host-buffer entry points around the REFERENCE library's own routines
+// (compiled from its sources by oracle/Makefile). Test infrastructure: used by
+// tests/golden/make_golden.py to record the reference's outputs, and by
+// bench.py's reference arm to time the reference on the same B200.
+// Column-major host arrays; every call uploads, runs the reference routine on
+// its default stream through its C++ API, and downloads.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "TensorBLAS.h"  // the reference's include/TensorBLAS.h
+
+namespace {
+cublasHandle_t handle() {
+  static cublasHandle_t h = nullptr;
+  if (!h) cublasCreate(&h);
+  return h;
+}
+template <class T>
+T* up(const T* h, size_t n) {
+  T* d = nullptr;
+  if (cudaMalloc(&d, n * sizeof(T)) != cudaSuccess) return nullptr;
+  if (h) cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice);
+  return d;
+}
+template <class T>
+int down(T* h, const T* d, size_t n) {
+  return cudaMemcpy(h, d, n * sizeof(T), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : 1;
+}
+int finish() {
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : 2;
+}
+struct Events {
+  cudaEvent_t a, b;
+  Events() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+  }
+  ~Events() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+double median(std::vector<float>& v) {
+  std::sort(v.begin(), v.end());
+  return v.empty() ? -1.0 : v[v.size() / 2];
+}
+}  // namespace
+
+extern "C" {
+
+// C(lower) = alpha A A^T + beta C ; A n x k (lda = n), C n x n (ldc = n).
+int ref_syrk(long n, long k, float alpha, const float* hA, float beta, float* hC, long nb) {
+  float* A = up(hA, (size_t)n * k);
+  float* C = up(hC, (size_t)n * n);
+  __half* w = nullptr;
+  cudaMalloc(&w, sizeof(__half) * 2 * n * k);
+  tc_syrk(handle(), n, k, alpha, A, n, beta, C, n, w, nb);
+  int rc = finish();
+  if (!rc) rc = down(hC, C, (size_t)n * n);
+  cudaFree(A);
+  cudaFree(C);
+  cudaFree(w);
+  return rc;
+}
+
+// X A^T = B (right/lower/T/non-unit), A n x n (lda = n), B m x n (ldb = m), B <- X.
+int ref_trsm(long m, long n, const float* hA, float* hB, long nb) {
+  float* A = up(hA, (size_t)n * n);
+  float* B = up(hB, (size_t)m * n);
+  __half* w = nullptr;
+  cudaMalloc(&w, sizeof(__half) * ((size_t)n / 2 * n / 2 + (size_t)m / 2 * n + 16));
+  tc_trsm(handle(), m, n, A, n, B, m, w, nb);
+  int rc = finish();
+  if (!rc) rc = down(hB, B, (size_t)m * n);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(w);
+  return rc;
+}
+
+// C = alpha A B, A m x m lower (strict upper must be zero), B, C m x n.
+int ref_trmm(long m, long n, float alpha, const float* hA, const float* hB, float* hC, long nb) {
+  float* A = up(hA, (size_t)m * m);
+  float* B = up(hB, (size_t)m * n);
+  float* C = up(hC, (size_t)m * n);
+  __half* w = nullptr;
+  cudaMalloc(&w, sizeof(__half) * ((size_t)m * n + (size_t)m * m));
+  tc_trmm(handle(), m, n, alpha, A, m, B, m, C, m, w, nb);
+  int rc = finish();
+  if (!rc) rc = down(hC, C, (size_t)m * n);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(C);
+  cudaFree(w);
+  return rc;
+}
+
+// C(lower) = alpha (A B^T + B A^T) + beta C ; A, B n x k, C n x n.
+int ref_syr2k(long n, long k, float alpha, const float* hA, const float* hB, float beta, float* hC, long nb) {
+  float* A = up(hA, (size_t)n * k);
+  float* B = up(hB, (size_t)n * k);
+  float* C = up(hC, (size_t)n * n);
+  __half* w = nullptr;
+  cudaMalloc(&w, sizeof(__half) * 2 * n * k);
+  tc_syr2k(handle(), n, k, alpha, A, n, B, n, beta, C, n, w, nb);
+  int rc = finish();
+  if (!rc) rc = down(hC, C, (size_t)n * n);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(C);
+  cudaFree(w);
+  return rc;
+}
+
+// C = alpha A B + beta C, A m x m symmetric (lower stored), B, C m x n (m == n
+// only: the reference's grids assume it, BLAS/tc_symm.cu:5-14).
+int ref_symm(long m, long n, float alpha, const float* hA, const float* hB, float beta, float* hC) {
+  float* A = up(hA, (size_t)m * m);
+  float* B = up(hB, (size_t)m * n);
+  float* C = up(hC, (size_t)m * n);
+  __half* w = nullptr;
+  cudaMalloc(&w, sizeof(__half) * ((size_t)m * m + (size_t)m * n));
+  tc_symm(handle(), m, n, alpha, A, m, B, (int)m, beta, C, m, w);
+  int rc = finish();
+  if (!rc) rc = down(hC, C, (size_t)m * n);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(C);
+  cudaFree(w);
+  return rc;
+}
+
+// FP64 SYRK through the reference's "ozimmu" driver (native FP64 cuBLAS).
+int ref_ozimmu_syrk(long n, long k, double alpha, const double* hA, double beta, double* hC, long nb) {
+  double* A = up(hA, (size_t)n * k);
+  double* C = up(hC, (size_t)n * n);
+  tc_ozimmu_syrk(handle(), n, k, alpha, A, n, beta, C, n, nb);
+  int rc = finish();
+  if (!rc) rc = down(hC, C, (size_t)n * n);
+  cudaFree(A);
+  cudaFree(C);
+  return rc;
+}
+
+// Median device time (ms) of tc_syrk(n, k, nb) on device-resident inputs.
+double ref_time_syrk(long n, long k, long nb, const float* hA, int warmup, int iters) {
+  float* A = up(hA, (size_t)n * k);
+  float* C = up<float>(nullptr, (size_t)n * n);
+  __half* w = nullptr;
+  cudaMalloc(&w, sizeof(__half) * 2 * n * k);
+  if (!A || !C || !w) return -1.0;
+  Events ev;
+  std::vector<float> t;
+  for (int i = 0; i < warmup + iters; ++i) {
+    cudaEventRecord(ev.a);
+    tc_syrk(handle(), n, k, 1.0f, A, n, 0.0f, C, n, w, nb);
+    cudaEventRecord(ev.b);
+    cudaEventSynchronize(ev.b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev.a, ev.b);
+    if (i >= warmup) t.push_back(ms);
+  }
+  int rc = finish();
+  cudaFree(A);
+  cudaFree(C);
+  cudaFree(w);
+  return rc ? -1.0 : median(t);
+}
+
+// Median device time (ms) of tc_trsm(m, n, nb); B restored before each call
+// (outside the timed region).
+double ref_time_trsm(long m, long n, long nb, const float* hA, const float* hB, int warmup, int iters) {
+  float* A = up(hA, (size_t)n * n);
+  float* B0 = up(hB, (size_t)m * n);
+  float* B = up<float>(nullptr, (size_t)m * n);
+  __half* w = nullptr;
+  cudaMalloc(&w, sizeof(__half) * ((size_t)n / 2 * n / 2 + (size_t)m / 2 * n + 16));
+  if (!A || !B0 || !B || !w) return -1.0;
+  Events ev;
+  std::vector<float> t;
+  for (int i = 0; i < warmup + iters; ++i) {
+    cudaMemcpy(B, B0, sizeof(float) * m * n, cudaMemcpyDeviceToDevice);
+    cudaEventRecord(ev.a);
+    tc_trsm(handle(), m, n, A, n, B, m, w, nb);
+    cudaEventRecord(ev.b);
+    cudaEventSynchronize(ev.b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev.a, ev.b);
+    if (i >= warmup) t.push_back(ms);
+  }
+  int rc = finish();
+  cudaFree(A);
+  cudaFree(B0);
+  cudaFree(B);
+  cudaFree(w);
+  return rc ? -1.0 : median(t);
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+"""CPU oracle for the TensorBLAS hot path — TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg (and the
+reference arm of bench.py) may import this module, and only as the checker or
+the timed CPU baseline; the library never calls it.
+
+It restates, in NumPy, the arithmetic model of the reference's tc_* routines
+(Orgline/Tensor-BLAS; paths relative to that project):
+
+* FP32 -> FP16 conversion is round-to-nearest-even (``__float2half`` in
+  ``s2h``/``s2h_swpipe``, util/util.cu:127-135, include/TensorBLAS.h:223).
+* SYRK (BLAS/tc_syrk.cu:41-157): every product of the recursion is
+  FP16 x FP16 with FP32 accumulation over the whole K, so in exact arithmetic
+  the plain result is  alpha * h(A) h(A)^T + beta * C  on the lower triangle,
+  whatever the chunking.  ``syrk_model`` computes that in FP64.
+* TRSM (BLAS/tc_trsm.cu:31-137): solves X A^T = B.  Leaves (n <= nb) are FP32
+  ``cublasStrsm``; each internal node converts A21 and B1(=X1) to FP16 and
+  applies B2 -= h(X1) h(A21)^T.  In exact arithmetic, with leaf blocks of nb
+  columns, X_b = (B_b - sum_{c<b} h(X_c) h(A_bc)^T) A_bb^{-T}.
+  ``trsm_right_model`` computes that in FP64.
+* The chunk planners find_mat_size_syrk / find_mat_size_trsm
+  (util/mat_size.cu:5-55) are restated exactly in ``find_mat_size``.
+* The split (error-corrected) form, the role of tc_cumpsgemm_*: operands
+  split as hi = h(x), lo = h((x - hi) * 2^11) (Ootomo & Yokota, IJHPCA 2022);
+  product = hi*hi + (hi*lo + lo*hi) / 2^11.  ``split_product`` models it.
+
+Parity pin: tests/golden/ holds outputs of the reference library itself
+(oracle/_ref/libTensorBLAS_ref.so, built from the reference sources by
+oracle/Makefile and run on a B200 by tests/golden/make_golden.py); the tests
+check this restatement against those vectors.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+LO_SCALE = 2048.0  # 2^11
+
+
+def h(x: np.ndarray) -> np.ndarray:
+    """FP32 -> FP16 round-to-nearest-even, returned as FP64 values."""
+    return np.asarray(x, dtype=np.float32).astype(np.float16).astype(np.float64)
+
+
+def split_hilo(x: np.ndarray):
+    """hi = h(x); lo = h((x - hi) * 2^11), both as FP64 values (lo unscaled)."""
+    x32 = np.asarray(x, dtype=np.float32)
+    hi16 = x32.astype(np.float16)
+    lo16 = ((x32 - hi16.astype(np.float32)) * np.float32(LO_SCALE)).astype(np.float16)
+    return hi16.astype(np.float64), lo16.astype(np.float64)
+
+
+def split_product(a: np.ndarray, b_t: np.ndarray) -> np.ndarray:
+    """Model of the 3-product split GEMM a @ b_t in FP64 arithmetic."""
+    ah, al = split_hilo(a)
+    bh, bl = split_hilo(b_t)
+    return ah @ bh + (ah @ bl + al @ bh) / LO_SCALE
+
+
+def find_mat_size(n: int, kind: str) -> list[int]:
+    """util/mat_size.cu:5-55 — greedy chunk list (the -1 terminator dropped).
+
+    kind "syrk": powers {8192, 16384 x11}, remainder threshold 8192.
+    kind "trsm": powers {2048, 4096, 8192, 16384 x8}, threshold 2048.
+    """
+    if kind == "syrk":
+        powers = [8192] + [16384] * 11
+        thresh = 8192
+    elif kind == "trsm":
+        powers = [2048, 4096, 8192] + [16384] * 9
+        thresh = 2048
+    else:
+        raise ValueError(kind)
+    out: list[int] = []
+    i = len(powers) - 1
+    while i >= -1:
+        if n < thresh:
+            if n != 0:
+                out.append(n)
+            break
+        if i < 0:  # the C loop would index powers[-1] here (n > ~188k)
+            raise ValueError("n too large for the reference planner")
+        if n >= powers[i]:
+            out.append(powers[i])
+            n -= powers[i]
+        i -= 1
+    return out
+
+
+def syrk_model(A: np.ndarray, alpha: float = 1.0, beta: float = 0.0, C: np.ndarray | None = None,
+               trans: bool = False, split: bool = False) -> np.ndarray:
+    """Lower triangle (incl. diagonal) of alpha*op(A)op(A)^T + beta*C in FP64.
+
+    A is given as the n x k matrix op(A) (FP32 values).  Upper triangle of the
+    result is copied from C (untouched by the routine) or zero.
+    """
+    A = np.asarray(A, dtype=np.float32)
+    if trans:
+        A = A.T
+    if split:
+        prod = split_product(A, A.T)
+    else:
+        Ah = h(A)
+        prod = Ah @ Ah.T
+    n = A.shape[0]
+    res = alpha * prod
+    if C is not None and beta != 0.0:
+        res = res + beta * np.asarray(C, dtype=np.float64)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    base = np.zeros((n, n)) if C is None else np.asarray(C, dtype=np.float64)
+    return np.where(low, res, base)
+
+
+def trsm_right_model(A: np.ndarray, B: np.ndarray, nb: int, split: bool = False) -> np.ndarray:
+    """X with X A^T = B (A lower n x n), leaf blocks of nb columns, FP64.
+
+    Off-diagonal block products use FP16-rounded operands (plain) or the
+    split model; diagonal blocks are solved exactly (the FP32 leaf).
+    """
+    A = np.asarray(A, dtype=np.float64)
+    B = np.asarray(B, dtype=np.float64)
+    m, n = B.shape
+    X = np.zeros_like(B)
+    blocks = [(s, min(s + nb, n)) for s in range(0, n, nb)]
+    for bi, (s, e) in enumerate(blocks):
+        R = B[:, s:e].copy()
+        for (cs, ce) in blocks[:bi]:
+            if split:
+                R -= split_product(X[:, cs:ce].astype(np.float32), A[s:e, cs:ce].T.astype(np.float32))
+            else:
+                R -= h(X[:, cs:ce]) @ h(A[s:e, cs:ce]).T
+        # R = X_b A_bb^T  ->  X_b^T = A_bb^{-1} R^T
+        X[:, s:e] = np.linalg.solve(A[s:e, s:e], R.T).T
+    return X
+
+
+def trsm_left_model(A: np.ndarray, B: np.ndarray, nb: int, split: bool = False) -> np.ndarray:
+    """X with A X = B (A lower m x m): the transpose of the right-side form."""
+    return trsm_right_model(A, np.asarray(B).T, nb, split).T
+
+
+def rel_errors(x: np.ndarray, ref: np.ndarray, mask: np.ndarray | None = None):
+    """(max elementwise relative, normwise relative) error of x vs ref."""
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    if mask is not None:
+        x = x[mask]
+        ref = ref[mask]
+    d = np.abs(x - ref)
+    scale = np.maximum(np.abs(ref), np.finfo(np.float64).tiny)
+    nrm = np.linalg.norm(ref)
+    return float(np.max(d / scale)) if d.size else 0.0, float(np.linalg.norm(d) / nrm) if nrm > 0 else 0.0

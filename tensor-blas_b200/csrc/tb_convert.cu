@@ -1,0 +1,108 @@
+// FP32 -> FP16 conversion kernels (the reference's s2h / s2h_swpipe /
+// s2hTranspose family, include/TensorBLAS.h:185-283 and util/util.cu:127-145),
+// re-done for HBM3e: 8 elements per thread, two 128-bit loads and one (hi) or
+// two (hi+lo) 128-bit stores, 64-bit indexing, grid sized in SM multiples.
+// Round-to-nearest-even as __float2half in the reference.
+//
+// The split form writes hi = fp16(x) and lo = fp16((x - hi) * lo_scale), the
+// error-corrected FP16 pair of Ootomo & Yokota (IJHPCA 2022).
+#include "tb_internal.h"
+
+namespace tb {
+
+namespace {
+
+__device__ __forceinline__ float4 ld_stream(const float* p) {
+  float4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ uint32_t pack2(__half a, __half b) {
+  return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+}
+
+// Vector path: rows % 8 == 0, lds % 4 == 0, ldd % 8 == 0, 16-byte aligned bases.
+__global__ void __launch_bounds__(256) convert8_kernel(long long rows, long long cols, const float* __restrict__ src,
+                                                       long long lds, __half* __restrict__ hi, __half* __restrict__ lo,
+                                                       long long ldd, float lo_scale, int tri) {
+  const long long rows8 = rows >> 3;
+  for (long long j = blockIdx.y; j < cols; j += gridDim.y) {
+    long long v0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tri == 2) v0 += (j >> 3);  // rows i >= j (rounded down to 8)
+    for (long long v = v0; v < rows8; v += (long long)gridDim.x * blockDim.x) {
+      const long long i = v << 3;
+      const float* s = src + i + j * lds;
+      const float4 a = ld_stream(s), b = ld_stream(s + 4);
+      float f[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      if (tri == 1) {
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+          if (i + e < j) f[e] = 0.f;
+      }
+      __half h[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) h[e] = __float2half_rn(f[e]);
+      uint4 o;
+      o.x = pack2(h[0], h[1]);
+      o.y = pack2(h[2], h[3]);
+      o.z = pack2(h[4], h[5]);
+      o.w = pack2(h[6], h[7]);
+      *reinterpret_cast<uint4*>(hi + i + j * ldd) = o;
+      if (lo) {
+        __half l[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) l[e] = __float2half_rn((f[e] - __half2float(h[e])) * lo_scale);
+        uint4 q;
+        q.x = pack2(l[0], l[1]);
+        q.y = pack2(l[2], l[3]);
+        q.z = pack2(l[4], l[5]);
+        q.w = pack2(l[6], l[7]);
+        *reinterpret_cast<uint4*>(lo + i + j * ldd) = q;
+      }
+    }
+  }
+}
+
+// Scalar fallback for ragged or unaligned shapes.
+__global__ void __launch_bounds__(256) convert1_kernel(long long rows, long long cols, const float* __restrict__ src,
+                                                       long long lds, __half* __restrict__ hi, __half* __restrict__ lo,
+                                                       long long ldd, float lo_scale, int tri) {
+  for (long long j = blockIdx.y; j < cols; j += gridDim.y) {
+    long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tri == 2) i0 += (j >> 3) << 3;
+    for (long long i = i0; i < rows; i += (long long)gridDim.x * blockDim.x) {
+      float f = src[i + j * lds];
+      if (tri == 1 && i < j) f = 0.f;
+      const __half h = __float2half_rn(f);
+      hi[i + j * ldd] = h;
+      if (lo) lo[i + j * ldd] = __float2half_rn((f - __half2float(h)) * lo_scale);
+    }
+  }
+}
+
+}  // namespace
+
+tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
+                          long long ldd, float lo_scale, int tri, cudaStream_t stream) {
+  if (rows <= 0 || cols <= 0) return TB_SUCCESS;
+  const bool vec = (rows % 8 == 0) && (lds % 4 == 0) && (ldd % 8 == 0) &&
+                   (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(hi) % 16 == 0) &&
+                   (lo == nullptr || reinterpret_cast<uintptr_t>(lo) % 16 == 0);
+  const int threads = 256;
+  const long long units = vec ? rows / 8 : rows;
+  long long gx = (units + threads - 1) / threads;
+  if (gx > 1024) gx = 1024;
+  long long gy = cols < 65535 ? cols : 65535;
+  dim3 grid((unsigned)gx, (unsigned)gy);
+  if (vec)
+    convert8_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri);
+  else
+    convert1_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri);
+  TB_CUDA_TRY(cudaGetLastError());
+  return TB_SUCCESS;
+}
+
+}  // namespace tb

@@ -1,0 +1,194 @@
+// Host side of the tcgen05 GEMM engine: tensor-map encoding, tile planning,
+// variant dispatch and launch.
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "tb_gemm.cuh"
+#include "tb_internal.h"
+
+namespace tb {
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// Tensor map for an fp16 operand; box_rows rows per load (K-major) or 64
+// (MN-major), 64 elements along the contiguous dimension, 128B swizzle.
+tb_status make_map(CUtensorMap* map, const Operand& op, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_last_error("cuTensorMapEncodeTiled unavailable");
+    return TB_ERROR_CUDA;
+  }
+  if ((reinterpret_cast<uintptr_t>(op.ptr) & 15) != 0 || (op.ld * 2) % 16 != 0) {
+    set_last_error("operand base must be 16-byte aligned and ld a multiple of 8 (ptr=%p ld=%lld)", op.ptr, op.ld);
+    return TB_ERROR_INVALID_VALUE;
+  }
+  cuuint64_t dims[2];
+  cuuint64_t strides[1] = {(cuuint64_t)op.ld * 2};
+  cuuint32_t box[2];
+  cuuint32_t estr[2] = {1, 1};
+  if (op.mn_major) {
+    dims[0] = (cuuint64_t)op.rows;
+    dims[1] = (cuuint64_t)op.cols;
+    box[0] = 64;
+    box[1] = 64;
+  } else {
+    dims[0] = (cuuint64_t)op.cols;
+    dims[1] = (cuuint64_t)op.rows;
+    box[0] = 64;
+    box[1] = (cuuint32_t)box_rows;
+  }
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(op.ptr), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled failed (%d) rows=%lld cols=%lld ld=%lld", (int)r, op.rows, op.cols, op.ld);
+    return TB_ERROR_CUDA;
+  }
+  return TB_SUCCESS;
+}
+
+template <class Cfg>
+tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream) {
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    TB_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES));
+    attr_set[dev] = true;
+  }
+  int grid = num_tiles < sm_count() ? num_tiles : sm_count();
+  gemm_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(args);
+  TB_CUDA_TRY(cudaGetLastError());
+  return TB_SUCCESS;
+}
+
+}  // namespace
+
+int gemm_bn(Split s) { return s == Split::kPlain ? 256 : 128; }
+
+tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
+  if (c.num_tiles <= 0) return TB_SUCCESS;
+  const bool split = c.split == Split::kHiLo;
+  const int bn = gemm_bn(c.split);
+  GemmArgs a;
+  memset(&a, 0, sizeof(a));
+  TB_TRY(make_map(&a.mapA[0], c.a_hi, kGemmBM));
+  TB_TRY(make_map(&a.mapB[0], c.b_hi, bn));
+  if (split) {
+    TB_TRY(make_map(&a.mapA[1], c.a_lo, kGemmBM));
+    TB_TRY(make_map(&a.mapB[1], c.b_lo, bn));
+  }
+  a.tiles = c.tiles;
+  a.num_tiles = c.num_tiles;
+  a.a_off = c.a_off;
+  a.b_off = c.b_off;
+  a.k_off = c.k_off;
+  a.M = c.M;
+  a.N = c.N;
+  a.C = c.C;
+  a.ldc = c.ldc;
+  a.alpha = c.alpha;
+  a.beta = c.beta;
+  a.tri = c.tri;
+  a.diag = c.diag;
+  a.corr_scale = c.corr_scale;
+  a.kchunk = c.kchunk > 0 ? c.kchunk : 1;
+  a.out_hi = c.out_hi;
+  a.out_lo = c.out_lo;
+  a.ld_out = c.ld_out;
+  a.out_lo_scale = c.out_lo_scale;
+  a.err = device_error_word();
+  // TMA coordinates along the contiguous dimension must be 16-byte aligned.
+  if (c.a_hi.mn_major && (c.a_off % 8) != 0) return TB_ERROR_INVALID_VALUE;
+  if (c.b_hi.mn_major && (c.b_off % 8) != 0) return TB_ERROR_INVALID_VALUE;
+  if ((!c.a_hi.mn_major || !c.b_hi.mn_major) && (c.k_off % 8) != 0) return TB_ERROR_INVALID_VALUE;
+
+  const bool amn = c.a_hi.mn_major, bmn = c.b_hi.mn_major;
+  if (!split) {
+    if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>>(a, c.num_tiles, stream);
+    if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>>(a, c.num_tiles, stream);
+    if (!amn && !bmn) return launch_variant<GemmCfg<256, 1, false, false>>(a, c.num_tiles, stream);
+    return launch_variant<GemmCfg<256, 1, false, true>>(a, c.num_tiles, stream);
+  } else {
+    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true>>(a, c.num_tiles, stream);
+    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false>>(a, c.num_tiles, stream);
+    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>>(a, c.num_tiles, stream);
+    return launch_variant<GemmCfg<128, 3, false, true>>(a, c.num_tiles, stream);
+  }
+}
+
+// --------------------------------------------------------------------- plans
+// Tiles are emitted in column-panel groups of kGroup tiles: within a group the
+// walk goes down the rows, so the ~148 tiles resident at once share a few A
+// row panels and kGroup B panels in L2.
+static constexpr int kGroup = 8;
+
+std::vector<int4> plan_rect(int M, int N, int bn, int kb0, int kb1) {
+  std::vector<int4> t;
+  const int mt = (M + kGemmBM - 1) / kGemmBM, nt = (N + bn - 1) / bn;
+  t.reserve((size_t)mt * nt);
+  for (int g = 0; g < nt; g += kGroup) {
+    const int ge = g + kGroup < nt ? g + kGroup : nt;
+    for (int i = 0; i < mt; ++i)
+      for (int j = g; j < ge; ++j) t.push_back(make_int4(i * kGemmBM, j * bn, kb0, kb1));
+  }
+  return t;
+}
+
+std::vector<int4> plan_lower(int n, int bn, int kb0, int kb1) {
+  std::vector<int4> t;
+  const int mt = (n + kGemmBM - 1) / kGemmBM, nt = (n + bn - 1) / bn;
+  for (int g = 0; g < nt; g += kGroup) {
+    const int ge = g + kGroup < nt ? g + kGroup : nt;
+    for (int i = 0; i < mt; ++i)
+      for (int j = g; j < ge; ++j) {
+        const int m0 = i * kGemmBM, n0 = j * bn;
+        if (m0 + kGemmBM - 1 >= n0) t.push_back(make_int4(m0, n0, kb0, kb1));
+      }
+  }
+  return t;
+}
+
+// Device copies of tile plans, cached by content (per device). Plans are
+// small (16 B per tile) and reused across calls of the same shape.
+const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream) {
+  static std::mutex mu;
+  static std::map<std::pair<int, std::string>, int4*> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::string key(reinterpret_cast<const char*>(tiles.data()), tiles.size() * sizeof(int4));
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find({dev, key});
+  if (it != cache.end()) return it->second;
+  int4* d = nullptr;
+  if (cudaMalloc(&d, tiles.size() * sizeof(int4)) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  (void)stream;
+  cache[{dev, key}] = d;
+  return d;
+}
+
+}  // namespace tb

@@ -1,0 +1,352 @@
+// Persistent warp-specialised tcgen05 GEMM engine (sm_100a).
+//
+//   C[m0+i, n0+j] = alpha * sum_k A(m0+i, k) * B(n0+j, k) + beta * C[...]
+//
+// over a host-built list of 128 x BN output tiles, each with its own K-block
+// range. This single kernel serves every contraction of the library: the
+// flattened recursion levels of SYRK/SYR2K (lower-triangle tile lists), the
+// off-diagonal updates and leaf products of TRSM, and TRMM/SYMM.
+//
+// Roles (192 threads, one CTA per SM):
+//   warp 0      TMA producer: 64-wide K slabs of A and B into a smem ring.
+//   warp 1      TMEM allocator + single-thread UMMA issuer.
+//   warps 2..5  epilogue: TMEM -> registers -> alpha/beta -> global fp32,
+//               optionally fused fp16 hi/lo copies of the result.
+// The fp32 accumulator is double-buffered in TMEM (2 x 256 columns) so the
+// epilogue of tile t overlaps the MMAs of tile t+1.
+//
+// Operands are fp16 (or bf16) in global memory, either MN-major (column-major
+// storage with the M/N index contiguous, the layout the reference's FP32->FP16
+// conversion produces) or K-major. Both map onto 128B-swizzled UMMA canonical
+// layouts:
+//   MN-major: TMA box {64 (MN), 64 (K)} -> 8 KB atoms; LBO = 8 KB between
+//             64-wide MN atoms, SBO = 1 KB between 8-row K groups; a K step of
+//             16 advances the descriptor by 2 KB.
+//   K-major : TMA box {64 (K), R rows} -> R x 128 B; SBO = 1 KB between
+//             8-row groups; a K step of 16 advances the descriptor by 32 B.
+//
+// Split ("3-product") mode holds hi and lo copies of both operands and runs
+//   acc0 += Ahi*Bhi ; acc1 += Ahi*Blo + Alo*Bhi
+// with the correction in its own TMEM accumulator (Ootomo & Yokota 2022,
+// the error-corrected FP16 scheme cuMpSGEMM's FP16TCEC mode uses);
+// epilogue: acc0 + corr_scale * acc1.
+#pragma once
+#include "tb_ptx.cuh"
+
+namespace tb {
+
+struct GemmArgs {
+  CUtensorMap mapA[2];  // [0] hi, [1] lo (split mode only)
+  CUtensorMap mapB[2];
+  const int4* tiles;  // {m0, n0, kb_begin, kb_end}; m0/n0 relative to C
+  int num_tiles;
+  int a_off;  // row offset of the A operand in mapA's row coordinate
+  int b_off;  // row offset of the B operand in mapB's row coordinate
+  int k_off;  // K offset (elements) applied to both operands
+  int M, N;   // extent of C (predication)
+  float* C;
+  long long ldc;
+  float alpha, beta;
+  int tri;   // 1: write only (i - j) >= diag (lower triangle)
+  int diag;
+  float corr_scale;  // weight of the correction accumulator
+  int kchunk;        // split mode: K-blocks per TMEM accumulation chunk
+  // Optional fused fp16 copies of the written result (column-major, ld_out):
+  //   out_hi = fp16(v), out_lo = fp16((v - out_hi) * out_lo_scale)
+  __half* out_hi;
+  __half* out_lo;
+  long long ld_out;
+  float out_lo_scale;
+  int* err;
+};
+
+template <int BN_, int NSPLIT_, bool A_MN_, bool B_MN_>
+struct GemmCfg {
+  static constexpr int BM = 128, BN = BN_, BK = 64;
+  static constexpr int NSPLIT = NSPLIT_;
+  static constexpr bool A_MN = A_MN_, B_MN = B_MN_;
+  static constexpr int NOPS = (NSPLIT == 1) ? 1 : 2;  // copies per operand (hi[, lo])
+  static constexpr int A_BYTES = BM * BK * 2;
+  static constexpr int B_BYTES = BN * BK * 2;
+  static constexpr int STAGE_BYTES = NOPS * (A_BYTES + B_BYTES);
+  static constexpr int STAGES = (STAGE_BYTES <= 48 * 1024) ? 4 : 3;
+  static constexpr int NACC = (NSPLIT == 1) ? 1 : 2;
+  static constexpr int ACC_COLS = NACC * BN;  // TMEM columns per accumulation buffer
+  static constexpr int TMEM_COLS = 2 * ACC_COLS;
+  static_assert(TMEM_COLS <= 512, "TMEM budget");
+  static constexpr int BAR_BYTES = 256;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + BAR_BYTES;
+  static constexpr uint32_t IDESC = idesc_f16(BM, BN, false, A_MN, B_MN);
+  static constexpr int THREADS = 192;
+};
+
+template <bool MN, int ROWS>
+__device__ __forceinline__ void load_operand(uint8_t* dst, const CUtensorMap* map, uint64_t* bar, int row0, int k) {
+  if constexpr (MN) {
+#pragma unroll
+    for (int j = 0; j < ROWS / 64; ++j) tma_load_2d(dst + j * 8192, map, bar, row0 + 64 * j, k);
+  } else {
+    tma_load_2d(dst, map, bar, k, row0);
+  }
+}
+
+template <bool MN>
+__device__ __forceinline__ uint64_t operand_desc(uint32_t base, int kk) {
+  if constexpr (MN) {
+    return sdesc_sw128(base + kk * 2048, 8192, 1024);
+  } else {
+    return sdesc_sw128(base + kk * 32, 16, 1024);
+  }
+}
+
+// alpha/beta update of 32 consecutive columns of one row of C, with the
+// lower-triangle mask, bounds and the optional fused fp16 hi/lo copies.
+__device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const float* v, long long gi, long long gj0) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const long long gj = gj0 + j;
+    const bool keep = gj < args.N && !(args.tri && (gi - gj) < args.diag);
+    if (!keep) continue;
+    float* cp = args.C + gi + gj * args.ldc;
+    float r = args.alpha * v[j];
+    if (args.beta != 0.0f) r = fmaf(args.beta, *cp, r);
+    *cp = r;
+    if (args.out_hi) {
+      const __half h = __float2half_rn(r);
+      args.out_hi[gi + gj * args.ld_out] = h;
+      if (args.out_lo) args.out_lo[gi + gj * args.ld_out] = __float2half_rn((r - __half2float(h)) * args.out_lo_scale);
+    }
+  }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ GemmArgs args) {
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * Cfg::STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* tfull = empty + STAGES;  // [2]
+  uint64_t* tempty = tfull + 2;      // [2]
+  uint64_t* drain = tempty + 2;      // [1] teardown barrier for the MMA issuer
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_map(&args.mapA[0]);
+    tma_prefetch_map(&args.mapB[0]);
+    if (Cfg::NSPLIT > 1) {
+      tma_prefetch_map(&args.mapA[1]);
+      tma_prefetch_map(&args.mapB[1]);
+    }
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      uint32_t issued_mask = 0, phase_mask = 0;  // per-stage: copy issued / its phase
+      bool ok = true;
+      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+        const int4 tile = args.tiles[t];
+        for (int kb = tile.z; kb < tile.w; ++kb) {
+          if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&full[s], Cfg::STAGE_BYTES);
+          uint8_t* st = smem + s * Cfg::STAGE_BYTES;
+          const int k = args.k_off + kb * BK;
+#pragma unroll
+          for (int h = 0; h < Cfg::NOPS; ++h) {
+            load_operand<Cfg::A_MN, BM>(st + h * Cfg::A_BYTES, &args.mapA[h], &full[s], args.a_off + tile.x, k);
+            load_operand<Cfg::B_MN, BN>(st + Cfg::NOPS * Cfg::A_BYTES + h * Cfg::B_BYTES, &args.mapB[h], &full[s],
+                                        args.b_off + tile.y, k);
+          }
+          issued_mask |= 1u << s;
+          phase_mask = (phase_mask & ~(1u << s)) | (ph << s);
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+      if (!ok) {
+        // Abort path: let every copy in flight land before the CTA exits.
+        for (int i = 0; i < STAGES; ++i) {
+          if (!((issued_mask >> i) & 1u)) continue;
+          const uint64_t t0 = globaltimer_ns();
+          while (!mbar_try_wait(&full[i], (phase_mask >> i) & 1u)) {
+            if (globaltimer_ns() - t0 > 1000000000ull) {
+              if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
+              break;
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    // Accumulation "chunks": plain mode accumulates a tile's whole K range in
+    // one TMEM buffer; split mode closes a chunk every `kchunk` K-blocks so
+    // the epilogue can fold it into round-to-nearest FP32 registers (the
+    // tensor core's own accumulation truncates).
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int it = 0;  // chunk counter (selects TMEM buffer and phase)
+      bool ok = true;
+      bool any = false;
+      const int kc = (Cfg::NSPLIT > 1) ? args.kchunk : (1 << 30);
+      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+        const int4 tile = args.tiles[t];
+        for (int c0 = tile.z; c0 < tile.w && ok; c0 += kc, ++it) {
+          const int c1 = (tile.w - c0 > kc) ? c0 + kc : tile.w;
+          const int buf = it & 1;
+          const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+          if (!mbar_wait(&tempty[buf], tph ^ 1u, abort_flag, args.err, kDevErrTimeoutMma)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d0 = tmem_base + (uint32_t)(buf * Cfg::ACC_COLS);
+          for (int kb = c0; kb < c1; ++kb) {
+            if (!mbar_wait(&full[s], ph, abort_flag, args.err, kDevErrTimeoutMma)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t st = smem_u32(smem + s * Cfg::STAGE_BYTES);
+            const uint32_t a_hi = st, b_hi = st + Cfg::NOPS * Cfg::A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint32_t acc = (kb > c0 || kk > 0) ? 1u : 0u;
+              const uint64_t da = operand_desc<Cfg::A_MN>(a_hi, kk);
+              const uint64_t db = operand_desc<Cfg::B_MN>(b_hi, kk);
+              umma_f16(d0, da, db, Cfg::IDESC, acc);
+              if constexpr (Cfg::NSPLIT > 1) {
+                const uint64_t da_lo = operand_desc<Cfg::A_MN>(a_hi + Cfg::A_BYTES, kk);
+                const uint64_t db_lo = operand_desc<Cfg::B_MN>(b_hi + Cfg::B_BYTES, kk);
+                umma_f16(d0 + BN, da, db_lo, Cfg::IDESC, acc);
+                umma_f16(d0 + BN, da_lo, db, Cfg::IDESC, 1u);
+              }
+            }
+            any = true;
+            tc_commit(&empty[s]);
+            if (++s == STAGES) {
+              s = 0;
+              ph ^= 1u;
+            }
+          }
+          if (!ok) break;
+          tc_commit(&tfull[buf]);
+        }
+      }
+      if (!ok && any) {
+        // Abort path: wait (bounded) until every issued MMA has retired.
+        tc_commit(drain);
+        const uint64_t t0 = globaltimer_ns();
+        while (!mbar_try_wait(drain, 0)) {
+          if (globaltimer_ns() - t0 > 1000000000ull) {
+            if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
+            break;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+    const int row = quarter * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    int it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+      const int4 tile = args.tiles[t];
+      const long long gi = (long long)tile.x + row;
+      const bool row_ok = gi < args.M;
+      if constexpr (Cfg::NSPLIT == 1) {
+        const int buf = it & 1;
+        const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+        ++it;
+        if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) break;
+        tc_fence_after();
+        const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+          float v[32];
+          tmem_ld32(tacc + c0, v);
+          if (row_ok) epilogue_store32(args, v, gi, (long long)tile.y + c0);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+      } else {
+        float acc[BN];
+#pragma unroll
+        for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+        for (int c0k = tile.z; c0k < tile.w; c0k += args.kchunk) {
+          const int buf = it & 1;
+          const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+          ++it;
+          if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+#pragma unroll
+          for (int c0 = 0; c0 < BN; c0 += 32) {
+            float v[32], w[32];
+            tmem_ld32(tacc + c0, v);
+            tmem_ld32(tacc + BN + c0, w);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc[c0 + j] += fmaf(args.corr_scale, w[j], v[j]);
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[buf]);
+        }
+        if (!ok) break;
+        if (row_ok) {
+#pragma unroll
+          for (int c0 = 0; c0 < BN; c0 += 32) epilogue_store32(args, acc + c0, gi, (long long)tile.y + c0);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
+}
+
+}  // namespace tb

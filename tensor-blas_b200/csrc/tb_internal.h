@@ -1,0 +1,96 @@
+// Internal host-side interfaces shared by the routine drivers.
+#pragma once
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/tb_capi.h"
+
+namespace tb {
+
+// ------------------------------------------------------------------ status
+#define TB_CUDA_TRY(expr)                              \
+  do {                                                 \
+    cudaError_t e_ = (expr);                           \
+    if (e_ != cudaSuccess) return tb::cuda_status(e_); \
+  } while (0)
+#define TB_TRY(expr)                       \
+  do {                                     \
+    tb_status s_ = (expr);                 \
+    if (s_ != TB_SUCCESS) return s_;       \
+  } while (0)
+
+tb_status cuda_status(cudaError_t e);
+void set_last_error(const char* fmt, ...);
+
+// ------------------------------------------------------------------ streams / pool
+cudaStream_t current_stream();
+// Device scratch owned by the library (grow-only, per device). Returns
+// nullptr on allocation failure. Growing synchronises the device.
+void* pool_get(size_t bytes);
+// Device error word used by bounded waits inside kernels (per device).
+int* device_error_word();
+// Reads and clears the device error word (synchronises `stream`).
+tb_status check_device_error(cudaStream_t stream);
+int sm_count();
+
+inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+// ------------------------------------------------------------------ operands
+// An fp16/bf16 matrix operand in global memory, indexed (row, k):
+//   mn_major: element (r, k) at ptr[r + k * ld]  (rows contiguous)
+//   k-major : element (r, k) at ptr[k + r * ld]  (k contiguous)
+struct Operand {
+  const void* ptr = nullptr;
+  long long rows = 0;
+  long long cols = 0;  // K extent
+  long long ld = 0;
+  bool mn_major = true;
+};
+
+enum class Split { kPlain = 1, kHiLo = 3 };
+
+struct GemmCall {
+  Operand a_hi, a_lo, b_hi, b_lo;  // lo used in kHiLo only
+  Split split = Split::kPlain;
+  int a_off = 0, b_off = 0, k_off = 0;
+  const int4* tiles = nullptr;  // device tile list
+  int num_tiles = 0;
+  float* C = nullptr;
+  long long ldc = 0;
+  int M = 0, N = 0;
+  float alpha = 1.f, beta = 0.f;
+  int tri = 0, diag = 0;
+  float corr_scale = 1.0f / 2048.0f;
+  int kchunk = 2;  // split mode: K-blocks (64) per round-to-nearest fold
+  __half* out_hi = nullptr;
+  __half* out_lo = nullptr;
+  long long ld_out = 0;
+  float out_lo_scale = 2048.0f;
+};
+
+// Tile width along N used by the engine for a given split mode.
+int gemm_bn(Split s);
+constexpr int kGemmBM = 128;
+constexpr int kGemmBK = 64;
+
+tb_status gemm_launch(const GemmCall& call, cudaStream_t stream);
+
+// Tile plans (host vectors of {m0, n0, kb_begin, kb_end}); uploaded and
+// cached on the device by `upload_tiles`.
+std::vector<int4> plan_rect(int M, int N, int bn, int kb0, int kb1);
+std::vector<int4> plan_lower(int n, int bn, int kb0, int kb1);
+const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
+
+// ------------------------------------------------------------------ conversion
+// fp32 (rows x cols, column-major, lds) -> fp16 hi [and lo] with the same
+// orientation (ldd). lo = fp16((x - hi) * lo_scale).
+//   tri == 0: whole matrix; tri == 1: zero the strict upper triangle;
+//   tri == 2: only rows i >= j (rounded down to 8) are written.
+tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
+                          long long ldd, float lo_scale, int tri, cudaStream_t stream);
+
+}  // namespace tb

@@ -1,0 +1,387 @@
+// TRSM driver (reference: BLAS/tc_trsm.cu:31-174, tc_cumpsgemm_trsm.cu).
+//
+// Method (the reference's): recursive halving of the triangular operand.
+// A node [s, e) solves its left half, applies the off-diagonal update
+//   right side  B[:, mid:e] -= X[:, s:mid] * A[mid:e, s:mid]^T
+//   left side   B[mid:e, :] -= A[mid:e, s:mid] * X[s:mid, :]
+// as one FP16-operand / FP32-accumulate tensor-core GEMM, then solves its
+// right half. Leaves are diagonal blocks of nb (<= 512) columns.
+//
+// B200 form of the pieces:
+//  * A is converted to FP16 once (lower part only), not per level.
+//  * X is converted exactly once, in the epilogue of the leaf product that
+//    produces it (fused hi[/lo] copies), not re-converted at every level as
+//    the reference does with B1 (BLAS/tc_trsm.cu:59-66).
+//  * The leaf replaces FP32 cublasStrsm with X_b = B_b * inv(A_bb)^T (or
+//    inv(A_bb) * B_b): inv(A_bb) is computed in FP64 by warp-level
+//    substitution on 32x32 diagonal sub-blocks plus blocked 32-wide column
+//    chains in shared memory, and applied with the split-FP16 3-product
+//    tensor-core GEMM, i.e. FP32-level accuracy like the reference's leaf.
+//  * Split points are multiples of 64 so every TMA coordinate stays aligned.
+//    For n = nb * 2^L (the configured 16384 / 512) the leaves coincide with
+//    the reference's recursion exactly.
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include "tb_internal.h"
+
+namespace tb {
+
+namespace {
+
+constexpr int kLeafMax = 512;  // largest diagonal block inverted explicitly
+
+// Inverse of each 32x32 diagonal sub-block of A (rows/cols >= n padded with
+// the identity). One warp per sub-block; lane c owns column c of the inverse
+// and runs forward substitution in FP64 registers; rows of L are broadcast
+// from shared memory. Output: D[t*1024 + i + 32*c] (column-major 32x32).
+__global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const float* __restrict__ A, long long lda,
+                                                        double* __restrict__ D) {
+  __shared__ double L[32][33];
+  const long long t = blockIdx.x;
+  const int c = threadIdx.x;
+  const long long base = t * 32;
+  for (int i = 0; i < 32; ++i) {
+    const long long gi = base + i, gj = base + c;
+    double v;
+    if (gi < n && gj < n)
+      v = (i >= c) ? (double)A[gi + gj * lda] : 0.0;
+    else
+      v = (i == c) ? 1.0 : 0.0;
+    L[i][c] = v;
+  }
+  __syncwarp();
+  double w[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    double s = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+    for (int p = 0; p < i; ++p) s -= L[i][p] * w[p];
+    w[i] = (i < c) ? 0.0 : s / L[i][i];
+  }
+#pragma unroll
+  for (int i = 0; i < 32; ++i) D[t * 1024 + i + 32 * c] = w[i];
+}
+
+// Column chain j of the inverse of leaf block b (rows/cols [s, s+size)):
+//   W[i][j] = -Dinv_i * sum_{p=j}^{i-1} L[i][p] W[p][j]   (32x32 sub-blocks)
+// The 32-wide column panel of W lives in shared memory (FP64); each 32x32
+// sub-block of L and each Dinv_i is staged through shared memory with
+// coalesced loads before use. The result is written as the FP16 hi/lo pair
+// (lo scaled by 2^11) of W, column-major with leading dimension ldw, zeros
+// above the diagonal.
+__global__ void __launch_bounds__(256) trtri_chain_kernel(const float* __restrict__ A, long long lda,
+                                                          const int2* __restrict__ leaves, const double* __restrict__ D,
+                                                          __half* __restrict__ Whi, __half* __restrict__ Wlo,
+                                                          long long ldw, long long wstride) {
+  extern __shared__ double sm[];
+  __shared__ double Ls[32][33];  // staged L sub-block (or Dinv_i)
+  __shared__ double Ts[32][33];
+  const int2 leaf = leaves[blockIdx.y];  // {s, size}
+  const int s = leaf.x, size = leaf.y;
+  const int nsub = (size + 31) / 32;
+  const int j = blockIdx.x;
+  if (j >= nsub) return;
+  double* Wp = sm;  // [(nsub - j) * 32][32]: row (within panel) major
+  const int tid = threadIdx.x;
+  const int r = tid & 31, cq = tid >> 5;     // compute role: row r, columns cq + 8q
+  const long long sub0 = (long long)s / 32;  // global 32-sub-block index of the leaf's first sub-block
+  for (int q = 0; q < 4; ++q) {
+    const int c = cq + 8 * q;
+    Wp[r * 32 + c] = D[(sub0 + j) * 1024 + r + 32 * c];
+  }
+  __syncthreads();
+  for (int i = j + 1; i < nsub; ++i) {
+    double acc[4] = {0, 0, 0, 0};
+    for (int p = j; p < i; ++p) {
+      // stage L(32i + rr, 32p + cc): thread loads rows rr = tid&31 of columns cc = tid>>5 + 8q
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int cc = cq + 8 * q;
+        const int gr = 32 * i + r, gc = 32 * p + cc;
+        Ls[r][cc] = (gr < size && gc < size) ? (double)A[(long long)s + gr + ((long long)s + gc) * lda] : 0.0;
+      }
+      __syncthreads();
+      const double* wrow = Wp + (32 * (p - j)) * 32;
+#pragma unroll 8
+      for (int kk = 0; kk < 32; ++kk) {
+        const double l = Ls[r][kk];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] = fma(l, wrow[kk * 32 + cq + 8 * q], acc[q]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      Ts[r][cq + 8 * q] = acc[q];
+      Ls[r][cq + 8 * q] = D[(sub0 + i) * 1024 + r + 32 * (cq + 8 * q)];  // Dinv_i(r, c)
+    }
+    __syncthreads();
+    double o[4] = {0, 0, 0, 0};
+#pragma unroll 8
+    for (int kk = 0; kk < 32; ++kk) {
+      const double dv = Ls[r][kk];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) o[q] = fma(-dv, Ts[kk][cq + 8 * q], o[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Wp[(32 * (i - j) + r) * 32 + cq + 8 * q] = o[q];
+    __syncthreads();
+  }
+  // write the 32 columns [32j, 32j+32) of W for all rows of the leaf
+  __half* hi = Whi + (long long)blockIdx.y * wstride;
+  __half* lo = Wlo + (long long)blockIdx.y * wstride;
+  for (int q = 0; q < 4; ++q) {
+    const int c = cq + 8 * q;
+    const int gc = 32 * j + c;
+    if (gc >= size) continue;
+    for (int row = r; row < size; row += 32) {
+      double v = 0.0;
+      if (row >= 32 * j) v = Wp[(row - 32 * j) * 32 + c];
+      const __half h = __float2half_rn((float)v);
+      hi[row + (long long)gc * ldw] = h;
+      lo[row + (long long)gc * ldw] = __float2half_rn((float)((v - (double)__half2float(h)) * 2048.0));
+    }
+  }
+}
+
+struct TrsmCtx {
+  bool right;
+  long m, n;  // B is m x n
+  long nt;    // order of A (n for right, m for left)
+  float* B;
+  long ldb;
+  Split split;
+  int leaf;  // leaf block size (multiple of 64)
+  // FP16 copies
+  __half *ah, *al;  // A (nt x nt, MN-major, lda_h)
+  long long lda_h;
+  __half *xh, *xl;  // X: right: m x n col-major (ld ldx, MN-major operand)
+                    //    left : m x n col-major (ld ldx, K-major operand, rows = n)
+  long long ldx;
+  __half *wh, *wl;  // per-leaf inverses (ldw x leaf each)
+  long long ldw, wstride;
+  __half *rh, *rl;  // current leaf block of B
+  long long ldr;
+  cudaStream_t st;
+};
+
+tb_status leaf_solve(TrsmCtx& c, int bidx, long s, long e) {
+  const long nbl = e - s;
+  GemmCall g;
+  g.split = Split::kHiLo;
+  const bool split_x = c.split == Split::kHiLo;
+  if (c.right) {
+    // R = B[:, s:e] (m x nbl) -> FP16 hi/lo; X_b = R * W^T
+    TB_TRY(convert_f32_f16(c.m, nbl, c.B + s * c.ldb, c.ldb, c.rh, c.rl, c.ldr, 2048.f, 0, c.st));
+    g.a_hi = {c.rh, c.m, nbl, c.ldr, true};
+    g.a_lo = {c.rl, c.m, nbl, c.ldr, true};
+    g.b_hi = {c.wh + bidx * c.wstride, nbl, nbl, c.ldw, true};
+    g.b_lo = {c.wl + bidx * c.wstride, nbl, nbl, c.ldw, true};
+    g.C = c.B + s * c.ldb;
+    g.ldc = c.ldb;
+    g.M = (int)c.m;
+    g.N = (int)nbl;
+    g.out_hi = c.xh + s * c.ldx;
+    g.out_lo = split_x ? c.xl + s * c.ldx : nullptr;
+    g.ld_out = c.ldx;
+  } else {
+    // R = B[s:e, :] (nbl x n) -> FP16 hi/lo (K-major operand, rows = n); X_b = W * R
+    TB_TRY(convert_f32_f16(nbl, c.n, c.B + s, c.ldb, c.rh, c.rl, c.ldr, 2048.f, 0, c.st));
+    g.a_hi = {c.wh + bidx * c.wstride, nbl, nbl, c.ldw, true};
+    g.a_lo = {c.wl + bidx * c.wstride, nbl, nbl, c.ldw, true};
+    g.b_hi = {c.rh, c.n, nbl, c.ldr, false};
+    g.b_lo = {c.rl, c.n, nbl, c.ldr, false};
+    g.C = c.B + s;
+    g.ldc = c.ldb;
+    g.M = (int)nbl;
+    g.N = (int)c.n;
+    g.out_hi = c.xh + s;
+    g.out_lo = split_x ? c.xl + s : nullptr;
+    g.ld_out = c.ldx;
+  }
+  g.alpha = 1.f;
+  g.beta = 0.f;
+  const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split), 0, (int)((nbl + kGemmBK - 1) / kGemmBK));
+  g.tiles = upload_tiles(plan, c.st);
+  if (!g.tiles) return TB_ERROR_ALLOC;
+  g.num_tiles = (int)plan.size();
+  return gemm_launch(g, c.st);
+}
+
+tb_status update(TrsmCtx& c, long s, long mid, long e) {
+  GemmCall g;
+  g.split = c.split;
+  const bool hilo = c.split == Split::kHiLo;
+  const long kk = mid - s;
+  if (c.right) {
+    // B[:, mid:e] -= X[:, s:mid] * A[mid:e, s:mid]^T
+    g.a_hi = {c.xh, c.m, c.n, c.ldx, true};
+    g.a_lo = {hilo ? c.xl : nullptr, c.m, c.n, c.ldx, true};
+    g.b_hi = {c.ah, c.nt, c.nt, c.lda_h, true};
+    g.b_lo = {hilo ? c.al : nullptr, c.nt, c.nt, c.lda_h, true};
+    g.a_off = 0;
+    g.b_off = (int)mid;
+    g.C = c.B + mid * c.ldb;
+    g.M = (int)c.m;
+    g.N = (int)(e - mid);
+  } else {
+    // B[mid:e, :] -= A[mid:e, s:mid] * X[s:mid, :]
+    g.a_hi = {c.ah, c.nt, c.nt, c.lda_h, true};
+    g.a_lo = {hilo ? c.al : nullptr, c.nt, c.nt, c.lda_h, true};
+    g.b_hi = {c.xh, c.n, c.m, c.ldx, false};
+    g.b_lo = {hilo ? c.xl : nullptr, c.n, c.m, c.ldx, false};
+    g.a_off = (int)mid;
+    g.b_off = 0;
+    g.C = c.B + mid;
+    g.M = (int)(e - mid);
+    g.N = (int)c.n;
+  }
+  g.k_off = (int)s;
+  g.ldc = c.ldb;
+  g.alpha = -1.f;
+  g.beta = 1.f;
+  const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split), 0, (int)((kk + kGemmBK - 1) / kGemmBK));
+  g.tiles = upload_tiles(plan, c.st);
+  if (!g.tiles) return TB_ERROR_ALLOC;
+  g.num_tiles = (int)plan.size();
+  return gemm_launch(g, c.st);
+}
+
+tb_status recurse(TrsmCtx& c, long s, long e, const std::vector<long>& leaf_start) {
+  if (e - s <= c.leaf) {
+    const int bidx = (int)(std::lower_bound(leaf_start.begin(), leaf_start.end(), s) - leaf_start.begin());
+    return leaf_solve(c, bidx, s, e);
+  }
+  // split at a leaf boundary near the middle (multiple of the leaf size)
+  const long nleaves = (e - s + c.leaf - 1) / c.leaf;
+  const long mid = s + ((nleaves + 1) / 2) * c.leaf;
+  TB_TRY(recurse(c, s, mid, leaf_start));
+  TB_TRY(update(c, s, mid, e));
+  return recurse(c, mid, e, leaf_start);
+}
+
+}  // namespace
+
+tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float* B, long ldb, long nb, Split split,
+                    cudaStream_t st) {
+  if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
+  const long nt = right ? n : m;
+  if (lda < (nt > 1 ? nt : 1) || ldb < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
+  if (m == 0 || n == 0) return TB_SUCCESS;
+  TrsmCtx c;
+  c.right = right;
+  c.m = m;
+  c.n = n;
+  c.nt = nt;
+  c.B = B;
+  c.ldb = ldb;
+  c.split = split;
+  c.st = st;
+  long leaf = round_up(std::min<long>(nb, kLeafMax), 64);
+  if (leaf > kLeafMax) leaf = kLeafMax;
+  c.leaf = (int)leaf;
+  const bool hilo = split == Split::kHiLo;
+
+  std::vector<long> leaf_start;
+  std::vector<int2> leaves;
+  for (long s = 0; s < nt; s += leaf) {
+    leaf_start.push_back(s);
+    leaves.push_back(make_int2((int)s, (int)std::min<long>(leaf, nt - s)));
+  }
+  const long nleaf = (long)leaves.size();
+
+  c.lda_h = round_up(nt, 64);
+  // X copy: right: m x n, MN-major rows m; left: m x n col-major, K-major (K = m rows)
+  c.ldx = round_up(m, 64);
+  c.ldw = leaf;
+  c.wstride = c.ldw * leaf;
+  c.ldr = right ? round_up(m, 64) : leaf;
+  const size_t a_bytes = (size_t)c.lda_h * nt * 2;
+  const size_t x_bytes = (size_t)c.ldx * n * 2;
+  const size_t w_bytes = (size_t)c.wstride * nleaf * 2;
+  const size_t r_bytes = (size_t)c.ldr * (right ? leaf : n) * 2;
+  const size_t d_bytes = (size_t)((nt + 31) / 32) * 1024 * sizeof(double);
+  const size_t l_bytes = (size_t)nleaf * sizeof(int2);
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t o = off;
+    off += round_up((long long)b, 256);
+    return o;
+  };
+  const size_t o_ah = take(a_bytes), o_al = hilo ? take(a_bytes) : 0;
+  const size_t o_xh = take(x_bytes), o_xl = hilo ? take(x_bytes) : 0;
+  const size_t o_wh = take(w_bytes), o_wl = take(w_bytes);
+  const size_t o_rh = take(r_bytes), o_rl = take(r_bytes);
+  const size_t o_d = take(d_bytes), o_lv = take(l_bytes);
+  char* ws = static_cast<char*>(pool_get(off));
+  if (!ws) {
+    set_last_error("trsm: cannot allocate %zu bytes of scratch", off);
+    return TB_ERROR_ALLOC;
+  }
+  c.ah = reinterpret_cast<__half*>(ws + o_ah);
+  c.al = hilo ? reinterpret_cast<__half*>(ws + o_al) : nullptr;
+  c.xh = reinterpret_cast<__half*>(ws + o_xh);
+  c.xl = hilo ? reinterpret_cast<__half*>(ws + o_xl) : nullptr;
+  c.wh = reinterpret_cast<__half*>(ws + o_wh);
+  c.wl = reinterpret_cast<__half*>(ws + o_wl);
+  c.rh = reinterpret_cast<__half*>(ws + o_rh);
+  c.rl = reinterpret_cast<__half*>(ws + o_rl);
+  double* D = reinterpret_cast<double*>(ws + o_d);
+  int2* dleaves = reinterpret_cast<int2*>(ws + o_lv);
+  TB_CUDA_TRY(cudaMemcpyAsync(dleaves, leaves.data(), l_bytes, cudaMemcpyHostToDevice, st));
+
+  // 1. FP16 copy of A's lower part (only off-diagonal leaf blocks are read)
+  if (nleaf > 1) TB_TRY(convert_f32_f16(nt, nt, A, lda, c.ah, c.al, c.lda_h, 2048.f, 2, st));
+  // 2. inverses of the diagonal leaf blocks (FP64), as FP16 hi/lo
+  const long nsub = (nt + 31) / 32;
+  diag_inv32_kernel<<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D);
+  TB_CUDA_TRY(cudaGetLastError());
+  const int max_chain = (int)(leaf / 32);
+  const size_t smem = (size_t)max_chain * 1024 * sizeof(double);
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_done[dev]) {
+    TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kLeafMax / 32 * 1024 * sizeof(double))));
+    attr_done[dev] = true;
+  }
+  dim3 grid((unsigned)max_chain, (unsigned)nleaf);
+  trtri_chain_kernel<<<grid, 256, smem, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride);
+  TB_CUDA_TRY(cudaGetLastError());
+  // 3. recursion
+  return recurse(c, 0, nt, leaf_start);
+}
+
+}  // namespace tb
+
+extern "C" tb_status tb_strsm(char side, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
+                              int precision) {
+  bool right;
+  if (side == 'R' || side == 'r')
+    right = true;
+  else if (side == 'L' || side == 'l')
+    right = false;
+  else
+    return TB_ERROR_INVALID_VALUE;
+  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT) return TB_ERROR_INVALID_VALUE;
+  return tb::trsm_impl(right, m, n, A, lda, B, ldb, nb,
+                       precision == TB_PREC_SPLIT ? tb::Split::kHiLo : tb::Split::kPlain, tb::current_stream());
+}
+
+// ------------------------------------------------------------------ reference C++ API
+#include "../../include/TensorBLAS.h"
+
+void tc_trsm(cublasHandle_t, long int m, long int n, float* A, long int lda, float* B, long int ldb, __half*,
+             long int nb) {
+  tb_status s = tb::trsm_impl(true, m, n, A, lda, B, ldb, nb, tb::Split::kPlain, tb::current_stream());
+  if (s != TB_SUCCESS) fprintf(stderr, "TensorBLAS tc_trsm: %s %s\n", tb_status_string(s), tb_last_error());
+}
+
+void tc_cumpsgemm_trsm(cublasHandle_t, cumpsgemm::handle_t, long int m, long int n, float* A, long int lda, float* B,
+                       long int ldb, long int nb) {
+  tb_status s = tb::trsm_impl(true, m, n, A, lda, B, ldb, nb, tb::Split::kHiLo, tb::current_stream());
+  if (s != TB_SUCCESS) fprintf(stderr, "TensorBLAS tc_cumpsgemm_trsm: %s %s\n", tb_status_string(s), tb_last_error());
+}

@@ -1,0 +1,152 @@
+"""Python front-end of the B200 TensorBLAS library (ctypes over the C ABI).
+
+Mirrors the reference's python/TensorBLAS.py (Orgline/Tensor-BLAS):
+``tc_syrk(A, transpose=False, nb=256)`` and ``tc_trsm(A, B, nb=256)`` with the
+same argument meaning, the same row-major torch <-> column-major bridging and
+the same failure behaviour (``assert status == 0``).  Beyond the reference it
+exposes the precision choice and the other BLAS3 routines of include/tb_capi.h.
+
+The shared library is loaded from ../lib/libTensorBLAS.so (built in-tree by
+``make -C tensor-blas_b200``); importing this module fails loudly if it is
+missing — there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import torch
+
+dir_path = os.path.dirname(os.path.realpath(__file__))
+LIB_PATH = os.path.join(dir_path, "..", "lib", "libTensorBLAS.so")
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"TensorBLAS native library not built: {LIB_PATH} (run make -C tensor-blas_b200)")
+lib = ctypes.CDLL(LIB_PATH)
+
+PLAIN = 0  # FP16 operands, FP32 accumulation (reference tc_*)
+SPLIT = 1  # FP16 hi + scaled-lo, 3 products, FP32-level accuracy
+
+_c_long = ctypes.c_long
+_fp = ctypes.c_void_p
+
+lib.tc_syrk_wrapper.argtypes = [_c_long, _c_long, _fp, _fp, _c_long]
+lib.tc_syrk_wrapper.restype = ctypes.c_int
+lib.tc_trsm_wrapper.argtypes = [_c_long, _c_long, _fp, _fp, _c_long]
+lib.tc_trsm_wrapper.restype = ctypes.c_int
+lib.tb_set_stream.argtypes = [ctypes.c_void_p]
+lib.tb_set_stream.restype = ctypes.c_int
+lib.tb_synchronize.argtypes = []
+lib.tb_synchronize.restype = ctypes.c_int
+lib.tb_last_error.argtypes = []
+lib.tb_last_error.restype = ctypes.c_char_p
+lib.tb_status_string.argtypes = [ctypes.c_int]
+lib.tb_status_string.restype = ctypes.c_char_p
+lib.tb_sgemm.argtypes = [ctypes.c_char, ctypes.c_char, _c_long, _c_long, _c_long, ctypes.c_float, _fp, _c_long, _fp,
+                         _c_long, ctypes.c_float, _fp, _c_long, ctypes.c_int]
+lib.tb_sgemm.restype = ctypes.c_int
+lib.tb_ssyrk.argtypes = [ctypes.c_char, ctypes.c_char, _c_long, _c_long, ctypes.c_float, _fp, _c_long,
+                         ctypes.c_float, _fp, _c_long, _c_long, ctypes.c_int]
+lib.tb_ssyrk.restype = ctypes.c_int
+lib.tb_strsm.argtypes = [ctypes.c_char, _c_long, _c_long, _fp, _c_long, _fp, _c_long, _c_long, ctypes.c_int]
+lib.tb_strsm.restype = ctypes.c_int
+
+
+class TensorBLASError(RuntimeError):
+    pass
+
+
+def _check(status):
+    if status != 0:
+        msg = lib.tb_last_error().decode(errors="replace")
+        name = lib.tb_status_string(status).decode()
+        raise TensorBLASError(f"{name}: {msg}")
+
+
+def _bind_stream(t):
+    lib.tb_set_stream(ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream))
+
+
+def _dev_f32(t, name):
+    if not (t.is_cuda and t.dtype == torch.float32):
+        raise TypeError(f"{name} must be a float32 CUDA tensor")
+
+
+# ---------------------------------------------------------------- reference API
+def tc_syrk(A, transpose=False, nb=256):
+    """C = A @ A.T (full symmetric n x n) for a row-major torch A (n x k).
+
+    With transpose=True computes A.T @ A, as python/TensorBLAS.py:11-34.
+    """
+    if transpose:
+        A = torch.clone(A.T).contiguous()
+    n = A.size(0)
+    k = A.size(1)
+    C = torch.zeros(n, n, device=A.device, dtype=torch.float32)
+    _bind_stream(A)
+    status = lib.tc_syrk_wrapper(n, k, A.data_ptr(), C.data_ptr(), nb)
+    assert status == 0
+    return C
+
+
+def tc_trsm(A, B, nb=256):
+    """X with X @ A.T = B for lower-triangular A, as python/TensorBLAS.py:43-68."""
+    n = A.size(0)
+    m = B.size(0)
+    A = torch.clone(A.T).contiguous()
+    B_inout = torch.clone(B.T).contiguous()
+    _bind_stream(B_inout)
+    status = lib.tc_trsm_wrapper(m, n, A.data_ptr(), B_inout.data_ptr(), nb)
+    assert status == 0
+    return B_inout.T
+
+
+# ---------------------------------------------------------------- column-major BLAS-style API
+# Matrices are passed as torch tensors holding COLUMN-MAJOR data: a tensor
+# `T` of shape (cols, rows) row-major is the rows x cols column-major matrix
+# T.T. Helpers below take the logical matrix and handle that.
+def sgemm(transa, transb, m, n, k, alpha, A_cm, lda, B_cm, ldb, beta, C_cm, ldc, precision=PLAIN):
+    """Raw column-major SGEMM on device buffers (tensor-core products at `precision`)."""
+    _check(lib.tb_sgemm(transa.encode(), transb.encode(), m, n, k, alpha, A_cm.data_ptr(), lda, B_cm.data_ptr(), ldb,
+                        beta, C_cm.data_ptr(), ldc, precision))
+
+
+def ssyrk(A_cm, C_cm, n, k, lda, ldc, alpha=1.0, beta=0.0, trans="N", nb=256, precision=PLAIN):
+    """Raw column-major SSYRK on device buffers (lower triangle)."""
+    _check(lib.tb_ssyrk(b"L", trans.encode(), n, k, alpha, A_cm.data_ptr(), lda, beta, C_cm.data_ptr(), ldc, nb,
+                        precision))
+
+
+def strsm(side, A_cm, B_cm, m, n, lda, ldb, nb=512, precision=PLAIN):
+    """Raw column-major STRSM (lower, non-unit); side 'R': X A^T = B, 'L': A X = B."""
+    _check(lib.tb_strsm(side.encode(), m, n, A_cm.data_ptr(), lda, B_cm.data_ptr(), ldb, nb, precision))
+
+
+def syrk(A, alpha=1.0, beta=0.0, C=None, nb=256, precision=PLAIN):
+    """Lower triangle of alpha * A @ A.T + beta * C for a logical n x k torch matrix A.
+
+    Returns an n x n tensor whose strict upper triangle is C's (or zero).
+    """
+    _dev_f32(A, "A")
+    n, k = A.shape
+    Acm = A.t().contiguous()  # storage = column-major n x k
+    if C is None:
+        Ccm = torch.zeros(n, n, device=A.device, dtype=torch.float32)
+    else:
+        Ccm = C.t().contiguous()
+    _bind_stream(A)
+    ssyrk(Acm, Ccm, n, k, n, n, alpha, beta, "N", nb, precision)
+    return Ccm.t()
+
+
+def trsm(A, B, side="L", nb=512, precision=PLAIN):
+    """Solve A X = B (side 'L') or X A^T = B (side 'R') for lower-triangular A."""
+    _dev_f32(A, "A")
+    _dev_f32(B, "B")
+    m, n = B.shape
+    Acm = A.t().contiguous()
+    Bcm = B.t().contiguous()
+    _bind_stream(B)
+    strsm(side, Acm, Bcm, m, n, A.shape[0], m, nb, precision)
+    return Bcm.t()
+
+
+def synchronize():
+    _check(lib.tb_synchronize())

@@ -1,0 +1,84 @@
+"""Records outputs of the REFERENCE library on seeded inputs (run on a B200).
+
+    make -C oracle                      # builds oracle/_ref/ from the reference sources
+    python tests/golden/make_golden.py  # writes tests/golden/ref_*.npz
+
+The reference routines run through oracle/_ref/libTensorBLAS_ref.so
+(oracle/ref_driver.cu wraps the reference's own tc_* C++ API with host
+buffers). Large outputs are stored as sampled entries plus row sums.
+"""
+import ctypes
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+import golden_inputs as gi  # noqa: E402
+
+lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libTensorBLAS_ref.so"))
+P = ctypes.c_void_p
+L = ctypes.c_long
+lib.ref_syrk.argtypes = [L, L, ctypes.c_float, P, ctypes.c_float, P, L]
+lib.ref_trsm.argtypes = [L, L, P, P, L]
+lib.ref_trmm.argtypes = [L, L, ctypes.c_float, P, P, P, L]
+lib.ref_syr2k.argtypes = [L, L, ctypes.c_float, P, P, ctypes.c_float, P, L]
+lib.ref_symm.argtypes = [L, L, ctypes.c_float, P, P, ctypes.c_float, P]
+lib.ref_ozimmu_syrk.argtypes = [L, L, ctypes.c_double, P, ctypes.c_double, P, L]
+for f in ("ref_syrk", "ref_trsm", "ref_trmm", "ref_syr2k", "ref_symm", "ref_ozimmu_syrk"):
+    getattr(lib, f).restype = ctypes.c_int
+
+
+def cm(x):
+    """Column-major (Fortran) copy and its pointer."""
+    a = np.asfortranarray(x)
+    return a, a.ctypes.data_as(P)
+
+
+def save(name, **kw):
+    np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **kw)
+    print("wrote", name, {k: getattr(v, "shape", v) for k, v in kw.items()})
+
+
+def sample_lower(n, count, seed):
+    g = gi.rng(seed)
+    i = g.integers(0, n, count)
+    j = g.integers(0, n, count)
+    lo, hi = np.maximum(i, j), np.minimum(i, j)
+    return lo, hi
+
+
+def syrk(name, n, k, nb, alpha, beta, seed, full):
+    A = gi.uniform(seed, (n, k))
+    C0 = gi.uniform(seed + 1, (n, n)) if beta != 0 else np.zeros((n, n), np.float32)
+    Af, pA = cm(A)
+    Cf, pC = cm(C0)
+    assert lib.ref_syrk(n, k, alpha, pA, beta, pC, nb) == 0
+    meta = dict(n=n, k=k, nb=nb, alpha=alpha, beta=beta, seed=seed, a_sum=gi.checksum(A))
+    if full:
+        save(name, C=np.tril(Cf).astype(np.float32), meta=json.dumps(meta))
+    else:
+        rows, cols = sample_lower(n, 20000, seed + 2)
+        save(name, rows=rows, cols=cols, vals=Cf[rows, cols].astype(np.float32),
+             rowsum=np.tril(Cf).astype(np.float64).sum(axis=1), meta=json.dumps(meta))
+
+
+def trsm(name, m, n, nb, seed):
+    A = gi.lower_tri(seed, n)
+    B = gi.uniform(seed + 1, (m, n))
+    Af, pA = cm(A)
+    Bf, pB = cm(B)
+    assert lib.ref_trsm(m, n, pA, pB, nb) == 0
+    save(name, X=Bf.astype(np.float32), meta=json.dumps(dict(m=m, n=n, nb=nb, seed=seed)))
+
+
+if __name__ == "__main__":
+    syrk("syrk_small", 256, 128, 64, 1.0, 0.0, 101, True)
+    syrk("syrk_beta", 200, 50, 64, 0.5, 2.0, 202, True)
+    syrk("syrk_p2", 8192, 64, 256, 1.0, 0.0, 303, False)
+    trsm("trsm_p2", 64, 2048, 256, 404)
+    trsm("trsm_small", 64, 1000, 256, 505)
+    trsm("trsm_p2_nb512", 32, 4096, 512, 606)
