@@ -46,6 +46,12 @@ TB_API const char* tb_last_error(void);
  * reported a bounded-wait timeout, TB_ERROR_CUDA on a CUDA error. */
 TB_API tb_status tb_synchronize(void);
 TB_API int tb_version(void);
+/* Number of kernels this library has launched in this process. */
+TB_API unsigned long long tb_launch_count(void);
+/* Event timing of every GEMM-engine launch between begin and end (on the
+ * launching stream): total device ms, total algorithmic flops, launches. */
+TB_API tb_status tb_profile_begin(void);
+TB_API tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launches);
 
 /*
  * GEMM: C = alpha * op(A) * op(B) + beta * C, op(A) m x k, op(B) k x n, all

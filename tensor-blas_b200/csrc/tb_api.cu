@@ -38,6 +38,7 @@ tb_status symmetrize_lower(long long n, float* A, long long lda, cudaStream_t st
   dim3 grid((unsigned)nt, (unsigned)nt);
   symmetrize_kernel<<<grid, 256, 0, st>>>(n, A, lda);
   TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
   return TB_SUCCESS;
 }
 

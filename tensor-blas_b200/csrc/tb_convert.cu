@@ -102,6 +102,7 @@ tb_status convert_f32_f16(long long rows, long long cols, const float* src, long
   else
     convert1_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri);
   TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
   return TB_SUCCESS;
 }
 

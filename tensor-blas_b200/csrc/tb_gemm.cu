@@ -68,7 +68,7 @@ tb_status make_map(CUtensorMap* map, const Operand& op, int box_rows) {
 }
 
 template <class Cfg>
-tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream) {
+tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -77,8 +77,11 @@ tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t strea
     attr_set[dev] = true;
   }
   int grid = num_tiles < sm_count() ? num_tiles : sm_count();
+  void* tok = prof_begin(stream);
   gemm_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(args);
   TB_CUDA_TRY(cudaGetLastError());
+  prof_end(tok, stream, flops);
+  note_launch();
   return TB_SUCCESS;
 }
 
@@ -125,15 +128,15 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
 
   const bool amn = c.a_hi.mn_major, bmn = c.b_hi.mn_major;
   if (!split) {
-    if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>>(a, c.num_tiles, stream);
-    if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>>(a, c.num_tiles, stream);
-    if (!amn && !bmn) return launch_variant<GemmCfg<256, 1, false, false>>(a, c.num_tiles, stream);
-    return launch_variant<GemmCfg<256, 1, false, true>>(a, c.num_tiles, stream);
+    if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>>(a, c.num_tiles, stream, c.flops);
+    if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>>(a, c.num_tiles, stream, c.flops);
+    if (!amn && !bmn) return launch_variant<GemmCfg<256, 1, false, false>>(a, c.num_tiles, stream, c.flops);
+    return launch_variant<GemmCfg<256, 1, false, true>>(a, c.num_tiles, stream, c.flops);
   } else {
-    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true>>(a, c.num_tiles, stream);
-    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false>>(a, c.num_tiles, stream);
-    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>>(a, c.num_tiles, stream);
-    return launch_variant<GemmCfg<128, 3, false, true>>(a, c.num_tiles, stream);
+    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true>>(a, c.num_tiles, stream, c.flops);
+    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false>>(a, c.num_tiles, stream, c.flops);
+    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>>(a, c.num_tiles, stream, c.flops);
+    return launch_variant<GemmCfg<128, 3, false, true>>(a, c.num_tiles, stream, c.flops);
   }
 }
 

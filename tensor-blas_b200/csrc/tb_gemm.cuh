@@ -101,20 +101,38 @@ __device__ __forceinline__ uint64_t operand_desc(uint32_t base, int kk) {
 
 // alpha/beta update of 32 consecutive columns of one row of C, with the
 // lower-triangle mask, bounds and the optional fused fp16 hi/lo copies.
+// With beta != 0 the 32 old values are loaded before any store so the loads
+// are in flight together (stores to C could otherwise alias them).
 __device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const float* v, long long gi, long long gj0) {
+  float* crow = args.C + gi + gj0 * args.ldc;
+  bool keep[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    const bool keep = gj < args.N && !(args.tri && (gi - gj) < args.diag);
-    if (!keep) continue;
-    float* cp = args.C + gi + gj * args.ldc;
-    float r = args.alpha * v[j];
-    if (args.beta != 0.0f) r = fmaf(args.beta, *cp, r);
-    *cp = r;
-    if (args.out_hi) {
-      const __half h = __float2half_rn(r);
-      args.out_hi[gi + gj * args.ld_out] = h;
-      if (args.out_lo) args.out_lo[gi + gj * args.ld_out] = __float2half_rn((r - __half2float(h)) * args.out_lo_scale);
+    keep[j] = gj < args.N && !(args.tri && (gi - gj) < args.diag);
+  }
+  float r[32];
+  if (args.beta != 0.0f) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) r[j] = keep[j] ? __ldg(crow + (long long)j * args.ldc) : 0.f;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) r[j] = fmaf(args.beta, r[j], args.alpha * v[j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) r[j] = args.alpha * v[j];
+  }
+#pragma unroll
+  for (int j = 0; j < 32; ++j)
+    if (keep[j]) crow[(long long)j * args.ldc] = r[j];
+  if (args.out_hi) {
+    __half* hrow = args.out_hi + gi + gj0 * args.ld_out;
+    __half* lrow = args.out_lo ? args.out_lo + gi + gj0 * args.ld_out : nullptr;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (!keep[j]) continue;
+      const __half h = __float2half_rn(r[j]);
+      hrow[(long long)j * args.ld_out] = h;
+      if (lrow) lrow[(long long)j * args.ld_out] = __float2half_rn((r[j] - __half2float(h)) * args.out_lo_scale);
     }
   }
 }

@@ -57,6 +57,7 @@ tb_status gemm_impl(bool ta, bool tb_, long m, long n, long k, float alpha, cons
   c.N = (int)n;
   c.alpha = alpha;
   c.beta = beta;
+  c.flops = 2.0 * m * n * k;
   return gemm_launch(c, st);
 }
 

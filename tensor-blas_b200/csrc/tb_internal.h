@@ -36,6 +36,12 @@ int* device_error_word();
 // Reads and clears the device error word (synchronises `stream`).
 tb_status check_device_error(cudaStream_t stream);
 int sm_count();
+// Counts kernel launches issued by the library (tb_launch_count).
+void note_launch(int n = 1);
+// Event timing of GEMM-engine launches between tb_profile_begin/end.
+bool profiling();
+void* prof_begin(cudaStream_t st);
+void prof_end(void* token, cudaStream_t st, double flops);
 
 inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
@@ -70,6 +76,7 @@ struct GemmCall {
   __half* out_lo = nullptr;
   long long ld_out = 0;
   float out_lo_scale = 2048.0f;
+  double flops = 0;  // algorithmic flops of this launch (profiling only)
 };
 
 // Tile width along N used by the engine for a given split mode.

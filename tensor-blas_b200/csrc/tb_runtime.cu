@@ -1,10 +1,12 @@
 // Library runtime: status strings, per-thread error text, the current stream,
 // the per-device scratch pool and the device error word used by the bounded
 // waits of the persistent kernels.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "tb_internal.h"
 
@@ -30,6 +32,50 @@ DeviceState* state() {
   return &g_dev[d];
 }
 }  // namespace
+
+// ------------------------------------------------------------------ accounting
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+struct ProfRec {
+  cudaEvent_t a, b;
+  double flops;
+};
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof_live;     // recorded since tb_profile_begin
+std::vector<cudaEvent_t> g_ev_free;  // recycled events
+cudaEvent_t ev_get() {
+  if (!g_ev_free.empty()) {
+    cudaEvent_t e = g_ev_free.back();
+    g_ev_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+void note_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+
+bool profiling() { return g_prof_on; }
+
+void* prof_begin(cudaStream_t st) {
+  if (!g_prof_on) return nullptr;
+  ProfRec r;
+  r.a = ev_get();
+  r.b = ev_get();
+  r.flops = 0;
+  cudaEventRecord(r.a, st);
+  g_prof_live.push_back(r);
+  return reinterpret_cast<void*>(g_prof_live.size());
+}
+
+void prof_end(void* token, cudaStream_t st, double flops) {
+  if (!token) return;
+  ProfRec& r = g_prof_live[reinterpret_cast<size_t>(token) - 1];
+  cudaEventRecord(r.b, st);
+  r.flops = flops;
+}
 
 void set_last_error(const char* fmt, ...) {
   va_list ap;
@@ -136,5 +182,36 @@ const char* tb_last_error(void) { return tb::g_last_error; }
 tb_status tb_synchronize(void) { return tb::check_device_error(tb::g_stream); }
 
 int tb_version(void) { return 100; }
+
+unsigned long long tb_launch_count(void) { return tb::g_launches.load(); }
+
+tb_status tb_profile_begin(void) {
+  tb::g_prof_live.clear();
+  tb::g_prof_on = true;
+  return TB_SUCCESS;
+}
+
+tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launches) {
+  tb::g_prof_on = false;
+  double ms = 0, fl = 0;
+  long cnt = 0;
+  tb_status st = TB_SUCCESS;
+  for (auto& r : tb::g_prof_live) {
+    if (cudaEventSynchronize(r.b) != cudaSuccess) st = TB_ERROR_CUDA;
+    float t = 0;
+    if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+      ms += t;
+      fl += r.flops;
+      ++cnt;
+    }
+    tb::g_ev_free.push_back(r.a);
+    tb::g_ev_free.push_back(r.b);
+  }
+  tb::g_prof_live.clear();
+  if (gemm_ms) *gemm_ms = ms;
+  if (gemm_flops) *gemm_flops = fl;
+  if (gemm_launches) *gemm_launches = cnt;
+  return st;
+}
 
 }  // extern "C"

@@ -35,6 +35,7 @@ tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, lon
     dim3 g((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)(n < 65535 ? n : 65535));
     scale_lower_kernel<<<g, 256, 0, st>>>(n, beta, C, ldc);
     TB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     return TB_SUCCESS;
   }
   const bool hilo = split == Split::kHiLo;
@@ -78,6 +79,7 @@ tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, lon
   c.beta = beta;
   c.tri = 1;
   c.diag = 0;
+  c.flops = (double)n * (double)(n + 1) * (double)k;  // lower triangle incl. diagonal, 2 flops per MAC
   return gemm_launch(c, st);
 }
 

@@ -203,6 +203,7 @@ tb_status leaf_solve(TrsmCtx& c, int bidx, long s, long e) {
   }
   g.alpha = 1.f;
   g.beta = 0.f;
+  g.flops = (double)g.M * g.N * nbl;  // triangular solve of the leaf: other * nbl^2 flops
   const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split), 0, (int)((nbl + kGemmBK - 1) / kGemmBK));
   g.tiles = upload_tiles(plan, c.st);
   if (!g.tiles) return TB_ERROR_ALLOC;
@@ -242,6 +243,7 @@ tb_status update(TrsmCtx& c, long s, long mid, long e) {
   g.ldc = c.ldb;
   g.alpha = -1.f;
   g.beta = 1.f;
+  g.flops = 2.0 * g.M * g.N * kk;
   const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split), 0, (int)((kk + kGemmBK - 1) / kGemmBK));
   g.tiles = upload_tiles(plan, c.st);
   if (!g.tiles) return TB_ERROR_ALLOC;
@@ -338,6 +340,7 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   const long nsub = (nt + 31) / 32;
   diag_inv32_kernel<<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D);
   TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
   const int max_chain = (int)(leaf / 32);
   const size_t smem = (size_t)max_chain * 1024 * sizeof(double);
   static bool attr_done[64] = {false};
@@ -351,6 +354,7 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   dim3 grid((unsigned)max_chain, (unsigned)nleaf);
   trtri_chain_kernel<<<grid, 256, smem, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride);
   TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
   // 3. recursion
   return recurse(c, 0, nt, leaf_start);
 }

@@ -1,0 +1,140 @@
+"""CPU tests: pin the oracle (tb_oracle) against the reference library's own
+outputs recorded in tests/golden/ (planner: util/mat_size.cu; SYRK/TRSM:
+BLAS/tc_syrk.cu, BLAS/tc_trsm.cu run on a B200 by make_golden.py)."""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import tb_oracle as orc
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+sys.path.insert(0, GOLD)
+import golden_inputs as gi  # noqa: E402
+
+ROOT = os.path.dirname(HERE)
+
+
+def load(name):
+    z = np.load(os.path.join(GOLD, f"ref_{name}.npz"))
+    return z, json.loads(str(z["meta"]))
+
+
+# ------------------------------------------------------------------ planner
+def test_planner_matches_reference_golden():
+    d = json.load(open(os.path.join(GOLD, "ref_planner.json")))
+    for kind in ("syrk", "trsm"):
+        for n, rec in d[kind].items():
+            chunks = orc.find_mat_size(int(n), kind)
+            assert chunks == rec["chunks"], (kind, n)
+            assert len(chunks) - 1 == rec["length"]
+
+
+def test_planner_matches_reference_library_live():
+    so = os.path.join(ROOT, "oracle", "_ref", "libref_matsize.so")
+    if not os.path.exists(so):
+        pytest.skip("reference planner library not built (make -C oracle)")
+    import ctypes
+
+    lib = ctypes.CDLL(so)
+    g = gi.rng(77)
+    for kind in ("syrk", "trsm"):
+        fn = getattr(lib, f"_Z18find_mat_size_{kind}lPi")
+        fn.restype = ctypes.POINTER(ctypes.c_int64)
+        fn.argtypes = [ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]
+        for n in list(g.integers(1, 150000, 300)) + [2048 * i for i in range(1, 40)]:
+            ln = ctypes.c_int(0)
+            p = fn(int(n), ctypes.byref(ln))
+            got = []
+            while p[len(got)] != -1:
+                got.append(int(p[len(got)]))
+            assert got == orc.find_mat_size(int(n), kind), (kind, n)
+
+
+# ------------------------------------------------------------------ SYRK
+def _syrk_inputs(meta):
+    A = gi.uniform(meta["seed"], (meta["n"], meta["k"]))
+    assert abs(gi.checksum(A) - meta["a_sum"]) <= 1e-6 * max(1.0, abs(meta["a_sum"]))
+    C0 = gi.uniform(meta["seed"] + 1, (meta["n"], meta["n"])) if meta["beta"] != 0 else None
+    return A, C0
+
+
+@pytest.mark.parametrize("name", ["syrk_small", "syrk_beta"])
+def test_syrk_model_vs_reference(name):
+    z, meta = load(name)
+    A, C0 = _syrk_inputs(meta)
+    n, k = meta["n"], meta["k"]
+    model = orc.syrk_model(A, meta["alpha"], meta["beta"], C0)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    ref = z["C"].astype(np.float64)
+    _, nrm = orc.rel_errors(ref, model, low)
+    A64 = np.abs(A.astype(np.float64))
+    bound = (2e-6 + 2e-8 * k) * (abs(meta["alpha"]) * (A64 @ A64.T) + (0 if C0 is None else abs(meta["beta"]) * np.abs(C0)))
+    assert np.all(np.abs(ref - model)[low] <= bound[low] + 1e-30)
+    assert nrm <= 1e-6 + 1e-8 * k, nrm
+
+
+def test_syrk_model_vs_reference_recursive_path():
+    """n = 8192 takes the reference's tc_syrk_p2 level-batched path."""
+    z, meta = load("syrk_p2")
+    A, _ = _syrk_inputs(meta)
+    h = orc.h(A)
+    r, c = z["rows"], z["cols"]
+    model = np.einsum("ij,ij->i", h[r], h[c])
+    ref = z["vals"].astype(np.float64)
+    scale = np.einsum("ij,ij->i", np.abs(h[r]), np.abs(h[c]))
+    assert np.all(np.abs(ref - model) <= (2e-6 + 2e-8 * meta["k"]) * scale + 1e-30)
+    # row sums of the lower triangle: rowsum_i = h_i . sum_{j<=i} h_j
+    pref = np.cumsum(h, axis=0)
+    rs = np.einsum("ij,ij->i", h, pref)
+    _, nrm = orc.rel_errors(z["rowsum"], rs)
+    assert nrm <= 1e-5
+
+
+def test_planted_truncation_is_detected():
+    """An oracle that converted FP32->FP16 by truncation instead of
+    round-to-nearest must disagree with the reference far beyond tolerance."""
+    z, meta = load("syrk_small")
+    A, _ = _syrk_inputs(meta)
+    n = meta["n"]
+    low = np.tril(np.ones((n, n), dtype=bool))
+    ref = z["C"].astype(np.float64)
+
+    def h_trunc(x):
+        x16 = x.astype(np.float16)
+        back = x16.astype(np.float32)
+        over = np.abs(back) > np.abs(x)  # rounded away from zero -> step back one ulp
+        x16 = np.where(over, np.nextafter(x16, np.float16(0)), x16)
+        return x16.astype(np.float64)
+
+    ht = h_trunc(A)
+    _, e_trunc = orc.rel_errors(ref, np.where(low, ht @ ht.T, 0), low)
+    _, e_rn = orc.rel_errors(ref, orc.syrk_model(A), low)
+    assert e_trunc > 20 * e_rn
+
+
+# ------------------------------------------------------------------ TRSM
+@pytest.mark.parametrize("name", ["trsm_p2", "trsm_small", "trsm_p2_nb512"])
+def test_trsm_model_vs_reference(name):
+    z, meta = load(name)
+    m, n, nb = meta["m"], meta["n"], meta["nb"]
+    A = gi.lower_tri(meta["seed"], n).astype(np.float64)
+    B = gi.uniform(meta["seed"] + 1, (m, n))
+    # the reference recurses only on chunks with n % 2048 == 0 (BLAS/tc_trsm.cu:99-112)
+    leaf = nb if n % 2048 == 0 else n
+    model = orc.trsm_right_model(A, B, leaf)
+    ref = z["X"].astype(np.float64)
+    _, nrm = orc.rel_errors(ref, model)
+    exact = np.linalg.solve(A, B.astype(np.float64).T).T
+    _, nrm_exact = orc.rel_errors(ref, exact)
+    print(f"{name}: ref vs model {nrm:.3e}, ref vs FP64 solve {nrm_exact:.3e}")
+    # FP16 rounding of X inside the recursion amplifies the reference's own
+    # FP32 error a little (values near an FP16 rounding boundary flip), hence
+    # 2e-5; the model must still explain the reference far better than the
+    # exact FP64 solution does.
+    assert nrm <= 2e-5
+    if leaf != n:
+        assert nrm < 0.2 * nrm_exact
