@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Benchmark of the TensorBLAS hot path on B200 (one JSON line on rank 0).
+
+Step = one plain SYRK (lower, C = A A^T, n = k = 16384, nb = 256, A i.i.d.
+U[-1,1]) + one plain TRSM (left/lower/no-trans/non-unit, m = n = 16384,
+nb = 512, A off-diagonal U[-1,1]/sqrt(n), diagonal U[1,2], B U[-1,1]).
+Metric: effective TFLOP/s = (n^2 k + m^2 n) / device time (reference flop
+conventions, testing/testing_syrk.cu:100 and testing_trsm.cu:61). The chosen
+(split, FP32-accurate) form is timed the same way and reported beside it,
+each with its error against an FP64 evaluation on the host.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+N > 1 runs independent replicas, one per GPU (the path has no exchange step);
+value = all ranks' flops / max-over-ranks device time.
+"""
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tensor-blas_b200", "python"))
+METRIC = "SYRK/TRSM n=16384 eff. TFLOP/s at stated FP64-oracle error, chosen vs plain"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    p.add_argument("--n", type=int, default=16384)
+    p.add_argument("--nb-syrk", type=int, default=256)
+    p.add_argument("--nb-trsm", type=int, default=512)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ process / ranks
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def physical_gpu(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local < len(ids) and ids[local].isdigit():
+            return int(ids[local])
+    return local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d.get("bf16_tflops"), d.get("bf16_tflops_sustained"), "measured"
+    except (OSError, ValueError):
+        return 1590.0, 1400.0, "fallback"
+
+
+def traffic_summary():
+    """Per-launch DRAM bytes of the GEMM engine from a committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "gemm_engine_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------------ inputs
+def make_inputs(n, seed=1234):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    A = torch.rand(n, n, device="cuda", generator=g) * 2 - 1            # SYRK A (column-major storage)
+    L = torch.rand(n, n, device="cuda", generator=g) * 2 - 1
+    L = torch.tril(L, -1) / n ** 0.5 + torch.diag(torch.rand(n, device="cuda", generator=g) + 1)
+    T = L.t().contiguous()                                             # column-major lower triangle
+    del L
+    B0 = torch.rand(n, n, device="cuda", generator=g) * 2 - 1           # column-major B
+    return A, T, B0
+
+
+# ------------------------------------------------------------------ error vs FP64 (sampled)
+def fp64_errors(n, A, C, T, B0, X, seed=7):
+    """Sampled errors against FP64 evaluation on the host.
+
+    SYRK: 4096 random lower entries C_ij = sum_p a_ip a_jp in FP64.
+    TRSM: 32 random columns x_j = A^{-1} b_j by FP64 forward substitution.
+    Returns max elementwise relative and normwise relative error of each.
+    """
+    from scipy.linalg import solve_triangular
+
+    g = np.random.Generator(np.random.PCG64(seed))
+    # element (i, p) of the column-major n x k matrix A is Ah[p, i]
+    Ah = A.cpu().numpy().astype(np.float64)
+    i = g.integers(0, n, 4096)
+    j = g.integers(0, n, 4096)
+    lo, hi = np.maximum(i, j), np.minimum(i, j)
+    ref = np.einsum("pk,pk->k", Ah[:, lo], Ah[:, hi])
+    Cs = C.cpu().numpy()
+    got = Cs[hi, lo].astype(np.float64)              # element (lo, hi) of column-major C at storage [hi, lo]
+    d = np.abs(got - ref)
+    syrk = {"max_rel": float(np.max(d / np.maximum(np.abs(ref), 1e-300))),
+            "norm_rel": float(np.linalg.norm(d) / np.linalg.norm(ref)), "sample": "4096 entries"}
+    cols = g.integers(0, n, 32)
+    Lh = T.cpu().numpy().T.astype(np.float64)        # logical lower-triangular A
+    Bh = B0.cpu().numpy().T.astype(np.float64)       # logical B (m x n)
+    Xh = X.cpu().numpy().T.astype(np.float64)
+    xr = solve_triangular(Lh, Bh[:, cols], lower=True)
+    dx = np.abs(Xh[:, cols] - xr)
+    trsm = {"max_rel": float(np.max(dx / np.maximum(np.abs(xr), 1e-300))),
+            "norm_rel": float(np.linalg.norm(dx) / np.linalg.norm(xr)), "sample": "32 columns"}
+    return {"syrk": syrk, "trsm": trsm}
+
+
+# ------------------------------------------------------------------ arms
+def run_mine(args, world, rank, local):
+    import TensorBLAS as TB
+
+    n = args.n
+    flops_step = 2.0 * float(n) ** 3
+    A, T, B0 = make_inputs(n)
+    C = torch.zeros(n, n, device="cuda")
+    Bw = torch.empty_like(B0)
+    stream = torch.cuda.current_stream()
+
+    def step(prec):
+        TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, prec)
+        TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, prec)
+
+    def timed(prec, steps, warmup, profile=False, clocks=None):
+        for _ in range(warmup):
+            Bw.copy_(B0)
+            step(prec)
+        TB.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        sampler = Clocks(physical_gpu(local)) if clocks else None
+        l0 = TB.lib.tb_launch_count()
+        if profile:
+            TB.lib.tb_profile_begin()
+        for e0, e1 in evs:
+            Bw.copy_(B0)                     # restore B (TRSM overwrites it); outside the event window
+            e0.record(stream)
+            step(prec)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        launches = TB.lib.tb_launch_count() - l0
+        prof = None
+        if profile:
+            ms, fl, cnt = TB.ctypes.c_double(), TB.ctypes.c_double(), TB.ctypes.c_long()
+            TB.lib.tb_profile_end(TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
+            prof = (ms.value, fl.value, cnt.value)
+        clk = sampler.stop() if sampler else None
+        barrier(world)
+        TB.synchronize()
+        ms_total = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+        return ms_total, launches, prof, clk
+
+
+    # ---- plain (headline)
+    ms_plain, launches, prof, clk = timed(TB.PLAIN, args.steps, args.warmup, profile=True, clocks=True)
+    ms_plain = max_over_ranks(ms_plain, world)
+    Bw.copy_(B0)
+    step(TB.PLAIN)
+    TB.synchronize()
+    err_plain = fp64_errors(n, A, C, T, B0, Bw) if rank == 0 else None
+    # ---- chosen (split)
+    ms_split, _, _, _ = timed(TB.SPLIT, args.steps, args.warmup)
+    ms_split = max_over_ranks(ms_split, world)
+    Bw.copy_(B0)
+    step(TB.SPLIT)
+    TB.synchronize()
+    err_split = fp64_errors(n, A, C, T, B0, Bw) if rank == 0 else None
+
+    value = world * args.steps * flops_step / (ms_plain * 1e-3) / 1e12
+    value_split = world * args.steps * flops_step / (ms_split * 1e-3) / 1e12
+
+    # ---- end to end through the public API with pinned host buffers
+    pin = lambda t: t.cpu().pin_memory()  # noqa: E731
+    hA, hT, hB = pin(A), pin(T), pin(B0)
+    hC = torch.empty(n, n, dtype=torch.float32).pin_memory()
+    hX = torch.empty(n, n, dtype=torch.float32).pin_memory()
+    dA, dT, dB, dC = torch.empty_like(A), torch.empty_like(T), torch.empty_like(B0), torch.zeros_like(C)
+
+    def e2e_step():
+        dA.copy_(hA, non_blocking=True)
+        dT.copy_(hT, non_blocking=True)
+        dB.copy_(hB, non_blocking=True)
+        TB.ssyrk(dA, dC, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN)
+        TB.strsm("L", dT, dB, n, n, n, n, args.nb_trsm, TB.PLAIN)
+        hC.copy_(dC, non_blocking=True)
+        hX.copy_(dB, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), world)
+    barrier(world)
+    e2e_value = world * args.e2e_steps * flops_step / (ms_e2e * 1e-3) / 1e12
+
+    if rank != 0:
+        return None
+    burst, sustained, peak_src = measured_peaks()
+    gemm_ms, gemm_flops, gemm_launches = prof
+    achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
+    tr = traffic_summary()
+    roof = {"bound": "tensor", "kernel": "tb::gemm_kernel (all GEMM-engine launches of the step)",
+            "achieved": achieved, "peak": sustained, "unit": "TFLOP/s",
+            "frac": (achieved / sustained) if achieved and sustained else None,
+            "peak_source": f"{peak_src} bf16_tflops_sustained (burst {burst})",
+            "launches_per_step": gemm_launches / args.steps,
+            "traffic": tr.get("bytes_per_launch") if tr else None,
+            "traffic_note": tr.get("note") if tr else "no ncu traffic summary committed"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_plain / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16 operands, f32 accumulate", "data": "synthetic (seeded)",
+        "config": {"workload": f"plain SYRK n=k={n} nb={args.nb_syrk} + plain TRSM left/lower/N m=n={n} "
+                               f"nb={args.nb_trsm} per step", "n": n, "precision": "plain",
+                   "l2": "inputs larger than L2 (1 GiB per matrix)", "parallelism": f"replicas x{world}"},
+        "errors_vs_fp64": err_plain,
+        "chosen": {"precision": "split (FP16 hi + scaled lo, 3 products, RN folds)", "value": value_split,
+                   "ms_per_step": ms_split / args.steps, "ratio_vs_plain": value_split / value,
+                   "errors_vs_fp64": err_split},
+        "e2e": {"value": e2e_value, "unit": "TFLOP/s", "steps": args.e2e_steps,
+                "h2d_bytes_per_step": 3 * n * n * 4, "d2h_bytes_per_step": 2 * n * n * 4,
+                "api": "TensorBLAS.ssyrk / TensorBLAS.strsm on pinned-host-staged buffers"},
+        "roofline": roof,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import tb_cpu
+
+        nc = 4096
+        fl, reps, el = tb_cpu.time_step(nc, min_seconds=10.0)
+        line["cpu_baseline"] = {"value": fl / 1e12, "unit": "TFLOP/s", "cores": tb_cpu.threads(), "kind": "port",
+                                "sample": f"{reps} x (SYRK n=k={nc} + TRSM m=n={nc}, FP16-rounded operands, "
+                                          f"FP32 OpenBLAS) in {el:.1f} s"}
+    return line
+
+
+def run_reference(args, world, rank, local):
+    """The reference library (built from its sources into oracle/_ref/) on this B200."""
+    if rank != 0:
+        return None
+    import ctypes
+
+    so = os.path.join(ROOT, "oracle", "_ref", "libTensorBLAS_ref.so")
+    if not os.path.exists(so):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libTensorBLAS_ref.so not built (make -C oracle)"}
+    lib = ctypes.CDLL(so)
+    P = ctypes.c_void_p
+    lib.ref_time_syrk.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, P, ctypes.c_int, ctypes.c_int]
+    lib.ref_time_syrk.restype = ctypes.c_double
+    lib.ref_time_trsm.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, P, P, ctypes.c_int, ctypes.c_int]
+    lib.ref_time_trsm.restype = ctypes.c_double
+    n = args.n
+    A, T, B0 = make_inputs(n)
+    hA = A.cpu().numpy()
+    hT = T.cpu().numpy()                            # column-major lower-triangular A, as tc_trsm takes it
+    hB = B0.cpu().numpy()
+    del A, T, B0
+    torch.cuda.empty_cache()
+    sampler = Clocks(physical_gpu(local))
+    t_syrk = lib.ref_time_syrk(n, n, args.nb_syrk, hA.ctypes.data_as(P), args.warmup, args.steps)
+    t_trsm = lib.ref_time_trsm(n, n, args.nb_trsm, hT.ctypes.data_as(P), hB.ctypes.data_as(P), args.warmup,
+                               args.steps)
+    clk = sampler.stop()
+    if t_syrk <= 0 or t_trsm <= 0:
+        return {"impl": "reference", "unavailable": "reference routine failed on this device"}
+    ms = t_syrk + t_trsm
+    value = 2.0 * float(n) ** 3 / (ms * 1e-3) / 1e12
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f16 operands, f32 accumulate (cuBLAS GemmEx) + f32 cublasStrsm leaves", "data": "synthetic (seeded)",
+        "config": {"workload": f"reference tc_syrk n=k={n} nb={args.nb_syrk} + tc_trsm m=n={n} nb={args.nb_trsm} "
+                               "(its right-side form X A^T = B: same shape and flops) per step", "n": n,
+                   "precision": "plain", "l2": "inputs larger than L2", "parallelism": "replicas x1"},
+        "detail": {"syrk_ms": t_syrk, "trsm_ms": t_trsm, "timing": "median per call, CUDA events, device-resident"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": 1, "kind": "reference",
+                         "sample": "the reference library itself (oracle/_ref, built from its sources for sm_100a; "
+                                   "its path is GPU code on cuBLAS) timed on this B200"},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk,
+    }
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        line = run_mine(args, world, rank, local) if args.impl == "mine" else run_reference(args, world, rank, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -66,77 +66,104 @@ __global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const float
 
 // Column chain j of the inverse of leaf block b (rows/cols [s, s+size)):
 //   W[i][j] = -Dinv_i * sum_{p=j}^{i-1} L[i][p] W[p][j]   (32x32 sub-blocks)
-// The 32-wide column panel of W lives in shared memory (FP64); each 32x32
-// sub-block of L and each Dinv_i is staged through shared memory with
-// coalesced loads before use. The result is written as the FP16 hi/lo pair
-// (lo scaled by 2^11) of W, column-major with leading dimension ldw, zeros
-// above the diagonal.
-__global__ void __launch_bounds__(256) trtri_chain_kernel(const float* __restrict__ A, long long lda,
-                                                          const int2* __restrict__ leaves, const double* __restrict__ D,
-                                                          __half* __restrict__ Whi, __half* __restrict__ Wlo,
-                                                          long long ldw, long long wstride) {
-  extern __shared__ double sm[];
-  __shared__ double Ls[32][33];  // staged L sub-block (or Dinv_i)
-  __shared__ double Ts[32][33];
+// The 32-wide column panel of W lives in shared memory (FP64). Each 32x32
+// sub-block of L and each Dinv_i is staged (transposed) through shared memory
+// with coalesced loads; each of the 128 threads owns a 2 x 4 block of the
+// 32x32 result so every shared-memory load feeds several FMAs. The result is
+// written as the FP16 hi/lo pair (lo scaled by 2^11) of W, column-major with
+// leading dimension ldw, zeros above the diagonal.
+constexpr int kChainThreads = 128;
+
+__global__ void __launch_bounds__(kChainThreads) trtri_chain_kernel(const float* __restrict__ A, long long lda,
+                                                                    const int2* __restrict__ leaves,
+                                                                    const double* __restrict__ D,
+                                                                    __half* __restrict__ Whi, __half* __restrict__ Wlo,
+                                                                    long long ldw, long long wstride) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ __align__(16) double LsT[32][34];  // LsT[k][r] = L(r, k) of the staged sub-block (or Dinv_i)
+  __shared__ __align__(16) double Ts[32][36];   // Ts[k][c]
   const int2 leaf = leaves[blockIdx.y];  // {s, size}
   const int s = leaf.x, size = leaf.y;
   const int nsub = (size + 31) / 32;
   const int j = blockIdx.x;
   if (j >= nsub) return;
-  double* Wp = sm;  // [(nsub - j) * 32][32]: row (within panel) major
+  double* Wp = sm;  // [(nsub - j) * 32][32]: Wp[row * 32 + col], row relative to 32j
   const int tid = threadIdx.x;
-  const int r = tid & 31, cq = tid >> 5;     // compute role: row r, columns cq + 8q
-  const long long sub0 = (long long)s / 32;  // global 32-sub-block index of the leaf's first sub-block
-  for (int q = 0; q < 4; ++q) {
-    const int c = cq + 8 * q;
-    Wp[r * 32 + c] = D[(sub0 + j) * 1024 + r + 32 * c];
+  const int r0 = 2 * (tid & 15), c0 = 4 * (tid >> 4);  // 2 x 4 output block
+  const int lr = tid & 31, lc = tid >> 5;              // load role: row lr, columns lc + 4q
+  const long long sub0 = (long long)s / 32;
+  for (int q = 0; q < 8; ++q) {
+    const int c = lc + 4 * q;
+    Wp[lr * 32 + c] = D[(sub0 + j) * 1024 + lr + 32 * c];
   }
   __syncthreads();
   for (int i = j + 1; i < nsub; ++i) {
-    double acc[4] = {0, 0, 0, 0};
+    double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
     for (int p = j; p < i; ++p) {
-      // stage L(32i + rr, 32p + cc): thread loads rows rr = tid&31 of columns cc = tid>>5 + 8q
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int cc = cq + 8 * q;
-        const int gr = 32 * i + r, gc = 32 * p + cc;
-        Ls[r][cc] = (gr < size && gc < size) ? (double)A[(long long)s + gr + ((long long)s + gc) * lda] : 0.0;
+      for (int q = 0; q < 8; ++q) {
+        const int cc = lc + 4 * q;
+        const int gr = 32 * i + lr, gc = 32 * p + cc;
+        LsT[cc][lr] = (gr < size && gc < size) ? (double)A[(long long)s + gr + ((long long)s + gc) * lda] : 0.0;
       }
       __syncthreads();
       const double* wrow = Wp + (32 * (p - j)) * 32;
-#pragma unroll 8
+#pragma unroll 4
       for (int kk = 0; kk < 32; ++kk) {
-        const double l = Ls[r][kk];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = fma(l, wrow[kk * 32 + cq + 8 * q], acc[q]);
+        const double2 l = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
+        const double2 w01 = *reinterpret_cast<const double2*>(wrow + kk * 32 + c0);
+        const double2 w23 = *reinterpret_cast<const double2*>(wrow + kk * 32 + c0 + 2);
+        acc[0][0] = fma(l.x, w01.x, acc[0][0]);
+        acc[0][1] = fma(l.x, w01.y, acc[0][1]);
+        acc[0][2] = fma(l.x, w23.x, acc[0][2]);
+        acc[0][3] = fma(l.x, w23.y, acc[0][3]);
+        acc[1][0] = fma(l.y, w01.x, acc[1][0]);
+        acc[1][1] = fma(l.y, w01.y, acc[1][1]);
+        acc[1][2] = fma(l.y, w23.x, acc[1][2]);
+        acc[1][3] = fma(l.y, w23.y, acc[1][3]);
       }
       __syncthreads();
     }
+    // T -> shared; Dinv_i -> LsT (transposed: LsT[k][r] = Dinv_i(r, k))
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      Ts[r][cq + 8 * q] = acc[q];
-      Ls[r][cq + 8 * q] = D[(sub0 + i) * 1024 + r + 32 * (cq + 8 * q)];  // Dinv_i(r, c)
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Ts[r0 + a][c0 + b] = acc[a][b];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int cc = lc + 4 * q;
+      LsT[cc][lr] = D[(sub0 + i) * 1024 + lr + 32 * cc];
     }
     __syncthreads();
-    double o[4] = {0, 0, 0, 0};
-#pragma unroll 8
+    double o[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll 4
     for (int kk = 0; kk < 32; ++kk) {
-      const double dv = Ls[r][kk];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) o[q] = fma(-dv, Ts[kk][cq + 8 * q], o[q]);
+      const double2 d = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
+      const double2 t01 = *reinterpret_cast<const double2*>(&Ts[kk][c0]);
+      const double2 t23 = *reinterpret_cast<const double2*>(&Ts[kk][c0 + 2]);
+      o[0][0] = fma(-d.x, t01.x, o[0][0]);
+      o[0][1] = fma(-d.x, t01.y, o[0][1]);
+      o[0][2] = fma(-d.x, t23.x, o[0][2]);
+      o[0][3] = fma(-d.x, t23.y, o[0][3]);
+      o[1][0] = fma(-d.y, t01.x, o[1][0]);
+      o[1][1] = fma(-d.y, t01.y, o[1][1]);
+      o[1][2] = fma(-d.y, t23.x, o[1][2]);
+      o[1][3] = fma(-d.y, t23.y, o[1][3]);
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) Wp[(32 * (i - j) + r) * 32 + cq + 8 * q] = o[q];
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Wp[(32 * (i - j) + r0 + a) * 32 + c0 + b] = o[a][b];
     __syncthreads();
   }
   // write the 32 columns [32j, 32j+32) of W for all rows of the leaf
   __half* hi = Whi + (long long)blockIdx.y * wstride;
   __half* lo = Wlo + (long long)blockIdx.y * wstride;
-  for (int q = 0; q < 4; ++q) {
-    const int c = cq + 8 * q;
+  for (int q = 0; q < 8; ++q) {
+    const int c = lc + 4 * q;
     const int gc = 32 * j + c;
     if (gc >= size) continue;
-    for (int row = r; row < size; row += 32) {
+    for (int row = lr; row < size; row += 32) {
       double v = 0.0;
       if (row >= 32 * j) v = Wp[(row - 32 * j) * 32 + c];
       const __half h = __float2half_rn((float)v);
@@ -352,7 +379,7 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
     attr_done[dev] = true;
   }
   dim3 grid((unsigned)max_chain, (unsigned)nleaf);
-  trtri_chain_kernel<<<grid, 256, smem, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride);
+  trtri_chain_kernel<<<grid, kChainThreads, smem, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   // 3. recursion

@@ -39,6 +39,13 @@ lib.tb_last_error.argtypes = []
 lib.tb_last_error.restype = ctypes.c_char_p
 lib.tb_status_string.argtypes = [ctypes.c_int]
 lib.tb_status_string.restype = ctypes.c_char_p
+lib.tb_launch_count.argtypes = []
+lib.tb_launch_count.restype = ctypes.c_ulonglong
+lib.tb_profile_begin.argtypes = []
+lib.tb_profile_begin.restype = ctypes.c_int
+lib.tb_profile_end.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_long)]
+lib.tb_profile_end.restype = ctypes.c_int
 lib.tb_sgemm.argtypes = [ctypes.c_char, ctypes.c_char, _c_long, _c_long, _c_long, ctypes.c_float, _fp, _c_long, _fp,
                          _c_long, ctypes.c_float, _fp, _c_long, ctypes.c_int]
 lib.tb_sgemm.restype = ctypes.c_int
