@@ -67,6 +67,20 @@ tb_status make_map(CUtensorMap* map, const Operand& op, int box_rows) {
   return TB_SUCCESS;
 }
 
+// Tensor map for the fp32 output C (rows x cols, column-major, ldc), box
+// {128 rows, 32 cols}, used by the TMA epilogue for loads and stores.
+bool make_c_map(CUtensorMap* map, float* C, long long rows, long long cols, long long ldc) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc || (reinterpret_cast<uintptr_t>(C) & 15) != 0 || (ldc * 4) % 16 != 0) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+  cuuint64_t strides[1] = {(cuuint64_t)ldc * 4};
+  cuuint32_t box[2] = {128, 32};
+  cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class Cfg>
 tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops) {
   static bool attr_set[64] = {false};
@@ -116,6 +130,7 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   a.diag = c.diag;
   a.corr_scale = c.corr_scale;
   a.kchunk = c.kchunk > 0 ? c.kchunk : 1;
+  a.tma_c = make_c_map(&a.mapC, c.C, c.M, c.N, c.ldc) ? 1 : 0;
   a.out_hi = c.out_hi;
   a.out_lo = c.out_lo;
   a.ld_out = c.ld_out;

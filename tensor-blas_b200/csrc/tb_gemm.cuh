@@ -10,13 +10,12 @@
 // Roles (192 threads, one CTA per SM):
 //   warp 0      TMA producer: 64-wide K slabs of A and B into a smem ring.
 //   warp 1      TMEM allocator + single-thread UMMA issuer.
-//   warps 2..5  epilogue: TMEM -> registers -> alpha/beta -> global fp32,
-//               optionally fused fp16 hi/lo copies of the result.
+//   warps 2..5  epilogue: TMEM -> registers -> alpha/beta -> C.
 // The fp32 accumulator is double-buffered in TMEM (2 x 256 columns) so the
 // epilogue of tile t overlaps the MMAs of tile t+1.
 //
-// Operands are fp16 (or bf16) in global memory, either MN-major (column-major
-// storage with the M/N index contiguous, the layout the reference's FP32->FP16
+// Operands are fp16 in global memory, either MN-major (column-major storage
+// with the M/N index contiguous, the layout the reference's FP32->FP16
 // conversion produces) or K-major. Both map onto 128B-swizzled UMMA canonical
 // layouts:
 //   MN-major: TMA box {64 (MN), 64 (K)} -> 8 KB atoms; LBO = 8 KB between
@@ -25,11 +24,21 @@
 //   K-major : TMA box {64 (K), R rows} -> R x 128 B; SBO = 1 KB between
 //             8-row groups; a K step of 16 advances the descriptor by 32 B.
 //
+// Output: each 128 x 32 chunk of the tile is staged in shared memory
+// (column-major, 512 B per column) and written with one TMA tensor store, so
+// HBM sees 512-byte runs instead of one 128-byte piece per warp and column.
+// When beta != 0, or when a tile crosses the lower-triangle mask, the chunk
+// of C is first brought in with a TMA load and combined in shared memory
+// (masked elements keep their old value). A plain per-element path remains
+// for C that TMA cannot address (unaligned base or leading dimension).
+//
 // Split ("3-product") mode holds hi and lo copies of both operands and runs
 //   acc0 += Ahi*Bhi ; acc1 += Ahi*Blo + Alo*Bhi
 // with the correction in its own TMEM accumulator (Ootomo & Yokota 2022,
-// the error-corrected FP16 scheme cuMpSGEMM's FP16TCEC mode uses);
-// epilogue: acc0 + corr_scale * acc1.
+// the error-corrected FP16 scheme cuMpSGEMM's FP16TCEC mode uses). Every
+// `kchunk` K-blocks the epilogue folds acc0 + corr_scale * acc1 into FP32
+// registers with round-to-nearest adds: the tensor core's own FP32
+// accumulation truncates, which would cost ~K/16 ulps.
 #pragma once
 #include "tb_ptx.cuh"
 
@@ -38,7 +47,8 @@ namespace tb {
 struct GemmArgs {
   CUtensorMap mapA[2];  // [0] hi, [1] lo (split mode only)
   CUtensorMap mapB[2];
-  const int4* tiles;  // {m0, n0, kb_begin, kb_end}; m0/n0 relative to C
+  CUtensorMap mapC;     // fp32 C, box {128, 32} (TMA epilogue only)
+  const int4* tiles;    // {m0, n0, kb_begin, kb_end}; m0/n0 relative to C
   int num_tiles;
   int a_off;  // row offset of the A operand in mapA's row coordinate
   int b_off;  // row offset of the B operand in mapB's row coordinate
@@ -50,7 +60,8 @@ struct GemmArgs {
   int tri;   // 1: write only (i - j) >= diag (lower triangle)
   int diag;
   float corr_scale;  // weight of the correction accumulator
-  int kchunk;        // split mode: K-blocks per TMEM accumulation chunk
+  int kchunk;        // split mode: K-blocks per round-to-nearest fold
+  int tma_c;         // 1: C through mapC (TMA epilogue)
   // Optional fused fp16 copies of the written result (column-major, ld_out):
   //   out_hi = fp16(v), out_lo = fp16((v - out_hi) * out_lo_scale)
   __half* out_hi;
@@ -74,8 +85,11 @@ struct GemmCfg {
   static constexpr int ACC_COLS = NACC * BN;  // TMEM columns per accumulation buffer
   static constexpr int TMEM_COLS = 2 * ACC_COLS;
   static_assert(TMEM_COLS <= 512, "TMEM budget");
+  static constexpr int EPI_CHUNK_BYTES = 128 * 32 * 4;  // one staged 128 x 32 fp32 chunk
+  static constexpr int EPI_BYTES = 2 * EPI_CHUNK_BYTES;
   static constexpr int BAR_BYTES = 256;
-  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + BAR_BYTES;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + BAR_BYTES;
+  static_assert(SMEM_BYTES <= 232448, "shared memory budget");
   static constexpr uint32_t IDESC = idesc_f16(BM, BN, false, A_MN, B_MN);
   static constexpr int THREADS = 192;
 };
@@ -99,10 +113,23 @@ __device__ __forceinline__ uint64_t operand_desc(uint32_t base, int kk) {
   }
 }
 
-// alpha/beta update of 32 consecutive columns of one row of C, with the
-// lower-triangle mask, bounds and the optional fused fp16 hi/lo copies.
-// With beta != 0 the 32 old values are loaded before any store so the loads
-// are in flight together (stores to C could otherwise alias them).
+// Fused fp16 hi[/lo] copies of 32 result values of one row.
+__device__ __forceinline__ void store_fp16_copies(const GemmArgs& args, const float* r, long long gi, long long gj0) {
+  __half* hrow = args.out_hi + gi + gj0 * args.ld_out;
+  __half* lrow = args.out_lo ? args.out_lo + gi + gj0 * args.ld_out : nullptr;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const long long gj = gj0 + j;
+    if (gj >= args.N || (args.tri && (gi - gj) < args.diag)) continue;
+    const __half h = __float2half_rn(r[j]);
+    hrow[(long long)j * args.ld_out] = h;
+    if (lrow) lrow[(long long)j * args.ld_out] = __float2half_rn((r[j] - __half2float(h)) * args.out_lo_scale);
+  }
+}
+
+// Per-element path: alpha/beta update of 32 consecutive columns of one row,
+// with the lower-triangle mask and bounds. With beta != 0 the 32 old values
+// are loaded before any store so the loads are in flight together.
 __device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const float* v, long long gi, long long gj0) {
   float* crow = args.C + gi + gj0 * args.ldc;
   bool keep[32];
@@ -124,17 +151,57 @@ __device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const flo
 #pragma unroll
   for (int j = 0; j < 32; ++j)
     if (keep[j]) crow[(long long)j * args.ldc] = r[j];
-  if (args.out_hi) {
-    __half* hrow = args.out_hi + gi + gj0 * args.ld_out;
-    __half* lrow = args.out_lo ? args.out_lo + gi + gj0 * args.ld_out : nullptr;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      if (!keep[j]) continue;
-      const __half h = __float2half_rn(r[j]);
-      hrow[(long long)j * args.ld_out] = h;
-      if (lrow) lrow[(long long)j * args.ld_out] = __float2half_rn((r[j] - __half2float(h)) * args.out_lo_scale);
+  if (args.out_hi) store_fp16_copies(args, r, gi, gj0);
+}
+
+// Epilogue state shared by the 4 epilogue warps (identical in all of them).
+struct EpiState {
+  int chunk;        // staged chunks written so far (selects the smem buffer)
+  uint32_t lphase;  // per-buffer phase bit of the C-load barriers
+};
+
+// TMA path for one 128 x 32 chunk at (m0, gj0): v[] holds this thread's row
+// (32 consecutive columns). All 128 epilogue threads call it together.
+__device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* stage, uint64_t* cload, EpiState& es,
+                                                   const float* v, int m0, int gj0, int row, bool need_load,
+                                                   bool issuer, volatile int* abort_flag) {
+  const int b = es.chunk & 1;
+  float* S = stage + b * (128 * 32);
+  if (issuer) {
+    bulk_wait_read<1>();  // the store that last used buffer b has finished reading it
+    if (need_load) {
+      mbar_arrive_expect_tx(&cload[b], 128 * 32 * 4);
+      tma_load_2d(S, &args.mapC, &cload[b], m0, gj0);
     }
   }
+  named_bar_sync(1, 128);
+  const long long gi = (long long)m0 + row;
+  float r[32];
+  if (need_load) {
+    mbar_wait(&cload[b], (es.lphase >> b) & 1u, abort_flag, args.err, kDevErrTimeoutEpilogue);
+    es.lphase ^= 1u << b;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float old = S[j * 128 + row];
+      const bool masked = args.tri && (gi - (long long)(gj0 + j)) < args.diag;
+      r[j] = masked ? old : fmaf(args.beta, old, args.alpha * v[j]);
+      S[j * 128 + row] = r[j];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      r[j] = args.alpha * v[j];
+      S[j * 128 + row] = r[j];
+    }
+  }
+  fence_proxy_async_smem();
+  named_bar_sync(1, 128);
+  if (issuer) {
+    tma_store_2d(&args.mapC, S, m0, gj0);
+    bulk_commit();
+  }
+  if (args.out_hi && gi < args.M) store_fp16_copies(args, r, gi, gj0);
+  ++es.chunk;
 }
 
 template <class Cfg>
@@ -142,12 +209,14 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * Cfg::STAGE_BYTES);
+  float* stage_c = reinterpret_cast<float*>(smem + STAGES * Cfg::STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * Cfg::STAGE_BYTES + Cfg::EPI_BYTES);
   uint64_t* empty = full + STAGES;
   uint64_t* tfull = empty + STAGES;  // [2]
   uint64_t* tempty = tfull + 2;      // [2]
   uint64_t* drain = tempty + 2;      // [1] teardown barrier for the MMA issuer
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  uint64_t* cload = drain + 1;       // [2] C-chunk loads of the TMA epilogue
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5;
@@ -161,6 +230,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4);
+      mbar_init(&cload[b], 1);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -173,6 +243,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
       tma_prefetch_map(&args.mapA[1]);
       tma_prefetch_map(&args.mapB[1]);
     }
+    if (args.tma_c) tma_prefetch_map(&args.mapC);
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
@@ -232,9 +303,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     // Accumulation "chunks": plain mode accumulates a tile's whole K range in
-    // one TMEM buffer; split mode closes a chunk every `kchunk` K-blocks so
-    // the epilogue can fold it into round-to-nearest FP32 registers (the
-    // tensor core's own accumulation truncates).
+    // one TMEM buffer; split mode closes a chunk every `kchunk` K-blocks.
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
@@ -304,12 +373,16 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
     const int quarter = warp & 3;  // TMEM lane quarter this warp may access
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    const bool issuer = (warp == 2 && lane == 0);
+    EpiState es{0, 0u};
     int it = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
       const int4 tile = args.tiles[t];
       const long long gi = (long long)tile.x + row;
       const bool row_ok = gi < args.M;
+      // the tile crosses the masked (upper) region: min(i - j) < diag
+      const bool tile_masked = args.tri && ((long long)tile.x - (long long)(tile.y + BN - 1)) < args.diag;
       if constexpr (Cfg::NSPLIT == 1) {
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -321,11 +394,19 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
         for (int c0 = 0; c0 < BN; c0 += 32) {
           float v[32];
           tmem_ld32(tacc + c0, v);
-          if (row_ok) epilogue_store32(args, v, gi, (long long)tile.y + c0);
+          if (c0 == BN - 32) {  // accumulator fully read: hand it back to the MMA warp
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[buf]);
+          }
+          if (args.tma_c) {
+            if (tile.y + c0 < args.N)
+              epilogue_chunk_tma(args, stage_c, cload, es, v, tile.x, tile.y + c0, row,
+                                 args.beta != 0.0f || tile_masked, issuer, abort_flag);
+          } else if (row_ok) {
+            epilogue_store32(args, v, gi, (long long)tile.y + c0);
+          }
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[buf]);
       } else {
         float acc[BN];
 #pragma unroll
@@ -353,12 +434,19 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
           if (lane == 0) mbar_arrive(&tempty[buf]);
         }
         if (!ok) break;
-        if (row_ok) {
 #pragma unroll
-          for (int c0 = 0; c0 < BN; c0 += 32) epilogue_store32(args, acc + c0, gi, (long long)tile.y + c0);
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+          if (args.tma_c) {
+            if (tile.y + c0 < args.N)
+              epilogue_chunk_tma(args, stage_c, cload, es, acc + c0, tile.x, tile.y + c0, row,
+                                 args.beta != 0.0f || tile_masked, issuer, abort_flag);
+          } else if (row_ok) {
+            epilogue_store32(args, acc + c0, gi, (long long)tile.y + c0);
+          }
         }
       }
     }
+    if (issuer) bulk_wait<0>();  // all TMA stores complete before the CTA retires
   }
 
   tc_fence_before();

@@ -45,8 +45,10 @@ def _check(got, model, absprod, tol, etol, mask=None):
 
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
-@pytest.mark.parametrize("m,n,k", [(256, 512, 128), (1000, 300, 200), (129, 257, 65)])
-def test_sgemm(tblas, ta, tb, m, n, k, precision):
+@pytest.mark.parametrize("m,n,k,ldc_pad", [(256, 512, 128, 0), (1000, 300, 200, 0), (129, 257, 65, 0),
+                                           (256, 300, 128, 1), (384, 256, 1024, 4)])
+def test_sgemm(tblas, ta, tb, m, n, k, ldc_pad, precision):
+    """ldc_pad = 1 makes C unreachable for TMA (per-element epilogue path)."""
     rng = _rng(1000 + m + n + k)
     opA = rng.uniform(-1, 1, (m, k)).astype(np.float32)
     opB = rng.uniform(-1, 1, (k, n)).astype(np.float32)
@@ -56,12 +58,17 @@ def test_sgemm(tblas, ta, tb, m, n, k, precision):
     B_st = opB if tb == "N" else opB.T.copy()
     dA = torch.from_numpy(np.ascontiguousarray(A_st.T)).cuda()  # row-major storage of A_st^T == col-major A_st
     dB = torch.from_numpy(np.ascontiguousarray(B_st.T)).cuda()
-    dC = torch.from_numpy(np.ascontiguousarray(C0.T)).cuda()
+    ldc = m + ldc_pad
+    Cpad = np.full((n, ldc), 7.0, dtype=np.float32)
+    Cpad[:, :m] = C0.T
+    dC = torch.from_numpy(Cpad).cuda()
     lda, ldb = A_st.shape[0], B_st.shape[0]
     tblas._check(tblas.lib.tb_sgemm(ta.encode(), tb.encode(), m, n, k, alpha, dA.data_ptr(), lda, dB.data_ptr(),
-                                    ldb, beta, dC.data_ptr(), m, precision))
+                                    ldb, beta, dC.data_ptr(), ldc, precision))
     tblas.synchronize()
-    got = dC.cpu().numpy().T
+    full = dC.cpu().numpy()
+    assert np.all(full[:, m:] == 7.0), "padding rows of C were written"
+    got = full[:, :m].T
     if precision == 0:
         prod = orc.h(opA) @ orc.h(opB)
     else:
