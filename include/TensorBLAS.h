@@ -58,4 +58,33 @@ TB_API void tc_trsm(cublasHandle_t handle, long int m, long int n, float* A, lon
 TB_API void tc_cumpsgemm_trsm(cublasHandle_t handle, cumpsgemm::handle_t cumpsgemm_handle, long int m, long int n,
                               float* A, long int lda, float* B, long int ldb, long int nb);
 
+/* include/TensorBLAS.h:159 — lower triangle of C = alpha (A B^T + B A^T)
+ * + beta C, A and B n x k. Ah: FP16 workspace (2 n k halves in the
+ * reference; used when large enough for this layout). */
+TB_API void tc_syr2k(cublasHandle_t handle, long int n, long int k, float alpha, float* A, long int lda, float* B,
+                     long int ldb, float beta, float* C, long int ldc, __half* Ah, long int nb);
+
+/* include/TensorBLAS.h:161 — FP32-accurate SYR2K. */
+TB_API void tc_cumpsgemm_syr2k(cumpsgemm::handle_t cumpsgemm_handle, long int n, long int k, float alpha, float* A,
+                               long int lda, float* B, long int ldb, float beta, float* C, long int ldc, long int nb);
+
+/* include/TensorBLAS.h:153 — C = alpha A B, A m x m lower (left, out of
+ * place). The strict upper triangle of A is ignored (the reference requires
+ * it to be zero). */
+TB_API void tc_trmm(cublasHandle_t handle, long int m, long int n, float alpha, float* A, long int lda, float* B,
+                    long int ldb, float* C, long int ldc, __half* hwork, long int nb);
+
+/* include/TensorBLAS.h:155 — FP32-accurate TRMM. */
+TB_API void tc_cumpsgemm_trmm(cumpsgemm::handle_t cumpsgemm_handle, long int m, long int n, float alpha, float* A,
+                              long int lda, float* B, long int ldb, float* C, long int ldc, long int nb);
+
+/* include/TensorBLAS.h:165 — C = alpha A B + beta C, A symmetric with its
+ * lower triangle stored (left). Unlike the reference, A is not modified. */
+TB_API void tc_symm(cublasHandle_t handle, long int m, long int n, float alpha, float* A, long int lda, float* B,
+                    int ldb, float beta, float* C, long int ldc, __half* Ah);
+
+/* include/TensorBLAS.h:167 — FP32-accurate SYMM. */
+TB_API void tc_cumpsgemm_symm(cumpsgemm::handle_t cumpsgemm_handle, long int m, long int n, float alpha, float* A,
+                              long int lda, float* B, int ldb, float beta, float* C, long int ldc);
+
 #endif /* TENSORBLAS_B200_H_ */

@@ -85,6 +85,30 @@ TB_API tb_status tb_ssyrk(char uplo, char trans, long n, long k, float alpha, co
 TB_API tb_status tb_strsm(char side, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
                           int precision);
 
+/*
+ * SYR2K: C = alpha (A B^T + B A^T) + beta C, lower triangle written, A and B
+ * n x k (trans 'N'). Replaces tc_syr2k (BLAS/tc_syr2k.cu:116-152) and, with
+ * TB_PREC_SPLIT, tc_cumpsgemm_syr2k (BLAS/tc_cumpsgemm_syr2k.cu).
+ */
+TB_API tb_status tb_ssyr2k(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
+                           const float* B, long ldb, float beta, float* C, long ldc, long nb, int precision);
+
+/*
+ * TRMM (left, out of place): C = alpha op(A) B, A m x m triangular ('L' lower
+ * or 'U' upper; the other triangle is never read), B and C m x n.
+ * Replaces tc_trmm (BLAS/tc_trmm.cu:99-135, lower) and tc_cumpsgemm_trmm.
+ */
+TB_API tb_status tb_strmm(char uplo, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
+                          float* C, long ldc, long nb, int precision);
+
+/*
+ * SYMM (left): C = alpha A B + beta C, A m x m symmetric with triangle `uplo`
+ * stored; A is not modified. Replaces tc_symm (BLAS/tc_symm.cu:3-19) and
+ * tc_cumpsgemm_symm (BLAS/tc_cumpsgemm_symm.cu).
+ */
+TB_API tb_status tb_ssymm(char uplo, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
+                          float beta, float* C, long ldc, int precision);
+
 /* Mirror lower -> upper of an n x n matrix (util/util.cu:148-157). */
 TB_API tb_status tb_ssymmetrize(long n, float* A, long lda);
 

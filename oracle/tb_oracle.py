@@ -149,3 +149,91 @@ def rel_errors(x: np.ndarray, ref: np.ndarray, mask: np.ndarray | None = None):
     scale = np.maximum(np.abs(ref), np.finfo(np.float64).tiny)
     nrm = np.linalg.norm(ref)
     return float(np.max(d / scale)) if d.size else 0.0, float(np.linalg.norm(d) / nrm) if nrm > 0 else 0.0
+
+
+def _prod(a, b_t, split):
+    """a @ b_t with FP16-rounded operands (plain) or the split model."""
+    if split:
+        return split_product(np.asarray(a, np.float32), np.asarray(b_t, np.float32))
+    return h(a) @ h(b_t)
+
+
+def syr2k_model(A, B, alpha=1.0, beta=0.0, C=None, split=False):
+    """Lower triangle of alpha (A B^T + B A^T) + beta C (BLAS/tc_syr2k.cu:3-34):
+    each product FP16 x FP16 with FP32 accumulation, evaluated exactly."""
+    A = np.asarray(A, np.float32)
+    B = np.asarray(B, np.float32)
+    n = A.shape[0]
+    res = alpha * (_prod(A, B.T, split) + _prod(B, A.T, split))
+    if C is not None and beta != 0.0:
+        res = res + beta * np.asarray(C, np.float64)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    base = np.zeros((n, n)) if C is None else np.asarray(C, np.float64)
+    return np.where(low, res, base)
+
+
+def trmm_model(A, B, alpha=1.0, upper=False, split=False):
+    """alpha op(A) B with A triangular (BLAS/tc_trmm.cu:4-98); the other
+    triangle of A is treated as zero."""
+    A = np.asarray(A, np.float32)
+    T = np.triu(A) if upper else np.tril(A)
+    return alpha * _prod(T, np.asarray(B, np.float32), split)
+
+
+def symm_model(A, B, alpha=1.0, beta=0.0, C=None, lower=True, split=False):
+    """alpha A B + beta C with A symmetric from its stored triangle
+    (BLAS/tc_symm.cu:3-19)."""
+    A = np.asarray(A, np.float32)
+    S = np.tril(A) + np.tril(A, -1).T if lower else np.triu(A) + np.triu(A, 1).T
+    res = alpha * _prod(S, np.asarray(B, np.float32), split)
+    if C is not None and beta != 0.0:
+        res = res + beta * np.asarray(C, np.float64)
+    return res
+
+
+# ------------------------------------------------------------------ Ozaki INT8 scheme
+def ozaki_slices(A, S):
+    """Exact slicing used for the INT8 emulation of FP64 products.
+
+    e_i = frexp exponent of max_p |a_ip| (so |a_ip| < 2^e_i; 0 for a zero
+    row); x = a * 2^-e_i; for each slice y = 128 x, q = trunc(y), x = y - q.
+    Returns (Q int8 [S, n, k], e int [n]). Every step is exact in FP64.
+    """
+    A = np.asarray(A, dtype=np.float64)
+    _, e = np.frexp(np.max(np.abs(A), axis=1) if A.size else np.zeros(A.shape[0]))
+    e = e.astype(np.int64)
+    x = np.ldexp(A, -e[:, None])
+    Q = np.empty((S,) + A.shape, dtype=np.int8)
+    for s in range(S):
+        y = x * 128.0
+        q = np.trunc(y)
+        x = y - q
+        Q[s] = q.astype(np.int8)
+    return Q, e
+
+
+def ozaki_level_product(Q, L):
+    """P_L = sum_{s+t=L} Q_s Q_t^T in exact int64 (slices numbered from 1)."""
+    S = Q.shape[0]
+    P = np.zeros((Q.shape[1], Q.shape[1]), dtype=np.int64)
+    for s in range(max(1, L - S), min(S, L - 1) + 1):
+        P += Q[s - 1].astype(np.int64) @ Q[L - s - 1].astype(np.int64).T
+    return P
+
+
+def ozaki_syrk_model(A, S):
+    """The truncated Ozaki sum C = sum_{L=2}^{S+1} 2^(e_i+e_j-7L) P_L (long double)."""
+    Q, e = ozaki_slices(A, S)
+    n = Q.shape[1]
+    C = np.zeros((n, n), dtype=np.longdouble)
+    scale = np.ldexp(np.longdouble(1.0), (e[:, None] + e[None, :]).astype(np.int64))
+    for L in range(2, S + 2):
+        C += ozaki_level_product(Q, L).astype(np.longdouble) * scale * np.ldexp(np.longdouble(1.0), -7 * L)
+    return C
+
+
+def syrk_extended(A, rows, cols):
+    """Entries (rows[i], cols[i]) of A A^T in long double (64-bit mantissa):
+    the higher-than-FP64 oracle for the FP64-emulation checks."""
+    Al = np.asarray(A, dtype=np.float64).astype(np.longdouble)
+    return np.einsum("ij,ij->i", Al[rows], Al[cols])

@@ -41,6 +41,10 @@ __global__ void __launch_bounds__(256) convert8_kernel(long long rows, long long
 #pragma unroll
         for (int e = 0; e < 8; ++e)
           if (i + e < j) f[e] = 0.f;
+      } else if (tri == 3) {
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+          if (i + e > j) f[e] = 0.f;
       }
       __half h[8];
 #pragma unroll
@@ -75,7 +79,7 @@ __global__ void __launch_bounds__(256) convert1_kernel(long long rows, long long
     if (tri == 2) i0 += (j >> 3) << 3;
     for (long long i = i0; i < rows; i += (long long)gridDim.x * blockDim.x) {
       float f = src[i + j * lds];
-      if (tri == 1 && i < j) f = 0.f;
+      if ((tri == 1 && i < j) || (tri == 3 && i > j)) f = 0.f;
       const __half h = __float2half_rn(f);
       hi[i + j * ldd] = h;
       if (lo) lo[i + j * ldd] = __float2half_rn((f - __half2float(h)) * lo_scale);
@@ -83,7 +87,48 @@ __global__ void __launch_bounds__(256) convert1_kernel(long long rows, long long
   }
 }
 
+// Full symmetric FP16 copy of an n x n matrix of which only one triangle is
+// stored: out(i, j) = A(i, j) on the stored side, A(j, i) on the other. Each
+// 32 x 32 output tile reads its own tile and the mirrored one through shared
+// memory, so every global read and write is coalesced (the reference instead
+// mirrors the caller's A in place with strided reads, BLAS/tc_symm.cu:7).
+__global__ void __launch_bounds__(256) convert_sym_kernel(long long n, const float* __restrict__ A, long long lda,
+                                                          int lower, __half* __restrict__ hi, __half* __restrict__ lo,
+                                                          long long ldd, float lo_scale) {
+  __shared__ float own[32][33], mir[32][33];
+  const long long bi = blockIdx.x, bj = blockIdx.y;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const long long i = bi * 32 + tx, j = bj * 32 + r;  // own tile element (i, j)
+    own[r][tx] = (i < n && j < n) ? A[i + j * lda] : 0.f;
+    const long long mi = bj * 32 + tx, mj = bi * 32 + r;  // mirrored tile element (mi, mj)
+    mir[r][tx] = (mi < n && mj < n) ? A[mi + mj * lda] : 0.f;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const long long i = bi * 32 + tx, j = bj * 32 + r;
+    if (i >= n || j >= n) continue;
+    const bool stored = lower ? (i >= j) : (i <= j);
+    const float f = stored ? own[r][tx] : mir[tx][r];  // mir[tx][r] = A(j, i)
+    const __half h = __float2half_rn(f);
+    hi[i + j * ldd] = h;
+    if (lo) lo[i + j * ldd] = __float2half_rn((f - __half2float(h)) * lo_scale);
+  }
+}
+
 }  // namespace
+
+tb_status convert_sym_f32_f16(long long n, const float* A, long long lda, bool lower, __half* hi, __half* lo,
+                              long long ldd, float lo_scale, cudaStream_t stream) {
+  if (n <= 0) return TB_SUCCESS;
+  const long long nt = (n + 31) / 32;
+  if (nt > 65535) return TB_ERROR_NOT_SUPPORTED;
+  convert_sym_kernel<<<dim3((unsigned)nt, (unsigned)nt), 256, 0, stream>>>(n, A, lda, lower ? 1 : 0, hi, lo, ldd,
+                                                                           lo_scale);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
 
 tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
                           long long ldd, float lo_scale, int tri, cudaStream_t stream) {

@@ -81,6 +81,21 @@ bool make_c_map(CUtensorMap* map, float* C, long long rows, long long cols, long
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map for an fp16 side copy restricted to rows x cols (the TMA store
+// clips to this extent, which implements the out_m / out_n region).
+bool make_half_out_map(CUtensorMap* map, __half* p, long long rows, long long cols, long long ld) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc || !p || rows <= 0 || cols <= 0 || (reinterpret_cast<uintptr_t>(p) & 15) != 0 || (ld * 2) % 16 != 0)
+    return false;
+  cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {128, 32};
+  cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class Cfg>
 tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops) {
   static bool attr_set[64] = {false};
@@ -135,7 +150,13 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   a.out_lo = c.out_lo;
   a.ld_out = c.ld_out;
   a.out_lo_scale = c.out_lo_scale;
-  a.err = device_error_word();
+  a.out_m = c.out_m >= 0 ? (c.out_m < c.M ? c.out_m : c.M) : c.M;
+  a.out_n = c.out_n >= 0 ? (c.out_n < c.N ? c.out_n : c.N) : c.N;
+  a.tma_out = 0;
+  if (c.out_hi && a.tma_c && c.tri == 0 && make_half_out_map(&a.mapOut[0], c.out_hi, a.out_m, a.out_n, c.ld_out) &&
+      (!c.out_lo || make_half_out_map(&a.mapOut[1], c.out_lo, a.out_m, a.out_n, c.ld_out)))
+    a.tma_out = 1;
+  a.err = c.err ? c.err : device_error_word();
   // TMA coordinates along the contiguous dimension must be 16-byte aligned.
   if (c.a_hi.mn_major && (c.a_off % 8) != 0) return TB_ERROR_INVALID_VALUE;
   if (c.b_hi.mn_major && (c.b_off % 8) != 0) return TB_ERROR_INVALID_VALUE;

@@ -48,6 +48,7 @@ struct GemmArgs {
   CUtensorMap mapA[2];  // [0] hi, [1] lo (split mode only)
   CUtensorMap mapB[2];
   CUtensorMap mapC;     // fp32 C, box {128, 32} (TMA epilogue only)
+  CUtensorMap mapOut[2];  // fp16 side copies hi / lo over [0,out_m) x [0,out_n), box {128, 32}
   const int4* tiles;    // {m0, n0, kb_begin, kb_end}; m0/n0 relative to C
   int num_tiles;
   int a_off;  // row offset of the A operand in mapA's row coordinate
@@ -68,6 +69,8 @@ struct GemmArgs {
   __half* out_lo;
   long long ld_out;
   float out_lo_scale;
+  int out_m, out_n;  // side copies only for rows < out_m and columns < out_n
+  int tma_out;       // 1: side copies through mapOut (requires tma_c and tri == 0)
   int* err;
 };
 
@@ -120,7 +123,7 @@ __device__ __forceinline__ void store_fp16_copies(const GemmArgs& args, const fl
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    if (gj >= args.N || (args.tri && (gi - gj) < args.diag)) continue;
+    if (gj >= args.out_n || (args.tri && (gi - gj) < args.diag)) continue;
     const __half h = __float2half_rn(r[j]);
     hrow[(long long)j * args.ld_out] = h;
     if (lrow) lrow[(long long)j * args.ld_out] = __float2half_rn((r[j] - __half2float(h)) * args.out_lo_scale);
@@ -151,7 +154,7 @@ __device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const flo
 #pragma unroll
   for (int j = 0; j < 32; ++j)
     if (keep[j]) crow[(long long)j * args.ldc] = r[j];
-  if (args.out_hi) store_fp16_copies(args, r, gi, gj0);
+  if (args.out_hi && gi < args.out_m) store_fp16_copies(args, r, gi, gj0);
 }
 
 // Epilogue state shared by the 4 epilogue warps (identical in all of them).
@@ -162,13 +165,22 @@ struct EpiState {
 
 // TMA path for one 128 x 32 chunk at (m0, gj0): v[] holds this thread's row
 // (32 consecutive columns). All 128 epilogue threads call it together.
+// With TMA side copies (tma_out) the second staging buffer holds the fp16
+// hi/lo chunk (8 KB each) and the fp32 chunk is single-buffered.
 __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* stage, uint64_t* cload, EpiState& es,
                                                    const float* v, int m0, int gj0, int row, bool need_load,
                                                    bool issuer, volatile int* abort_flag) {
-  const int b = es.chunk & 1;
+  const bool side_mode = args.tma_out != 0;
+  const bool side = side_mode && gj0 < args.out_n && m0 < args.out_m;
+  const int b = side_mode ? 0 : (es.chunk & 1);
   float* S = stage + b * (128 * 32);
+  __half* Hs = reinterpret_cast<__half*>(stage + 128 * 32);
+  __half* Ls = Hs + 128 * 32;
   if (issuer) {
-    bulk_wait_read<1>();  // the store that last used buffer b has finished reading it
+    if (side_mode)
+      bulk_wait_read<0>();  // single-buffered: every earlier store has read smem
+    else
+      bulk_wait_read<1>();  // the store that last used buffer b has finished reading it
     if (need_load) {
       mbar_arrive_expect_tx(&cload[b], 128 * 32 * 4);
       tma_load_2d(S, &args.mapC, &cload[b], m0, gj0);
@@ -194,13 +206,25 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
       S[j * 128 + row] = r[j];
     }
   }
+  if (side) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const __half hv = __float2half_rn(r[j]);
+      Hs[j * 128 + row] = hv;
+      Ls[j * 128 + row] = __float2half_rn((r[j] - __half2float(hv)) * args.out_lo_scale);
+    }
+  }
   fence_proxy_async_smem();
   named_bar_sync(1, 128);
   if (issuer) {
     tma_store_2d(&args.mapC, S, m0, gj0);
+    if (side) {
+      tma_store_2d(&args.mapOut[0], Hs, m0, gj0);
+      if (args.out_lo) tma_store_2d(&args.mapOut[1], Ls, m0, gj0);
+    }
     bulk_commit();
   }
-  if (args.out_hi && gi < args.M) store_fp16_copies(args, r, gi, gj0);
+  if (!side_mode && args.out_hi && gi < args.out_m) store_fp16_copies(args, r, gi, gj0);
   ++es.chunk;
 }
 
@@ -244,6 +268,10 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
       tma_prefetch_map(&args.mapB[1]);
     }
     if (args.tma_c) tma_prefetch_map(&args.mapC);
+    if (args.tma_out) {
+      tma_prefetch_map(&args.mapOut[0]);
+      if (args.out_lo) tma_prefetch_map(&args.mapOut[1]);
+    }
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, Cfg::TMEM_COLS);

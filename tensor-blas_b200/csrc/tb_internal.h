@@ -76,7 +76,9 @@ struct GemmCall {
   __half* out_lo = nullptr;
   long long ld_out = 0;
   float out_lo_scale = 2048.0f;
+  int out_m = -1, out_n = -1;  // side-copy region (default: all of C)
   double flops = 0;  // algorithmic flops of this launch (profiling only)
+  int* err = nullptr;  // device error word (nullptr: the library's per-device word)
 };
 
 // Tile width along N used by the engine for a given split mode.
@@ -96,8 +98,14 @@ const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
 // fp32 (rows x cols, column-major, lds) -> fp16 hi [and lo] with the same
 // orientation (ldd). lo = fp16((x - hi) * lo_scale).
 //   tri == 0: whole matrix; tri == 1: zero the strict upper triangle;
-//   tri == 2: only rows i >= j (rounded down to 8) are written.
+//   tri == 2: only rows i >= j (rounded down to 8) are written;
+//   tri == 3: zero the strict lower triangle.
 tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
                           long long ldd, float lo_scale, int tri, cudaStream_t stream);
+// C(lower) *= beta (C = 0 when beta == 0).
+tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st);
+// Full symmetric FP16 copy of an n x n matrix with one stored triangle.
+tb_status convert_sym_f32_f16(long long n, const float* A, long long lda, bool lower, __half* hi, __half* lo,
+                              long long ldd, float lo_scale, cudaStream_t stream);
 
 }  // namespace tb

@@ -24,20 +24,22 @@ __global__ void scale_lower_kernel(long long n, float beta, float* C, long long 
 }
 }  // namespace
 
+// C(lower) *= beta (C = 0 when beta == 0), the k == 0 / alpha == 0 case.
+tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st) {
+  dim3 g((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)(n < 65535 ? n : 65535));
+  scale_lower_kernel<<<g, 256, 0, st>>>(n, beta, C, ldc);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
+
 tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, long lda, float beta, float* C, long ldc,
                     long nb, Split split, void* ws, size_t ws_bytes, cudaStream_t st) {
   if (n < 0 || k < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
   if (ldc < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
   if (lda < ((trans ? k : n) > 1 ? (trans ? k : n) : 1)) return TB_ERROR_INVALID_VALUE;
   if (n == 0) return TB_SUCCESS;
-  if (k == 0 || alpha == 0.f) {
-    if (beta == 1.f) return TB_SUCCESS;
-    dim3 g((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)(n < 65535 ? n : 65535));
-    scale_lower_kernel<<<g, 256, 0, st>>>(n, beta, C, ldc);
-    TB_CUDA_TRY(cudaGetLastError());
-    note_launch();
-    return TB_SUCCESS;
-  }
+  if (k == 0 || alpha == 0.f) return beta == 1.f ? TB_SUCCESS : scale_lower(n, beta, C, ldc, st);
   const bool hilo = split == Split::kHiLo;
   const long long rows = trans ? k : n, cols = trans ? n : k;
   const long long ldh = round_up(rows, 64);

@@ -194,14 +194,20 @@ struct TrsmCtx {
   cudaStream_t st;
 };
 
+// Leaf block [s, e): X_b = B_b * W^T (right) or W * B_b (left), W = inv(A_bb),
+// as a split-FP16 product. W is lower triangular, so each output tile only
+// needs the K-blocks up to its own diagonal position. The FP16 hi/lo copy of
+// B_b (R) was written by the epilogue of the update that last touched B_b,
+// except for the first leaf, which converts it here.
 tb_status leaf_solve(TrsmCtx& c, int bidx, long s, long e) {
   const long nbl = e - s;
   GemmCall g;
   g.split = Split::kHiLo;
   const bool split_x = c.split == Split::kHiLo;
+  const bool need_convert = (s == 0);
   if (c.right) {
     // R = B[:, s:e] (m x nbl) -> FP16 hi/lo; X_b = R * W^T
-    TB_TRY(convert_f32_f16(c.m, nbl, c.B + s * c.ldb, c.ldb, c.rh, c.rl, c.ldr, 2048.f, 0, c.st));
+    if (need_convert) TB_TRY(convert_f32_f16(c.m, nbl, c.B + s * c.ldb, c.ldb, c.rh, c.rl, c.ldr, 2048.f, 0, c.st));
     g.a_hi = {c.rh, c.m, nbl, c.ldr, true};
     g.a_lo = {c.rl, c.m, nbl, c.ldr, true};
     g.b_hi = {c.wh + bidx * c.wstride, nbl, nbl, c.ldw, true};
@@ -215,7 +221,7 @@ tb_status leaf_solve(TrsmCtx& c, int bidx, long s, long e) {
     g.ld_out = c.ldx;
   } else {
     // R = B[s:e, :] (nbl x n) -> FP16 hi/lo (K-major operand, rows = n); X_b = W * R
-    TB_TRY(convert_f32_f16(nbl, c.n, c.B + s, c.ldb, c.rh, c.rl, c.ldr, 2048.f, 0, c.st));
+    if (need_convert) TB_TRY(convert_f32_f16(nbl, c.n, c.B + s, c.ldb, c.rh, c.rl, c.ldr, 2048.f, 0, c.st));
     g.a_hi = {c.wh + bidx * c.wstride, nbl, nbl, c.ldw, true};
     g.a_lo = {c.wl + bidx * c.wstride, nbl, nbl, c.ldw, true};
     g.b_hi = {c.rh, c.n, nbl, c.ldr, false};
@@ -231,7 +237,13 @@ tb_status leaf_solve(TrsmCtx& c, int bidx, long s, long e) {
   g.alpha = 1.f;
   g.beta = 0.f;
   g.flops = (double)g.M * g.N * nbl;  // triangular solve of the leaf: other * nbl^2 flops
-  const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split), 0, (int)((nbl + kGemmBK - 1) / kGemmBK));
+  const int bn = gemm_bn(g.split);
+  std::vector<int4> plan = plan_rect(g.M, g.N, bn, 0, (int)((nbl + kGemmBK - 1) / kGemmBK));
+  for (int4& t : plan) {  // K (= columns of W) beyond the tile's last W row is zero
+    const long lim = c.right ? (long)t.y + bn : (long)t.x + kGemmBM;
+    const long kmax = lim < nbl ? lim : nbl;
+    t.w = (int)((kmax + kGemmBK - 1) / kGemmBK);
+  }
   g.tiles = upload_tiles(plan, c.st);
   if (!g.tiles) return TB_ERROR_ALLOC;
   g.num_tiles = (int)plan.size();
@@ -270,6 +282,16 @@ tb_status update(TrsmCtx& c, long s, long mid, long e) {
   g.ldc = c.ldb;
   g.alpha = -1.f;
   g.beta = 1.f;
+  // The next leaf is [mid, mid + leaf): this is the last update that touches
+  // it, so its FP16 hi/lo copy is written here, fused into the epilogue.
+  const long next = std::min<long>(c.leaf, e - mid);
+  g.out_hi = c.rh;
+  g.out_lo = c.rl;
+  g.ld_out = c.ldr;
+  if (c.right)
+    g.out_n = (int)next;
+  else
+    g.out_m = (int)next;
   g.flops = 2.0 * g.M * g.N * kk;
   const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split), 0, (int)((kk + kGemmBK - 1) / kGemmBK));
   g.tiles = upload_tiles(plan, c.st);

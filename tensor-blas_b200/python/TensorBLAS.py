@@ -46,6 +46,15 @@ lib.tb_profile_begin.restype = ctypes.c_int
 lib.tb_profile_end.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(ctypes.c_long)]
 lib.tb_profile_end.restype = ctypes.c_int
+lib.tb_ssyr2k.argtypes = [ctypes.c_char, ctypes.c_char, _c_long, _c_long, ctypes.c_float, _fp, _c_long, _fp, _c_long,
+                          ctypes.c_float, _fp, _c_long, _c_long, ctypes.c_int]
+lib.tb_ssyr2k.restype = ctypes.c_int
+lib.tb_strmm.argtypes = [ctypes.c_char, _c_long, _c_long, ctypes.c_float, _fp, _c_long, _fp, _c_long, _fp, _c_long,
+                         _c_long, ctypes.c_int]
+lib.tb_strmm.restype = ctypes.c_int
+lib.tb_ssymm.argtypes = [ctypes.c_char, _c_long, _c_long, ctypes.c_float, _fp, _c_long, _fp, _c_long, ctypes.c_float,
+                         _fp, _c_long, ctypes.c_int]
+lib.tb_ssymm.restype = ctypes.c_int
 lib.tb_sgemm.argtypes = [ctypes.c_char, ctypes.c_char, _c_long, _c_long, _c_long, ctypes.c_float, _fp, _c_long, _fp,
                          _c_long, ctypes.c_float, _fp, _c_long, ctypes.c_int]
 lib.tb_sgemm.restype = ctypes.c_int
@@ -153,6 +162,45 @@ def trsm(A, B, side="L", nb=512, precision=PLAIN):
     _bind_stream(B)
     strsm(side, Acm, Bcm, m, n, A.shape[0], m, nb, precision)
     return Bcm.t()
+
+
+def syr2k(A, B, alpha=1.0, beta=0.0, C=None, nb=256, precision=PLAIN):
+    """Lower triangle of alpha (A B^T + B A^T) + beta C (logical n x k torch matrices)."""
+    _dev_f32(A, "A")
+    _dev_f32(B, "B")
+    n, k = A.shape
+    Acm, Bcm = A.t().contiguous(), B.t().contiguous()
+    Ccm = torch.zeros(n, n, device=A.device, dtype=torch.float32) if C is None else C.t().contiguous()
+    _bind_stream(A)
+    _check(lib.tb_ssyr2k(b"L", b"N", n, k, alpha, Acm.data_ptr(), n, Bcm.data_ptr(), n, beta, Ccm.data_ptr(), n, nb,
+                         precision))
+    return Ccm.t()
+
+
+def trmm(A, B, alpha=1.0, uplo="L", nb=256, precision=PLAIN):
+    """alpha op(A) B for triangular A ('L' lower / 'U' upper), left side, out of place."""
+    _dev_f32(A, "A")
+    _dev_f32(B, "B")
+    m, n = B.shape
+    Acm, Bcm = A.t().contiguous(), B.t().contiguous()
+    Ccm = torch.empty(n, m, device=B.device, dtype=torch.float32)
+    _bind_stream(B)
+    _check(lib.tb_strmm(uplo.encode(), m, n, alpha, Acm.data_ptr(), m, Bcm.data_ptr(), m, Ccm.data_ptr(), m, nb,
+                        precision))
+    return Ccm.t()
+
+
+def symm(A, B, alpha=1.0, beta=0.0, C=None, uplo="L", precision=PLAIN):
+    """alpha A B + beta C for symmetric A stored in triangle `uplo` (left side)."""
+    _dev_f32(A, "A")
+    _dev_f32(B, "B")
+    m, n = B.shape
+    Acm, Bcm = A.t().contiguous(), B.t().contiguous()
+    Ccm = torch.zeros(n, m, device=B.device, dtype=torch.float32) if C is None else C.t().contiguous()
+    _bind_stream(B)
+    _check(lib.tb_ssymm(uplo.encode(), m, n, alpha, Acm.data_ptr(), m, Bcm.data_ptr(), m, beta, Ccm.data_ptr(), m,
+                        precision))
+    return Ccm.t()
 
 
 def synchronize():

@@ -75,6 +75,51 @@ def trsm(name, m, n, nb, seed):
     save(name, X=Bf.astype(np.float32), meta=json.dumps(dict(m=m, n=n, nb=nb, seed=seed)))
 
 
+def syr2k(name, n, k, nb, seed, full):
+    A = gi.uniform(seed, (n, k))
+    B = gi.uniform(seed + 1, (n, k))
+    C0 = np.zeros((n, n), np.float32)
+    Af, pA = cm(A)
+    Bf, pB = cm(B)
+    Cf, pC = cm(C0)
+    assert lib.ref_syr2k(n, k, 1.0, pA, pB, 0.0, pC, nb) == 0
+    meta = json.dumps(dict(n=n, k=k, nb=nb, seed=seed))
+    if full:
+        save(name, C=np.tril(Cf).astype(np.float32), meta=meta)
+    else:
+        rows, cols = sample_lower(n, 20000, seed + 2)
+        save(name, rows=rows, cols=cols, vals=Cf[rows, cols].astype(np.float32), meta=meta)
+
+
+def trmm(name, m, n, nb, seed):
+    A = np.tril(gi.uniform(seed, (m, m)))  # the reference needs a zero upper triangle
+    B = gi.uniform(seed + 1, (m, n))
+    Af, pA = cm(A)
+    Bf, pB = cm(B)
+    Cf, pC = cm(np.zeros((m, n), np.float32))
+    assert lib.ref_trmm(m, n, 1.0, pA, pB, pC, nb) == 0
+    save(name, C=Cf.astype(np.float32), meta=json.dumps(dict(m=m, n=n, nb=nb, seed=seed)))
+
+
+def symm(name, m, seed):
+    A = gi.uniform(seed, (m, m))
+    B = gi.uniform(seed + 1, (m, m))
+    Af, pA = cm(A)
+    Bf, pB = cm(B)
+    Cf, pC = cm(np.zeros((m, m), np.float32))
+    assert lib.ref_symm(m, m, 1.0, pA, pB, 0.0, pC) == 0
+    save(name, C=Cf.astype(np.float32), meta=json.dumps(dict(m=m, seed=seed)))
+
+
+def ozimmu_syrk(name, n, k, nb, seed, phi):
+    g = gi.rng(seed)
+    A = g.standard_normal((n, k)) * np.exp(phi * g.standard_normal((n, k)))
+    Af, pA = cm(A)
+    Cf, pC = cm(np.zeros((n, n)))
+    assert lib.ref_ozimmu_syrk(n, k, 1.0, pA, 0.0, pC, nb) == 0
+    save(name, C=np.tril(Cf), meta=json.dumps(dict(n=n, k=k, nb=nb, seed=seed, phi=phi)))
+
+
 if __name__ == "__main__":
     syrk("syrk_small", 256, 128, 64, 1.0, 0.0, 101, True)
     syrk("syrk_beta", 200, 50, 64, 0.5, 2.0, 202, True)
@@ -82,3 +127,9 @@ if __name__ == "__main__":
     trsm("trsm_p2", 64, 2048, 256, 404)
     trsm("trsm_small", 64, 1000, 256, 505)
     trsm("trsm_p2_nb512", 32, 4096, 512, 606)
+    syr2k("syr2k_small", 256, 64, 64, 707, True)
+    syr2k("syr2k_p2", 8192, 32, 256, 808, False)
+    trmm("trmm_small", 256, 128, 64, 909)
+    trmm("trmm_p2", 8192, 16, 256, 1010)
+    symm("symm_small", 256, 1111)
+    ozimmu_syrk("dsyrk_small", 256, 128, 64, 1212, 0.5)
