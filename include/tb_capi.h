@@ -109,6 +109,25 @@ TB_API tb_status tb_strmm(char uplo, long m, long n, float alpha, const float* A
 TB_API tb_status tb_ssymm(char uplo, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
                           float beta, float* C, long ldc, int precision);
 
+/*
+ * tb_ssyrk_noalloc: tb_ssyrk for callers that cannot allocate device memory
+ * (no counterpart in the reference library). Same arguments and results as
+ * tb_ssyrk, but every byte of scratch comes from one static 64 MiB device
+ * array compiled into the library, so the call makes no cudaMalloc/cudaFree.
+ * It is meant for callers whose GPU memory is owned by another allocator
+ * (e.g. a framework's caching allocator holding nearly all HBM) and for
+ * latency-critical code that cannot absorb the device-wide synchronisation
+ * cudaMalloc/cudaFree imply. Limit: the tile list plus the FP16 copy of A
+ * (round_up(rows, 64) * cols * 2 bytes, twice that for TB_PREC_SPLIT) must
+ * fit in 64 MiB, else TB_ERROR_INVALID_VALUE with the size in tb_last_error.
+ * The first call on a device looks up the array's address; make it before
+ * any stream capture. All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. k == 0 / alpha == 0 are
+ * not supported here (use tb_ssyrk).
+ */
+TB_API tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
+                                  float beta, float* C, long ldc, long nb, int precision);
+
 /* Mirror lower -> upper of an n x n matrix (util/util.cu:148-157). */
 TB_API tb_status tb_ssymmetrize(long n, float* A, long lda);
 
