@@ -41,6 +41,9 @@ def parse():
     p.add_argument("--nb-trsm", type=int, default=512)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    p.add_argument("--no-extra", action="store_true", help="skip the other configurations")
+    p.add_argument("--profile-step", action="store_true",
+                   help="run one untimed step (plain, then split) and exit: the command profiled with ncu")
     return p.parse_args()
 
 
@@ -326,7 +329,128 @@ def run_mine(args, world, rank, local):
         line["cpu_baseline"] = {"value": fl / 1e12, "unit": "TFLOP/s", "cores": tb_cpu.threads(), "kind": "port",
                                 "sample": f"{reps} x (SYRK n=k={nc} + TRSM m=n={nc}, FP16-rounded operands, "
                                           f"FP32 OpenBLAS) in {el:.1f} s"}
+    if world == 1 and not args.no_extra:
+        line["other_configs"] = other_configs(TB)
     return line
+
+
+def _median_ms(fn, reps, prep=None):
+    fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(reps):
+        if prep:
+            prep()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return float(np.median(out))
+
+
+def other_configs(TB):
+    """The other configurations of the hot path, one measurement each:
+    SYRK n=k=4096 (plain, the CPU-runnable case), FP64 DSYRK n=k=8192 by
+    Ozaki-INT8 vs the reference's native-FP64 tc_ozimmu_syrk, and 512 uneven
+    SYRK/TRSM instances as one grouped batch vs a per-instance plain loop."""
+    import ctypes
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import tb_oracle as orc
+
+    res = {}
+    # ---- SYRK n = k = 4096 (plain)
+    n = 4096
+    A = torch.rand(n, n, device="cuda") * 2 - 1
+    C = torch.zeros(n, n, device="cuda")
+    ms = _median_ms(lambda: TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", 256, TB.PLAIN), 20)
+    res["syrk_4096_plain"] = {"ms": ms, "tflops": float(n) ** 3 / (ms * 1e-3) / 1e12}
+    del A, C
+    # ---- Ozaki DSYRK n = k = 8192
+    lib = TB.lib
+    P, L = ctypes.c_void_p, ctypes.c_long
+    lib.tb_dsyrk_ozaki.argtypes = [ctypes.c_char, ctypes.c_char, L, L, ctypes.c_double, P, L, ctypes.c_double, P, L,
+                                   ctypes.c_int]
+    n = k = 8192
+    oz = {}
+    ref_lib = None
+    so = os.path.join(ROOT, "oracle", "_ref", "libTensorBLAS_ref.so")
+    if os.path.exists(so):
+        ref_lib = ctypes.CDLL(so)
+        ref_lib.ref_time_ozimmu_syrk.argtypes = [L, L, L, P, ctypes.c_int, ctypes.c_int]
+        ref_lib.ref_time_ozimmu_syrk.restype = ctypes.c_double
+    for phi, slices in ((0.5, 8), (2.0, 9)):
+        g = np.random.Generator(np.random.PCG64(17))
+        Ah = g.standard_normal((n, k)) * np.exp(phi * g.standard_normal((n, k)))
+        dA = torch.from_numpy(np.ascontiguousarray(Ah.T)).cuda()
+        dC = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+        run = lambda: TB._check(lib.tb_dsyrk_ozaki(b"L", b"N", n, k, 1.0, dA.data_ptr(), n, 0.0,  # noqa: E731
+                                                   dC.data_ptr(), n, slices))
+        ms = _median_ms(run, 5)
+        Ch = dC.cpu().numpy().T
+        r = g.integers(0, n, 3000)
+        c = g.integers(0, n, 3000)
+        lo, hi = np.maximum(r, c), np.minimum(r, c)
+        ex = orc.syrk_extended(Ah, lo, hi)
+        d = np.abs(Ch[lo, hi] - ex).astype(np.float64)
+        entry = {"slices": slices, "ms": ms, "tflops_eff": float(n) ** 2 * k / (ms * 1e-3) / 1e12,
+                 "normwise_err_vs_long_double": float(np.linalg.norm(d) / np.linalg.norm(ex.astype(np.float64)))}
+        if ref_lib is not None:
+            t_ref = ref_lib.ref_time_ozimmu_syrk(n, k, 256, np.asfortranarray(Ah).ctypes.data_as(P), 1, 3)
+            entry["reference_native_fp64_ms"] = t_ref
+            entry["speedup_vs_native_fp64"] = t_ref / ms if t_ref > 0 else None
+        oz[f"phi={phi}"] = entry
+        del dA, dC
+    res["dsyrk_ozaki_8192"] = oz
+    torch.cuda.empty_cache()
+    # ---- 512 uneven instances, grouped batch (split) vs per-instance loop (plain)
+    g = np.random.Generator(np.random.PCG64(2025))
+    ns = np.round(np.exp(g.uniform(np.log(64), np.log(2048), 512))).astype(int)
+    kinds, As, BC, B0 = [], [], [], []
+    flops = 0.0
+    for i, m in enumerate(ns):
+        if i % 2 == 0:
+            a = torch.rand(m, m, device="cuda") * 2 - 1
+            bc = torch.zeros(m, m, device="cuda")
+        else:
+            lt = torch.tril(torch.rand(m, m, device="cuda") * 2 - 1, -1) / m ** 0.5
+            a = (lt + torch.diag(torch.rand(m, device="cuda") + 1)).t().contiguous()
+            bc = torch.rand(m, m, device="cuda") * 2 - 1
+        kinds.append(i % 2)
+        As.append(a)
+        BC.append(bc)
+        B0.append(bc.clone())
+        flops += float(m) ** 3
+    restore = lambda: [b.copy_(b0) for b, b0 in zip(BC, B0)]  # noqa: E731
+    batch = TB.Batch(kinds, As, BC, precision=TB.SPLIT)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        batch.run()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        batch.run()
+    ms_graph = _median_ms(graph.replay, 5, restore)
+
+    def loop():
+        for kind, a, bc, m in zip(kinds, As, BC, ns):
+            if kind == 0:
+                TB.ssyrk(a, bc, m, m, m, m, 1.0, 0.0, "N", 256, TB.PLAIN)
+            else:
+                TB.strsm("R", a, bc, m, m, m, m, 512, TB.PLAIN)
+
+    ms_loop = _median_ms(loop, 3, restore)
+    res["batched_512_uneven"] = {"instances": 512, "flops_sum_n3": flops, "grouped_split_graph_ms": ms_graph,
+                                 "grouped_split_tflops": flops / (ms_graph * 1e-3) / 1e12,
+                                 "per_instance_plain_loop_ms": ms_loop,
+                                 "per_instance_plain_loop_tflops": flops / (ms_loop * 1e-3) / 1e12}
+    del graph
+    batch.close()
+    return res
 
 
 def run_reference(args, world, rank, local):
@@ -376,9 +500,28 @@ def run_reference(args, world, rank, local):
     }
 
 
+def profile_step(args):
+    """One plain and one split step on fresh inputs, nothing timed (the
+    command the committed ncu summaries were captured from)."""
+    import TensorBLAS as TB
+
+    n = args.n
+    A, T, B0 = make_inputs(n)
+    C = torch.zeros(n, n, device="cuda")
+    for prec in (TB.PLAIN, TB.SPLIT):
+        Bw = B0.clone()
+        TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, prec)
+        TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, prec)
+        TB.synchronize()
+    print("profile step done", flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.profile_step:
+        profile_step(args)
+        return
     try:
         line = run_mine(args, world, rank, local) if args.impl == "mine" else run_reference(args, world, rank, local)
         if rank == 0 and line is not None:

@@ -87,4 +87,9 @@ TB_API void tc_symm(cublasHandle_t handle, long int m, long int n, float alpha, 
 TB_API void tc_cumpsgemm_symm(cumpsgemm::handle_t cumpsgemm_handle, long int m, long int n, float alpha, float* A,
                               long int lda, float* B, int ldb, float beta, float* C, long int ldc);
 
+/* include/TensorBLAS.h:143 — FP64 SYRK, here on the INT8 tensor cores
+ * (Ozaki scheme, 10 slices; see tb_dsyrk_ozaki). nb is accepted and unused. */
+TB_API void tc_ozimmu_syrk(cublasHandle_t handle, long int n, long int k, double alpha, double* A, long int lda,
+                           double beta, double* C, long int ldc, long int nb);
+
 #endif /* TENSORBLAS_B200_H_ */

@@ -128,6 +128,44 @@ TB_API tb_status tb_ssymm(char uplo, long m, long n, float alpha, const float* A
 TB_API tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
                                   float beta, float* C, long ldc, long nb, int precision);
 
+/*
+ * FP64 SYRK on the INT8 tensor cores (Ozaki scheme): C = alpha A A^T + beta C,
+ * lower triangle, A n x k FP64 (trans 'N'). `slices` INT8 slices per element
+ * (1..14; <= 0 selects 10); every slice-pair product is exact (INT32), so the
+ * result is FP64-accurate once 7 * slices exceeds 53 bits plus the in-row
+ * exponent spread. Replaces tc_ozimmu_syrk (BLAS/tc_ozimmu_syrk.cu:108-143),
+ * which runs native FP64 cuBLAS GEMMs in the reference.
+ */
+TB_API tb_status tb_dsyrk_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
+                                double beta, double* C, long ldc, int slices);
+/* The slicing step alone: `slices` int8 planes Q[s][i][p] (row stride ldq,
+ * plane stride n * ldq, ldq a multiple of 16 and >= k rounded up to 16) and
+ * row exponents, exactly as tb_dsyrk_ozaki forms them. */
+TB_API tb_status tb_ozaki_slice(long n, long k, const double* A, long lda, int slices, signed char* Q, long ldq,
+                                int* exponents);
+/* The exact INT32 level product P_L = sum_{s+t=L} Q_s Q_t^T (lower triangle,
+ * column-major, ldp) that tb_dsyrk_ozaki folds into C, for checking. */
+TB_API tb_status tb_ozaki_level_product(long n, long k, const double* A, long lda, int slices, int level, int* P,
+                                        long ldp);
+
+/*
+ * Batched uneven instances (no reference counterpart: the reference loops
+ * over tc_syrk / tc_trsm, BLAS/tc_syrk.cu:126-157, BLAS/tc_trsm.cu:139-174).
+ * kind[i] = 0: SYRK, C_i(lower) = A_i A_i^T, A_i n_i x n_i, BC[i] = C_i.
+ * kind[i] = 1: TRSM, X_i A_i^T = B_i (A_i lower n_i x n_i), BC[i] = B_i,
+ *              overwritten by X_i (the reference's tc_trsm semantics).
+ * tb_batch_create plans everything (scratch, FP16 copies' layout, tile lists,
+ * per-problem descriptors); tb_batch_run enqueues a few grouped launches on
+ * the current stream, allocates nothing and does not synchronise (it may be
+ * captured in a CUDA graph); the pointers given at creation must stay valid.
+ * nb: TRSM leaf-block cap (<= 0: 512); precision as elsewhere.
+ */
+typedef struct tb_batch_s* tb_batch_t;
+TB_API tb_status tb_batch_create(tb_batch_t* batch, int count, const int* kind, const long* n, const float* const* A,
+                                 const long* lda, float* const* BC, const long* ldbc, long nb, int precision);
+TB_API tb_status tb_batch_run(tb_batch_t batch);
+TB_API tb_status tb_batch_destroy(tb_batch_t batch);
+
 /* Mirror lower -> upper of an n x n matrix (util/util.cu:148-157). */
 TB_API tb_status tb_ssymmetrize(long n, float* A, long lda);
 

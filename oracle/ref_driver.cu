@@ -201,3 +201,28 @@ double ref_time_trsm(long m, long n, long nb, const float* hA, const float* hB, 
 }
 
 }  // extern "C"
+
+extern "C" {
+// Median device time (ms) of the reference's tc_ozimmu_syrk (native FP64
+// cuBLAS in its recursion) on device-resident inputs.
+double ref_time_ozimmu_syrk(long n, long k, long nb, const double* hA, int warmup, int iters) {
+  double* A = up(hA, (size_t)n * k);
+  double* C = up<double>(nullptr, (size_t)n * n);
+  if (!A || !C) return -1.0;
+  Events ev;
+  std::vector<float> t;
+  for (int i = 0; i < warmup + iters; ++i) {
+    cudaEventRecord(ev.a);
+    tc_ozimmu_syrk(handle(), n, k, 1.0, A, n, 0.0, C, n, nb);
+    cudaEventRecord(ev.b);
+    cudaEventSynchronize(ev.b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev.a, ev.b);
+    if (i >= warmup) t.push_back(ms);
+  }
+  int rc = finish();
+  cudaFree(A);
+  cudaFree(C);
+  return rc ? -1.0 : median(t);
+}
+}  // extern "C"

@@ -96,18 +96,19 @@ bool make_half_out_map(CUtensorMap* map, __half* p, long long rows, long long co
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <class Cfg>
+template <class Cfg, bool GROUPED>
 tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    TB_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES));
+    TB_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<Cfg, GROUPED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     Cfg::SMEM_BYTES));
     attr_set[dev] = true;
   }
   int grid = num_tiles < sm_count() ? num_tiles : sm_count();
   void* tok = prof_begin(stream);
-  gemm_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(args);
+  gemm_kernel<Cfg, GROUPED><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(args);
   TB_CUDA_TRY(cudaGetLastError());
   prof_end(tok, stream, flops);
   note_launch();
@@ -118,11 +119,10 @@ tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t strea
 
 int gemm_bn(Split s) { return s == Split::kPlain ? 256 : 128; }
 
-tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
-  if (c.num_tiles <= 0) return TB_SUCCESS;
+tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
   const bool split = c.split == Split::kHiLo;
   const int bn = gemm_bn(c.split);
-  GemmArgs a;
+  GemmArgs& a = *out;
   memset(&a, 0, sizeof(a));
   TB_TRY(make_map(&a.mapA[0], c.a_hi, kGemmBM));
   TB_TRY(make_map(&a.mapB[0], c.b_hi, bn));
@@ -161,19 +161,54 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   if (c.a_hi.mn_major && (c.a_off % 8) != 0) return TB_ERROR_INVALID_VALUE;
   if (c.b_hi.mn_major && (c.b_off % 8) != 0) return TB_ERROR_INVALID_VALUE;
   if ((!c.a_hi.mn_major || !c.b_hi.mn_major) && (c.k_off % 8) != 0) return TB_ERROR_INVALID_VALUE;
+  return TB_SUCCESS;
+}
 
+tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
+  if (c.num_tiles <= 0) return TB_SUCCESS;
+  GemmArgs a;
+  TB_TRY(gemm_build_args(c, &a));
+  const bool split = c.split == Split::kHiLo;
   const bool amn = c.a_hi.mn_major, bmn = c.b_hi.mn_major;
   if (!split) {
-    if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>>(a, c.num_tiles, stream, c.flops);
-    if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>>(a, c.num_tiles, stream, c.flops);
-    if (!amn && !bmn) return launch_variant<GemmCfg<256, 1, false, false>>(a, c.num_tiles, stream, c.flops);
-    return launch_variant<GemmCfg<256, 1, false, true>>(a, c.num_tiles, stream, c.flops);
+    if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>, false>(a, c.num_tiles, stream, c.flops);
+    if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>, false>(a, c.num_tiles, stream, c.flops);
+    if (!amn && !bmn) return launch_variant<GemmCfg<256, 1, false, false>, false>(a, c.num_tiles, stream, c.flops);
+    return launch_variant<GemmCfg<256, 1, false, true>, false>(a, c.num_tiles, stream, c.flops);
   } else {
-    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true>>(a, c.num_tiles, stream, c.flops);
-    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false>>(a, c.num_tiles, stream, c.flops);
-    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>>(a, c.num_tiles, stream, c.flops);
-    return launch_variant<GemmCfg<128, 3, false, true>>(a, c.num_tiles, stream, c.flops);
+    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true>, false>(a, c.num_tiles, stream, c.flops);
+    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false>, false>(a, c.num_tiles, stream, c.flops);
+    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>, false>(a, c.num_tiles, stream, c.flops);
+    return launch_variant<GemmCfg<128, 3, false, true>, false>(a, c.num_tiles, stream, c.flops);
   }
+}
+
+// Kernel attributes of the grouped variants, set outside any stream capture.
+tb_status gemm_prepare_grouped() {
+  TB_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<GemmCfg<128, 3, true, true>, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<128, 3, true, true>::SMEM_BYTES));
+  TB_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<GemmCfg<256, 1, true, true>, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<256, 1, true, true>::SMEM_BYTES));
+  return TB_SUCCESS;
+}
+
+// Grouped launch over problems whose descriptors (built by gemm_build_args
+// and copied to the device) all use MN-major operands.
+tb_status gemm_launch_grouped(Split split, const GemmArgs* d_problems, const int4* d_tiles, const int* d_tile_prob,
+                              int num_tiles, double flops, cudaStream_t stream) {
+  if (num_tiles <= 0) return TB_SUCCESS;
+  GemmArgs a;
+  memset(&a, 0, sizeof(a));
+  a.tiles = d_tiles;
+  a.num_tiles = num_tiles;
+  a.problems = d_problems;
+  a.tile_prob = d_tile_prob;
+  a.corr_scale = 1.0f / 2048.0f;
+  a.kchunk = 2;
+  a.err = device_error_word();
+  if (split == Split::kHiLo)
+    return launch_variant<GemmCfg<128, 3, true, true>, true>(a, num_tiles, stream, flops);
+  return launch_variant<GemmCfg<256, 1, true, true>, true>(a, num_tiles, stream, flops);
 }
 
 // --------------------------------------------------------------------- plans

@@ -72,7 +72,22 @@ struct GemmArgs {
   int out_m, out_n;  // side copies only for rows < out_m and columns < out_n
   int tma_out;       // 1: side copies through mapOut (requires tma_c and tri == 0)
   int* err;
+  // Grouped launches: per-tile problem index into a device array of
+  // GemmArgs (64-byte aligned; their tensor maps are read from global memory).
+  const struct GemmArgs* problems;
+  const int* tile_prob;
 };
+
+// The problem a tile belongs to: the launch's own arguments, or (grouped
+// launches) one of the descriptors in global memory.
+template <bool GROUPED>
+__device__ __forceinline__ const GemmArgs& tile_problem(const GemmArgs& args, int t) {
+  if constexpr (GROUPED) {
+    return args.problems[args.tile_prob[t]];
+  } else {
+    return args;
+  }
+}
 
 template <int BN_, int NSPLIT_, bool A_MN_, bool B_MN_>
 struct GemmCfg {
@@ -169,9 +184,9 @@ struct EpiState {
 // hi/lo chunk (8 KB each) and the fp32 chunk is single-buffered.
 __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* stage, uint64_t* cload, EpiState& es,
                                                    const float* v, int m0, int gj0, int row, bool need_load,
-                                                   bool issuer, volatile int* abort_flag) {
-  const bool side_mode = args.tma_out != 0;
-  const bool side = side_mode && gj0 < args.out_n && m0 < args.out_m;
+                                                   bool issuer, volatile int* abort_flag, bool single_buffer) {
+  const bool side_mode = single_buffer || args.tma_out != 0;
+  const bool side = args.tma_out != 0 && gj0 < args.out_n && m0 < args.out_m;
   const int b = side_mode ? 0 : (es.chunk & 1);
   float* S = stage + b * (128 * 32);
   __half* Hs = reinterpret_cast<__half*>(stage + 128 * 32);
@@ -228,7 +243,7 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
   ++es.chunk;
 }
 
-template <class Cfg>
+template <class Cfg, bool GROUPED>
 __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ GemmArgs args) {
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
   extern __shared__ uint8_t smem_raw[];
@@ -260,7 +275,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
     *abort_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 0 && lane == 0) {
+  if (!GROUPED && warp == 0 && lane == 0) {
     tma_prefetch_map(&args.mapA[0]);
     tma_prefetch_map(&args.mapB[0]);
     if (Cfg::NSPLIT > 1) {
@@ -298,12 +313,13 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
           }
           mbar_arrive_expect_tx(&full[s], Cfg::STAGE_BYTES);
           uint8_t* st = smem + s * Cfg::STAGE_BYTES;
-          const int k = args.k_off + kb * BK;
+          const GemmArgs& P = tile_problem<GROUPED>(args, t);
+          const int k = P.k_off + kb * BK;
 #pragma unroll
           for (int h = 0; h < Cfg::NOPS; ++h) {
-            load_operand<Cfg::A_MN, BM>(st + h * Cfg::A_BYTES, &args.mapA[h], &full[s], args.a_off + tile.x, k);
-            load_operand<Cfg::B_MN, BN>(st + Cfg::NOPS * Cfg::A_BYTES + h * Cfg::B_BYTES, &args.mapB[h], &full[s],
-                                        args.b_off + tile.y, k);
+            load_operand<Cfg::A_MN, BM>(st + h * Cfg::A_BYTES, &P.mapA[h], &full[s], P.a_off + tile.x, k);
+            load_operand<Cfg::B_MN, BN>(st + Cfg::NOPS * Cfg::A_BYTES + h * Cfg::B_BYTES, &P.mapB[h], &full[s],
+                                        P.b_off + tile.y, k);
           }
           issued_mask |= 1u << s;
           phase_mask = (phase_mask & ~(1u << s)) | (ph << s);
@@ -407,10 +423,11 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
     bool ok = true;
     for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
       const int4 tile = args.tiles[t];
+      const GemmArgs& P = tile_problem<GROUPED>(args, t);
       const long long gi = (long long)tile.x + row;
-      const bool row_ok = gi < args.M;
+      const bool row_ok = gi < P.M;
       // the tile crosses the masked (upper) region: min(i - j) < diag
-      const bool tile_masked = args.tri && ((long long)tile.x - (long long)(tile.y + BN - 1)) < args.diag;
+      const bool tile_masked = P.tri && ((long long)tile.x - (long long)(tile.y + BN - 1)) < P.diag;
       if constexpr (Cfg::NSPLIT == 1) {
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -427,12 +444,12 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[buf]);
           }
-          if (args.tma_c) {
-            if (tile.y + c0 < args.N)
-              epilogue_chunk_tma(args, stage_c, cload, es, v, tile.x, tile.y + c0, row,
-                                 args.beta != 0.0f || tile_masked, issuer, abort_flag);
+          if (P.tma_c) {
+            if (tile.y + c0 < P.N)
+              epilogue_chunk_tma(P, stage_c, cload, es, v, tile.x, tile.y + c0, row, P.beta != 0.0f || tile_masked,
+                                 issuer, abort_flag, GROUPED);
           } else if (row_ok) {
-            epilogue_store32(args, v, gi, (long long)tile.y + c0);
+            epilogue_store32(P, v, gi, (long long)tile.y + c0);
           }
         }
       } else {
@@ -464,12 +481,12 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
         if (!ok) break;
 #pragma unroll
         for (int c0 = 0; c0 < BN; c0 += 32) {
-          if (args.tma_c) {
-            if (tile.y + c0 < args.N)
-              epilogue_chunk_tma(args, stage_c, cload, es, acc + c0, tile.x, tile.y + c0, row,
-                                 args.beta != 0.0f || tile_masked, issuer, abort_flag);
+          if (P.tma_c) {
+            if (tile.y + c0 < P.N)
+              epilogue_chunk_tma(P, stage_c, cload, es, acc + c0, tile.x, tile.y + c0, row,
+                                 P.beta != 0.0f || tile_masked, issuer, abort_flag, GROUPED);
           } else if (row_ok) {
-            epilogue_store32(args, acc + c0, gi, (long long)tile.y + c0);
+            epilogue_store32(P, acc + c0, gi, (long long)tile.y + c0);
           }
         }
       }

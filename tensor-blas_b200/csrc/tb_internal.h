@@ -88,6 +88,14 @@ constexpr int kGemmBK = 64;
 
 tb_status gemm_launch(const GemmCall& call, cudaStream_t stream);
 
+// Grouped launches: each problem's descriptor is built on the host by
+// gemm_build_args (tensor maps included), copied to a 64-byte aligned device
+// array, and every tile carries the index of its problem.
+struct GemmArgs;
+tb_status gemm_build_args(const GemmCall& c, GemmArgs* out);
+tb_status gemm_launch_grouped(Split split, const GemmArgs* d_problems, const int4* d_tiles, const int* d_tile_prob,
+                              int num_tiles, double flops, cudaStream_t stream);
+
 // Tile plans (host vectors of {m0, n0, kb_begin, kb_end}); uploaded and
 // cached on the device by `upload_tiles`.
 std::vector<int4> plan_rect(int M, int N, int bn, int kb0, int kb1);
@@ -102,6 +110,32 @@ const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
 //   tri == 3: zero the strict lower triangle.
 tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
                           long long ldd, float lo_scale, int tri, cudaStream_t stream);
+// ------------------------------------------------------------------ grouped TRSM pieces
+// 32x32 diagonal-block inverses of one triangular matrix: sub-blocks
+// [first, first + ceil(n/32)) of a grouped launch write D[0 ..].
+struct DiagJob {
+  const float* A;
+  long long lda;
+  long long n;
+  double* D;
+  long long first;
+};
+// One leaf inverse (rows/cols [s, s+size) of A) as FP16 hi/lo, column-major.
+struct ChainJob {
+  const float* A;
+  long long lda;
+  int s, size;
+  const double* D;  // the instance's 32x32 inverses
+  __half* Whi;
+  __half* Wlo;
+  long long ldw;
+};
+tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblocks, const ChainJob* d_chain,
+                                int nchain, cudaStream_t st);
+// One-time kernel attribute set-up for the grouped launches (not capturable).
+tb_status gemm_prepare_grouped();
+tb_status trsm_prepare_grouped();
+
 // C(lower) *= beta (C = 0 when beta == 0).
 tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st);
 // Full symmetric FP16 copy of an n x n matrix with one stored triangle.

@@ -36,10 +36,9 @@ constexpr int kLeafMax = 512;  // largest diagonal block inverted explicitly
 // the identity). One warp per sub-block; lane c owns column c of the inverse
 // and runs forward substitution in FP64 registers; rows of L are broadcast
 // from shared memory. Output: D[t*1024 + i + 32*c] (column-major 32x32).
-__global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const float* __restrict__ A, long long lda,
-                                                        double* __restrict__ D) {
+__device__ __forceinline__ void diag_inv32_body(long long n, const float* __restrict__ A, long long lda,
+                                                double* __restrict__ D, long long t) {
   __shared__ double L[32][33];
-  const long long t = blockIdx.x;
   const int c = threadIdx.x;
   const long long base = t * 32;
   for (int i = 0; i < 32; ++i) {
@@ -64,6 +63,27 @@ __global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const float
   for (int i = 0; i < 32; ++i) D[t * 1024 + i + 32 * c] = w[i];
 }
 
+__global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const float* __restrict__ A, long long lda,
+                                                        double* __restrict__ D) {
+  diag_inv32_body(n, A, lda, D, blockIdx.x);
+}
+
+// Grouped form: block b belongs to the job whose [first, first + count)
+// range of sub-blocks holds b (jobs sorted by `first`).
+__global__ void __launch_bounds__(32) diag_inv32_grouped_kernel(const DiagJob* __restrict__ jobs, int njobs) {
+  int lo = 0, hi = njobs - 1;
+  const long long b = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (jobs[mid].first <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const DiagJob& jb = jobs[lo];
+  diag_inv32_body(jb.n, jb.A, jb.lda, jb.D, b - jb.first);
+}
+
 // Column chain j of the inverse of leaf block b (rows/cols [s, s+size)):
 //   W[i][j] = -Dinv_i * sum_{p=j}^{i-1} L[i][p] W[p][j]   (32x32 sub-blocks)
 // The 32-wide column panel of W lives in shared memory (FP64). Each 32x32
@@ -74,18 +94,13 @@ __global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const float
 // leading dimension ldw, zeros above the diagonal.
 constexpr int kChainThreads = 128;
 
-__global__ void __launch_bounds__(kChainThreads) trtri_chain_kernel(const float* __restrict__ A, long long lda,
-                                                                    const int2* __restrict__ leaves,
-                                                                    const double* __restrict__ D,
-                                                                    __half* __restrict__ Whi, __half* __restrict__ Wlo,
-                                                                    long long ldw, long long wstride) {
+__device__ __forceinline__ void trtri_chain_body(const float* __restrict__ A, long long lda, int s, int size,
+                                                 const double* __restrict__ D, __half* __restrict__ hi,
+                                                 __half* __restrict__ lo, long long ldw, int j) {
   extern __shared__ __align__(16) double sm[];
   __shared__ __align__(16) double LsT[32][34];  // LsT[k][r] = L(r, k) of the staged sub-block (or Dinv_i)
   __shared__ __align__(16) double Ts[32][36];   // Ts[k][c]
-  const int2 leaf = leaves[blockIdx.y];  // {s, size}
-  const int s = leaf.x, size = leaf.y;
   const int nsub = (size + 31) / 32;
-  const int j = blockIdx.x;
   if (j >= nsub) return;
   double* Wp = sm;  // [(nsub - j) * 32][32]: Wp[row * 32 + col], row relative to 32j
   const int tid = threadIdx.x;
@@ -157,8 +172,6 @@ __global__ void __launch_bounds__(kChainThreads) trtri_chain_kernel(const float*
     __syncthreads();
   }
   // write the 32 columns [32j, 32j+32) of W for all rows of the leaf
-  __half* hi = Whi + (long long)blockIdx.y * wstride;
-  __half* lo = Wlo + (long long)blockIdx.y * wstride;
   for (int q = 0; q < 8; ++q) {
     const int c = lc + 4 * q;
     const int gc = 32 * j + c;
@@ -171,6 +184,22 @@ __global__ void __launch_bounds__(kChainThreads) trtri_chain_kernel(const float*
       lo[row + (long long)gc * ldw] = __float2half_rn((float)((v - (double)__half2float(h)) * 2048.0));
     }
   }
+}
+
+__global__ void __launch_bounds__(kChainThreads) trtri_chain_kernel(const float* __restrict__ A, long long lda,
+                                                                    const int2* __restrict__ leaves,
+                                                                    const double* __restrict__ D,
+                                                                    __half* __restrict__ Whi, __half* __restrict__ Wlo,
+                                                                    long long ldw, long long wstride) {
+  const int2 leaf = leaves[blockIdx.y];  // {s, size}
+  trtri_chain_body(A, lda, leaf.x, leaf.y, D, Whi + (long long)blockIdx.y * wstride,
+                   Wlo + (long long)blockIdx.y * wstride, ldw, blockIdx.x);
+}
+
+// Grouped form: one job per (instance, leaf) along blockIdx.y.
+__global__ void __launch_bounds__(kChainThreads) trtri_chain_grouped_kernel(const ChainJob* __restrict__ jobs) {
+  const ChainJob& jb = jobs[blockIdx.y];
+  trtri_chain_body(jb.A, jb.lda, jb.s, jb.size, jb.D, jb.Whi, jb.Wlo, jb.ldw, blockIdx.x);
 }
 
 struct TrsmCtx {
@@ -315,6 +344,37 @@ tb_status recurse(TrsmCtx& c, long s, long e, const std::vector<long>& leaf_star
 
 }  // namespace
 
+tb_status trsm_prepare_grouped() {
+  TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kLeafMax / 32 * 1024 * sizeof(double))));
+  return TB_SUCCESS;
+}
+
+// Diagonal-block inverses of many triangular matrices in two launches.
+tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblocks, const ChainJob* d_chain,
+                                int nchain, cudaStream_t st) {
+  if (ndiag > 0 && nblocks > 0) {
+    diag_inv32_grouped_kernel<<<(unsigned)nblocks, 32, 0, st>>>(d_diag, ndiag);
+    TB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+  }
+  if (nchain > 0) {
+    static bool attr_done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !attr_done[dev]) {
+      TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(kLeafMax / 32 * 1024 * sizeof(double))));
+      attr_done[dev] = true;
+    }
+    const size_t smem = (size_t)(kLeafMax / 32) * 1024 * sizeof(double);
+    trtri_chain_grouped_kernel<<<dim3(kLeafMax / 32, (unsigned)nchain), kChainThreads, smem, st>>>(d_chain);
+    TB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+  }
+  return TB_SUCCESS;
+}
+
 tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float* B, long ldb, long nb, Split split,
                     cudaStream_t st) {
   if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
@@ -328,12 +388,16 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   c.nt = nt;
   c.B = B;
   c.ldb = ldb;
-  c.split = split;
+  // The reference's chunk planner (util/mat_size.cu:31-55) sends an order
+  // below 2048 to FP32 cublasStrsm with no FP16 step at all
+  // (BLAS/tc_trsm.cu:103-112); the plain form keeps that accuracy contract
+  // by using the FP32-accurate split products for such orders.
+  c.split = (split == Split::kPlain && nt < 2048) ? Split::kHiLo : split;
   c.st = st;
   long leaf = round_up(std::min<long>(nb, kLeafMax), 64);
   if (leaf > kLeafMax) leaf = kLeafMax;
   c.leaf = (int)leaf;
-  const bool hilo = split == Split::kHiLo;
+  const bool hilo = c.split == Split::kHiLo;
 
   std::vector<long> leaf_start;
   std::vector<int2> leaves;

@@ -205,3 +205,56 @@ def symm(A, B, alpha=1.0, beta=0.0, C=None, uplo="L", precision=PLAIN):
 
 def synchronize():
     _check(lib.tb_synchronize())
+
+
+# ---------------------------------------------------------------- batched uneven instances
+lib.tb_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_void_p),
+                                ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_void_p),
+                                ctypes.POINTER(ctypes.c_long), ctypes.c_long, ctypes.c_int]
+lib.tb_batch_create.restype = ctypes.c_int
+lib.tb_batch_run.argtypes = [ctypes.c_void_p]
+lib.tb_batch_run.restype = ctypes.c_int
+lib.tb_batch_destroy.argtypes = [ctypes.c_void_p]
+lib.tb_batch_destroy.restype = ctypes.c_int
+
+SYRK_KIND, TRSM_KIND = 0, 1
+
+
+class Batch:
+    """Many independent SYRK / TRSM instances run by a few grouped launches.
+
+    kinds[i] = SYRK_KIND: C_i(lower) = A_i A_i^T; BC[i] is C_i.
+    kinds[i] = TRSM_KIND: X_i A_i^T = B_i with A_i lower; BC[i] is B_i (overwritten).
+    A[i], BC[i] are float32 CUDA tensors holding column-major n_i x n_i storage;
+    they must stay alive while the batch exists. run() may be captured in a
+    CUDA graph.
+    """
+
+    def __init__(self, kinds, A, BC, nb=0, precision=SPLIT):
+        count = len(kinds)
+        self._keep = (list(A), list(BC))
+        n = [int(round(a.numel() ** 0.5)) for a in A]
+        k_arr = (ctypes.c_int * count)(*kinds)
+        n_arr = (ctypes.c_long * count)(*n)
+        a_arr = (ctypes.c_void_p * count)(*[a.data_ptr() for a in A])
+        bc_arr = (ctypes.c_void_p * count)(*[b.data_ptr() for b in BC])
+        ld = (ctypes.c_long * count)(*[max(v, 1) for v in n])
+        self.handle = ctypes.c_void_p()
+        _check(lib.tb_batch_create(ctypes.byref(self.handle), count, k_arr, n_arr, a_arr, ld, bc_arr, ld, nb,
+                                   precision))
+
+    def run(self):
+        lib.tb_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        _check(lib.tb_batch_run(self.handle))
+
+    def close(self):
+        if self.handle:
+            lib.tb_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

@@ -138,3 +138,71 @@ def test_trsm_model_vs_reference(name):
     assert nrm <= 2e-5
     if leaf != n:
         assert nrm < 0.2 * nrm_exact
+
+
+# ------------------------------------------------------------------ SYR2K / TRMM / SYMM / FP64 SYRK
+def test_syr2k_model_vs_reference():
+    z, meta = load("syr2k_small")
+    n, k = meta["n"], meta["k"]
+    A = gi.uniform(meta["seed"], (n, k))
+    B = gi.uniform(meta["seed"] + 1, (n, k))
+    model = orc.syr2k_model(A, B)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    _, nrm = orc.rel_errors(z["C"].astype(np.float64), model, low)
+    assert nrm <= 1e-6 + 1e-8 * 2 * k, nrm
+
+
+def test_syr2k_model_vs_reference_recursive_path():
+    z, meta = load("syr2k_p2")
+    n, k = meta["n"], meta["k"]
+    A = gi.uniform(meta["seed"], (n, k))
+    B = gi.uniform(meta["seed"] + 1, (n, k))
+    ha, hb = orc.h(A), orc.h(B)
+    r, c = z["rows"], z["cols"]
+    model = np.einsum("ij,ij->i", ha[r], hb[c]) + np.einsum("ij,ij->i", hb[r], ha[c])
+    scale = np.einsum("ij,ij->i", np.abs(ha[r]), np.abs(hb[c])) + np.einsum("ij,ij->i", np.abs(hb[r]), np.abs(ha[c]))
+    assert np.all(np.abs(z["vals"] - model) <= (2e-6 + 2e-8 * 2 * k) * scale + 1e-30)
+
+
+@pytest.mark.parametrize("name", ["trmm_small", "trmm_p2"])
+def test_trmm_model_vs_reference(name):
+    z, meta = load(name)
+    m, n = meta["m"], meta["n"]
+    A = np.tril(gi.uniform(meta["seed"], (m, m)))
+    B = gi.uniform(meta["seed"] + 1, (m, n))
+    model = orc.trmm_model(A, B)
+    _, nrm = orc.rel_errors(z["C"].astype(np.float64), model)
+    assert nrm <= 1e-6 + 1e-8 * m, nrm
+
+
+def test_symm_model_vs_reference():
+    z, meta = load("symm_small")
+    m = meta["m"]
+    A = gi.uniform(meta["seed"], (m, m))
+    B = gi.uniform(meta["seed"] + 1, (m, m))
+    model = orc.symm_model(A, B, lower=True)
+    _, nrm = orc.rel_errors(z["C"].astype(np.float64), model)
+    assert nrm <= 1e-6 + 1e-8 * m, nrm
+
+
+def test_fp64_syrk_reference_vs_extended_oracle():
+    """The reference's tc_ozimmu_syrk (native FP64 cuBLAS) against long double."""
+    z, meta = load("dsyrk_small")
+    n, k = meta["n"], meta["k"]
+    g = gi.rng(meta["seed"])
+    A = g.standard_normal((n, k)) * np.exp(meta["phi"] * g.standard_normal((n, k)))
+    r, c = np.tril_indices(n)
+    ex = orc.syrk_extended(A, r, c)
+    d = (z["C"][r, c] - ex).astype(np.float64)
+    assert np.linalg.norm(d) / np.linalg.norm(ex.astype(np.float64)) <= 1e-15
+
+
+def test_ozaki_slicing_reconstructs_exactly():
+    """sum_s q_s 2^-7s 2^e reproduces A to within 2^-7S of each row's scale."""
+    g = gi.rng(5)
+    A = g.standard_normal((40, 70)) * np.exp(2.0 * g.standard_normal((40, 70)))
+    for S in (4, 8, 14):
+        Q, e = orc.ozaki_slices(A, S)
+        rec = sum(Q[s].astype(np.float64) * 2.0 ** (-7 * (s + 1)) for s in range(S)) * np.ldexp(1.0, e)[:, None]
+        assert np.all(np.abs(rec - A) <= np.ldexp(1.0, e)[:, None] * 2.0 ** (-7 * S))
+        assert np.abs(Q).max() <= 127
