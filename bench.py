@@ -33,7 +33,7 @@ METRIC = "SYRK/TRSM n=16384 eff. TFLOP/s at stated FP64-oracle error, chosen vs 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["mine", "reference"], default="mine")
     p.add_argument("--n", type=int, default=16384)
@@ -99,7 +99,7 @@ class Clocks:
         self.proc = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -210,7 +210,7 @@ def run_mine(args, world, rank, local):
         TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, prec)
         TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, prec)
 
-    def timed(prec, steps, warmup, profile=False, clocks=None):
+    def timed(prec, steps, warmup, profile=False):
         for _ in range(warmup):
             Bw.copy_(B0)
             step(prec)
@@ -218,7 +218,6 @@ def run_mine(args, world, rank, local):
         barrier(world)
         torch.cuda.synchronize()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        sampler = Clocks(physical_gpu(local)) if clocks else None
         l0 = TB.lib.tb_launch_count()
         if profile:
             TB.lib.tb_profile_begin()
@@ -234,23 +233,23 @@ def run_mine(args, world, rank, local):
             ms, fl, cnt = TB.ctypes.c_double(), TB.ctypes.c_double(), TB.ctypes.c_long()
             TB.lib.tb_profile_end(TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
             prof = (ms.value, fl.value, cnt.value)
-        clk = sampler.stop() if sampler else None
         barrier(world)
         TB.synchronize()
         ms_total = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-        return ms_total, launches, prof, clk
+        return ms_total, launches, prof
 
 
-    # ---- plain (headline)
-    ms_plain, launches, prof, clk = timed(TB.PLAIN, args.steps, args.warmup, profile=True, clocks=True)
+    # ---- plain (headline), then chosen (split); clocks sampled over both timed regions
+    sampler = Clocks(physical_gpu(local))
+    ms_plain, launches, prof = timed(TB.PLAIN, args.steps, args.warmup, profile=True)
+    ms_split, _, _ = timed(TB.SPLIT, args.steps, args.warmup)
+    clk = sampler.stop()
     ms_plain = max_over_ranks(ms_plain, world)
+    ms_split = max_over_ranks(ms_split, world)
     Bw.copy_(B0)
     step(TB.PLAIN)
     TB.synchronize()
     err_plain = fp64_errors(n, A, C, T, B0, Bw) if rank == 0 else None
-    # ---- chosen (split)
-    ms_split, _, _, _ = timed(TB.SPLIT, args.steps, args.warmup)
-    ms_split = max_over_ranks(ms_split, world)
     Bw.copy_(B0)
     step(TB.SPLIT)
     TB.synchronize()
@@ -350,10 +349,103 @@ def _median_ms(fn, reps, prep=None):
     return float(np.median(out))
 
 
+def blas3_config(TB, ref_lib):
+    """SYR2K n=16384 k=4096, TRMM left/upper m=n=16384 and SYMM left/lower
+    m=n=16384 with entries N(0,1) * 2^U(-8,8): plain and split, each with a
+    sampled FP64 error, beside the reference's tc_syr2k / tc_trmm / tc_symm
+    on inputs of the same shape (its TRMM is lower-only; the flops are the
+    same). Flop conventions: SYR2K 2 n^2 k, TRMM m^2 n, SYMM 2 m^2 n."""
+    import ctypes
+
+    lib = TB.lib
+    P = ctypes.c_void_p
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(99)
+    rng = np.random.Generator(np.random.PCG64(99))
+
+    def draw(r, c):  # torch (r, c) = column-major c x r matrix
+        x = torch.randn(r, c, device="cuda", generator=gen)
+        return x * torch.exp2(torch.rand(r, c, device="cuda", generator=gen) * 16 - 8)
+
+    def err(got, ref):
+        d = np.abs(got - ref)
+        return float(np.linalg.norm(d) / np.linalg.norm(ref))
+
+    out = {}
+    n, k = 16384, 4096
+    # SYR2K: A, B n x k column-major (torch (k, n)); C lower
+    A, B = draw(k, n), draw(k, n)
+    C = torch.zeros(n, n, device="cuda")
+    Ah, Bh = A.cpu().numpy().astype(np.float64), B.cpu().numpy().astype(np.float64)
+    i = rng.integers(0, n, 256)
+    j = rng.integers(0, n, 256)
+    lo, hi = np.maximum(i, j), np.minimum(i, j)
+    ref = np.einsum("pk,pk->k", Ah[:, lo], Bh[:, hi]) + np.einsum("pk,pk->k", Bh[:, lo], Ah[:, hi])
+    entry = {"n": n, "k": k, "flops": 2.0 * n * n * k}
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split")):
+        run = lambda: TB._check(lib.tb_ssyr2k(b"L", b"N", n, k, 1.0, A.data_ptr(), n, B.data_ptr(), n,  # noqa: E731
+                                              0.0, C.data_ptr(), n, 256, prec))
+        ms = _median_ms(run, 5)
+        got = C.cpu().numpy()[hi, lo].astype(np.float64)
+        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "err_vs_fp64": err(got, ref)}
+    if ref_lib is not None:
+        t = ref_lib.ref_time_syr2k(n, k, 256, A.cpu().numpy().ctypes.data_as(P), B.cpu().numpy().ctypes.data_as(P),
+                                   1, 3)
+        entry["reference_plain_ms"] = t
+        entry["speedup_plain_vs_reference"] = t / entry["plain"]["ms"] if t > 0 else None
+    out["syr2k"] = entry
+    del A, B, C, Ah, Bh
+    torch.cuda.empty_cache()
+
+    m = n = 16384
+    A, B = draw(m, m), draw(n, m)  # A m x m (upper part read), B m x n, column-major
+    C = torch.zeros(n, m, device="cuda")
+    An, Bn = A.cpu().numpy(), B.cpu().numpy()  # An[p, i] = A(i, p); Bn[j, p] = B(p, j)
+    i = rng.integers(0, m, 128)
+    j = rng.integers(0, n, 128)
+    # TRMM upper: C(i, j) = sum_{p >= i} A(i, p) B(p, j)
+    ref = np.array([np.dot(An[ii:, ii].astype(np.float64), Bn[jj, ii:].astype(np.float64)) for ii, jj in zip(i, j)])
+    entry = {"m": m, "n": n, "uplo": "U", "flops": float(m) * m * n}
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split")):
+        run = lambda: TB._check(lib.tb_strmm(b"U", m, n, 1.0, A.data_ptr(), m, B.data_ptr(), m,  # noqa: E731
+                                             C.data_ptr(), m, 256, prec))
+        ms = _median_ms(run, 5)
+        got = C.cpu().numpy()[j, i].astype(np.float64)
+        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "err_vs_fp64": err(got, ref)}
+    if ref_lib is not None:
+        t = ref_lib.ref_time_trmm(m, n, 256, An.ctypes.data_as(P), Bn.ctypes.data_as(P), 1, 3)
+        entry["reference_plain_ms"] = t
+        entry["reference_note"] = "reference tc_trmm is lower-only: timed on a lower operand of the same size"
+        entry["speedup_plain_vs_reference"] = t / entry["plain"]["ms"] if t > 0 else None
+    out["trmm"] = entry
+    # SYMM lower: C(i, j) = sum_p A(i, p) B(p, j), A(i, p) = A(max, min) from the lower triangle
+    ref = []
+    for ii, jj in zip(i, j):
+        row = np.concatenate([An[:ii + 1, ii], An[ii, ii + 1:]]).astype(np.float64)
+        ref.append(np.dot(row, Bn[jj, :].astype(np.float64)))
+    ref = np.array(ref)
+    entry = {"m": m, "n": n, "uplo": "L", "flops": 2.0 * m * m * n}
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split")):
+        run = lambda: TB._check(lib.tb_ssymm(b"L", m, n, 1.0, A.data_ptr(), m, B.data_ptr(), m, 0.0,  # noqa: E731
+                                             C.data_ptr(), m, prec))
+        ms = _median_ms(run, 5)
+        got = C.cpu().numpy()[j, i].astype(np.float64)
+        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "err_vs_fp64": err(got, ref)}
+    if ref_lib is not None:
+        t = ref_lib.ref_time_symm(m, n, An.ctypes.data_as(P), Bn.ctypes.data_as(P), 1, 3)
+        entry["reference_plain_ms"] = t
+        entry["speedup_plain_vs_reference"] = t / entry["plain"]["ms"] if t > 0 else None
+    out["symm"] = entry
+    del A, B, C
+    torch.cuda.empty_cache()
+    return out
+
+
 def other_configs(TB):
     """The other configurations of the hot path, one measurement each:
     SYRK n=k=4096 (plain, the CPU-runnable case), FP64 DSYRK n=k=8192 by
-    Ozaki-INT8 vs the reference's native-FP64 tc_ozimmu_syrk, and 512 uneven
+    Ozaki-INT8 vs the reference's native-FP64 tc_ozimmu_syrk, SYR2K / TRMM /
+    SYMM at 16384 vs the reference's tc_* forms, and 512 uneven
     SYRK/TRSM instances as one grouped batch vs a per-instance plain loop."""
     import ctypes
 
@@ -405,6 +497,13 @@ def other_configs(TB):
         del dA, dC
     res["dsyrk_ozaki_8192"] = oz
     torch.cuda.empty_cache()
+    if ref_lib is not None:
+        for name in ("ref_time_syr2k", "ref_time_trmm"):
+            getattr(ref_lib, name).argtypes = [L, L, L, P, P, ctypes.c_int, ctypes.c_int]
+            getattr(ref_lib, name).restype = ctypes.c_double
+        ref_lib.ref_time_symm.argtypes = [L, L, P, P, ctypes.c_int, ctypes.c_int]
+        ref_lib.ref_time_symm.restype = ctypes.c_double
+    res["syr2k_trmm_symm_16384"] = blas3_config(TB, ref_lib)
     # ---- 512 uneven instances, grouped batch (split) vs per-instance loop (plain)
     g = np.random.Generator(np.random.PCG64(2025))
     ns = np.round(np.exp(g.uniform(np.log(64), np.log(2048), 512))).astype(int)
@@ -482,6 +581,12 @@ def run_reference(args, world, rank, local):
     clk = sampler.stop()
     if t_syrk <= 0 or t_trsm <= 0:
         return {"impl": "reference", "unavailable": "reference routine failed on this device"}
+    # end to end through the reference's public API: the same host <-> device
+    # bytes per step as the library's own e2e measurement
+    lib.ref_time_e2e.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, P, P, P, ctypes.c_int, ctypes.c_int]
+    lib.ref_time_e2e.restype = ctypes.c_double
+    t_e2e = lib.ref_time_e2e(n, args.nb_syrk, args.nb_trsm, hA.ctypes.data_as(P), hT.ctypes.data_as(P),
+                             hB.ctypes.data_as(P), 1, args.e2e_steps)
     ms = t_syrk + t_trsm
     value = 2.0 * float(n) ** 3 / (ms * 1e-3) / 1e12
     return {
@@ -495,7 +600,10 @@ def run_reference(args, world, rank, local):
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": 1, "kind": "reference",
                          "sample": "the reference library itself (oracle/_ref, built from its sources for sm_100a; "
                                    "its path is GPU code on cuBLAS) timed on this B200"},
-        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": ({"value": 2.0 * float(n) ** 3 / (t_e2e * 1e-3) / 1e12, "unit": "TFLOP/s",
+                 "steps": args.e2e_steps, "h2d_bytes_per_step": 3 * n * n * 4, "d2h_bytes_per_step": 2 * n * n * 4,
+                 "api": "tc_syrk / tc_trsm with cudaMemcpyAsync from/to page-locked host buffers"}
+                if t_e2e > 0 else {"value": None, "unit": "TFLOP/s", "note": "end-to-end run failed"}),
         "clocks": clk,
     }
 

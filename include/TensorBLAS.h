@@ -92,4 +92,22 @@ TB_API void tc_cumpsgemm_symm(cumpsgemm::handle_t cumpsgemm_handle, long int m, 
 TB_API void tc_ozimmu_syrk(cublasHandle_t handle, long int n, long int k, double alpha, double* A, long int lda,
                            double beta, double* C, long int ldc, long int nb);
 
+/* include/TensorBLAS.h:151 — FP64 TRSM X A^T = B (right/lower/transpose/
+ * non-unit), B overwritten; Ozaki-scheme updates and FP64 leaf inverses of
+ * nb (<= 512) columns (see tb_dtrsm_ozaki). */
+TB_API void tc_ozimmu_trsm(cublasHandle_t handle, long int m, long int n, double* A, long int lda, double* B,
+                           long int ldb, long int nb);
+
+/* include/TensorBLAS.h:157 — FP64 TRMM C = alpha A B, A lower, left side,
+ * out of place; the strict upper triangle of A is never read (see
+ * tb_dtrmm_ozaki). nb is accepted and unused. */
+TB_API void tc_ozimmu_trmm(cublasHandle_t handle, long int m, long int n, double alpha, double* A, long int lda,
+                           double* B, long int ldb, double* C, long int ldc, long int nb);
+
+/* include/TensorBLAS.h:163 — FP64 SYR2K, lower triangle of
+ * alpha (A B^T + B A^T) + beta C (see tb_dsyr2k_ozaki). nb is accepted and
+ * unused. */
+TB_API void tc_ozimmu_syr2k(cublasHandle_t handle, long int n, long int k, double alpha, double* A, long int lda,
+                            double* B, long int ldb, double beta, double* C, long int ldc, long int nb);
+
 #endif /* TENSORBLAS_B200_H_ */

@@ -129,15 +129,34 @@ TB_API tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, float a
                                   float beta, float* C, long ldc, long nb, int precision);
 
 /*
- * FP64 SYRK on the INT8 tensor cores (Ozaki scheme): C = alpha A A^T + beta C,
- * lower triangle, A n x k FP64 (trans 'N'). `slices` INT8 slices per element
- * (1..14; <= 0 selects 10); every slice-pair product is exact (INT32), so the
- * result is FP64-accurate once 7 * slices exceeds 53 bits plus the in-row
- * exponent spread. Replaces tc_ozimmu_syrk (BLAS/tc_ozimmu_syrk.cu:108-143),
- * which runs native FP64 cuBLAS GEMMs in the reference.
+ * FP64 routines on the INT8 tensor cores (Ozaki scheme). Each operand row is
+ * split into `slices` INT8 slices (1..14; <= 0 selects 10) under a per-row
+ * power-of-two exponent; every slice-pair product is exact (INT32, K chunked
+ * so the level sums cannot overflow), and the result is FP64-accurate once
+ * 7 * slices exceeds 53 bits plus the in-row exponent spread. The reference's
+ * tc_ozimmu_* drivers run native FP64 cuBLAS GEMMs instead.
+ *
+ * SYRK: C = alpha op(A) op(A)^T + beta C, lower triangle; A n x k ('N') or
+ * k x n ('T'). Replaces tc_ozimmu_syrk (BLAS/tc_ozimmu_syrk.cu:108-143).
  */
 TB_API tb_status tb_dsyrk_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
                                 double beta, double* C, long ldc, int slices);
+/* SYR2K: C = alpha (A B^T + B A^T) + beta C, lower triangle, A and B n x k
+ * (trans 'N'). Replaces tc_ozimmu_syr2k (BLAS/tc_ozimmu_syr2k.cu:97-123). */
+TB_API tb_status tb_dsyr2k_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
+                                 const double* B, long ldb, double beta, double* C, long ldc, int slices);
+/* TRMM (left, out of place): C = alpha op(A) B, A m x m lower ('L') or upper
+ * ('U'), the other triangle never read. Replaces tc_ozimmu_trmm
+ * (BLAS/tc_ozimmu_trmm.cu:118-149, lower). */
+TB_API tb_status tb_dtrmm_ozaki(char uplo, long m, long n, double alpha, const double* A, long lda, const double* B,
+                                long ldb, double* C, long ldc, int slices);
+/* TRSM, A lower-triangular non-unit, B overwritten by X:
+ *   side 'R': X A^T = B (A n x n, B m x n; tc_ozimmu_trsm,
+ *             BLAS/tc_ozimmu_trsm.cu:103-136)
+ *   side 'L': A X = B   (A m x m)
+ * Leaves of nb (<= 512) columns are multiplied by their FP64 inverses. */
+TB_API tb_status tb_dtrsm_ozaki(char side, long m, long n, const double* A, long lda, double* B, long ldb, long nb,
+                                int slices);
 /* The slicing step alone: `slices` int8 planes Q[s][i][p] (row stride ldq,
  * plane stride n * ldq, ldq a multiple of 16 and >= k rounded up to 16) and
  * row exponents, exactly as tb_dsyrk_ozaki forms them. */

@@ -232,6 +232,28 @@ def ozaki_syrk_model(A, S):
     return C
 
 
+def ozaki_gemm_model(A, B, S):
+    """The truncated Ozaki product of A (M x K) and B^T (B: N x K), each row
+    sliced under its own exponent: sum_{L=2}^{S+1} 2^(eA_i+eB_j-7L) P_L with
+    P_L = sum_{s+t=L} QA_s QB_t^T (long double). The FP64 SYR2K/TRMM/TRSM
+    products of the INT8 engine are this sum (per K chunk), folded in FP64."""
+    QA, ea = ozaki_slices(A, S)
+    QB, eb = ozaki_slices(B, S)
+    C = np.zeros((QA.shape[1], QB.shape[1]), dtype=np.longdouble)
+    scale = np.ldexp(np.longdouble(1.0), (ea[:, None] + eb[None, :]).astype(np.int64))
+    for L in range(2, S + 2):
+        P = np.zeros(C.shape, dtype=np.int64)
+        for s in range(max(1, L - S), min(S, L - 1) + 1):
+            P += QA[s - 1].astype(np.int64) @ QB[L - s - 1].astype(np.int64).T
+        C += P.astype(np.longdouble) * scale * np.ldexp(np.longdouble(1.0), -7 * L)
+    return C
+
+
+def gemm_extended(A, B):
+    """A B^T in long double (64-bit mantissa); A M x K, B N x K."""
+    return np.asarray(A, np.float64).astype(np.longdouble) @ np.asarray(B, np.float64).astype(np.longdouble).T
+
+
 def syrk_extended(A, rows, cols):
     """Entries (rows[i], cols[i]) of A A^T in long double (64-bit mantissa):
     the higher-than-FP64 oracle for the FP64-emulation checks."""

@@ -132,6 +132,37 @@ struct ChainJob {
 };
 tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblocks, const ChainJob* d_chain,
                                 int nchain, cudaStream_t st);
+// FP64 inverses of the diagonal leaf blocks {s, size} (s a multiple of 32,
+// size <= 512) of an FP64 lower-triangular matrix of order nt; W_b at
+// W + b * wstride, leading dimension ldw. D: (nt + 31) / 32 * 1024 doubles.
+tb_status trsm_leaf_inverses_f64(long nt, const double* A, long lda, const int2* d_leaves, int nleaf, int max_size,
+                                 double* D, double* W, long long ldw, long long wstride, cudaStream_t st);
+// FP32 TRSM with its triangular operand prepared once (FP16 copy, leaf
+// inverses) and applied to one or more right-hand-side blocks.
+struct TrsmCtx {
+  bool right;
+  long m, n;  // B is m x n
+  long nt;    // order of A (n for right, m for left)
+  float* B;
+  long ldb;
+  Split split;
+  int leaf;  // leaf block size (multiple of 64)
+  // FP16 copies
+  __half *ah, *al;  // A (nt x nt, MN-major, lda_h)
+  long long lda_h;
+  __half *xh, *xl;  // X: right: m x n col-major (ld ldx, MN-major operand)
+                    //    left : m x n col-major (ld ldx, K-major operand, rows = n)
+  long long ldx;
+  __half *wh, *wl;  // per-leaf inverses (ldw x leaf each)
+  long long ldw, wstride;
+  __half *rh, *rl;  // current leaf block of B
+  long long ldr;
+  cudaStream_t st;
+};
+tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long nb, Split split, cudaStream_t st,
+                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start);
+size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split);
+tb_status trsm_solve(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
 // One-time kernel attribute set-up for the grouped launches (not capturable).
 tb_status gemm_prepare_grouped();
 tb_status trsm_prepare_grouped();

@@ -17,6 +17,7 @@
 // FP64 C by the epilogue: C += alpha 2^(e_i+e_j-7L) P_L (one FP64 rounding per
 // level). Slices are stored K-major, one int8 plane per slice, so a single
 // 3-D tensor map (k, row, slice) feeds every pair.
+#include <algorithm>
 #include <climits>
 #include <cstring>
 #include <cstdio>
@@ -34,6 +35,7 @@ constexpr int kOzABytes = kOzBM * kOzBK, kOzBBytes = kOzBN * kOzBK;
 constexpr int kOzStageBytes = kOzABytes + kOzBBytes;
 constexpr int kOzSmem = kOzStages * kOzStageBytes + 1024 + 256;
 constexpr int kOzMaxSlices = 14;
+constexpr int kOzLeaf = 512;  // largest TRSM diagonal block inverted explicitly
 
 // kind::i8 instruction descriptor: c_format S32 (2), a/b_format signed int8 (1),
 // both K-major, N >> 3 at [17,23), M >> 4 at [24,29).
@@ -67,45 +69,58 @@ __device__ __forceinline__ void tmem_ld32_s32(uint32_t taddr, int* v) {
 }
 
 // ---------------------------------------------------------------- slicing
-// e[i] = max_p frexp-exponent(a_ip) (|a_ip| < 2^e[i]); e[] pre-set very negative.
-__global__ void __launch_bounds__(256) oz_rowexp_kernel(long long n, long long k, const double* __restrict__ A,
-                                                        long long lda, int* __restrict__ e) {
-  const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
-  if (i >= n) return;
-  int m = INT_MIN / 2;
-  for (long long p = blockIdx.y; p < k; p += gridDim.y) {
-    const double v = A[i + p * lda];
-    if (v != 0.0) {
-      int ex;
-      frexp(v, &ex);
-      m = ex > m ? ex : m;
-    }
+// An operand is a rows x k matrix whose row i is one K-vector:
+//   by rows (cols == 0): element (i, p) = X[i + p * ldx] (rows of a column-major matrix)
+//   by cols (cols == 1): element (i, p) = X[p + i * ldx] (columns of a column-major matrix)
+// mask 1 keeps only p + koff <= i, mask 2 only p + koff >= i (a triangular
+// operand whose K range starts at koff); masked elements read as zero.
+__device__ __forceinline__ bool oz_keep(int mask, long long i, long long p, long long koff) {
+  return mask == 0 || (mask == 1 ? p + koff <= i : p + koff >= i);
+}
+
+__device__ __forceinline__ int oz_frexp_max(int m, double v) {
+  if (v != 0.0) {
+    int ex;
+    frexp(v, &ex);
+    m = ex > m ? ex : m;
   }
+  return m;
+}
+
+// e[i] = max(e[i], max_p exponent(x_ip)) with |x_ip| < 2^e; e[] pre-set very
+// negative (all-zero rows keep it and are sliced with exponent 0).
+__global__ void __launch_bounds__(256) oz_exp_rows_kernel(long long rows, long long k, const double* __restrict__ X,
+                                                          long long ldx, int mask, long long koff,
+                                                          int* __restrict__ e) {
+  const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (i >= rows) return;
+  int m = INT_MIN / 2;
+  for (long long p = blockIdx.y; p < k; p += gridDim.y)
+    if (oz_keep(mask, i, p, koff)) m = oz_frexp_max(m, X[i + p * ldx]);
   atomicMax(&e[i], m);
 }
 
-// 32 rows x 128 columns per block: FP64 tile through shared memory, then
-// each thread slices 16 consecutive columns of one row and writes them as one
-// 16-byte int8 vector per slice (K-major planes Q[s][i][p], row stride ldq).
-__global__ void __launch_bounds__(256) oz_slice_kernel(long long n, long long k, const double* __restrict__ A,
-                                                       long long lda, const int* __restrict__ e, int S,
-                                                       int8_t* __restrict__ Q, long long ldq, long long plane) {
-  __shared__ double tile[128][33];
-  const long long r0 = (long long)blockIdx.x * 32, p0 = (long long)blockIdx.y * 128;
-  const int t = threadIdx.x;
-  for (int idx = t; idx < 32 * 128; idx += 256) {
-    const int r = idx & 31, c = idx >> 5;
-    const long long gi = r0 + r, gp = p0 + c;
-    tile[c][r] = (gi < n && gp < k) ? A[gi + gp * lda] : 0.0;
-  }
-  __syncthreads();
-  const int r = t >> 3, c0 = (t & 7) * 16;
-  const long long gi = r0 + r;
-  if (gi >= n) return;
-  const int ex = e[gi] < -1000 ? 0 : e[gi];
-  double x[16];
+// One warp per operand row (a column of X, contiguous in memory).
+__global__ void __launch_bounds__(256) oz_exp_cols_kernel(long long rows, long long k, const double* __restrict__ X,
+                                                          long long ldx, int mask, long long koff,
+                                                          int* __restrict__ e) {
+  const long long i = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= rows) return;
+  int m = INT_MIN / 2;
+  for (long long p = lane; p < k; p += 32)
+    if (oz_keep(mask, i, p, koff)) m = oz_frexp_max(m, X[p + i * ldx]);
 #pragma unroll
-  for (int j = 0; j < 16; ++j) x[j] = ldexp(tile[c0 + j][r], -ex);
+  for (int o = 16; o > 0; o >>= 1) {
+    const int t = __shfl_xor_sync(0xffffffffu, m, o);
+    m = t > m ? t : m;
+  }
+  if (lane == 0) atomicMax(&e[i], m);
+}
+
+// Slices 16 consecutive K values of one row (already scaled by 2^-e) into S
+// int8 planes: one 16-byte vector per slice at Q[s * plane + i * ldq + col].
+__device__ __forceinline__ void oz_emit16(double* x, int S, int8_t* __restrict__ Q, long long plane, long long off) {
   for (int s = 0; s < S; ++s) {
     uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
@@ -115,23 +130,78 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(long long n, long long k,
       x[j] = y - q;
       w[j >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)q) << (8 * (j & 3));
     }
-    const long long gp = p0 + c0;
-    if (gp < k) *reinterpret_cast<uint4*>(Q + s * plane + gi * ldq + gp) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(Q + s * plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
+// By-rows operand: 32 rows x 128 K values per block, transposed through
+// shared memory so global reads are coalesced along the rows. Columns
+// [k, kw) of the planes are written as zeros (kw a multiple of 16).
+__global__ void __launch_bounds__(256) oz_slice_rows_kernel(long long rows, long long k, const double* __restrict__ X,
+                                                            long long ldx, int mask, long long koff,
+                                                            const int* __restrict__ e, int S, int8_t* __restrict__ Q,
+                                                            long long ldq, long long plane, long long qoff,
+                                                            long long kw) {
+  __shared__ double tile[128][33];
+  const long long r0 = (long long)blockIdx.x * 32, p0 = (long long)blockIdx.y * 128;
+  const int t = threadIdx.x;
+  for (int idx = t; idx < 32 * 128; idx += 256) {
+    const int r = idx & 31, c = idx >> 5;
+    const long long gi = r0 + r, gp = p0 + c;
+    tile[c][r] = (gi < rows && gp < k && oz_keep(mask, gi, gp, koff)) ? X[gi + gp * ldx] : 0.0;
+  }
+  __syncthreads();
+  const int r = t >> 3, c0 = (t & 7) * 16;
+  const long long gi = r0 + r, gp = p0 + c0;
+  if (gi >= rows || gp >= kw) return;
+  const int ex = e[gi] < -1000 ? 0 : e[gi];
+  double x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = ldexp(tile[c0 + j][r], -ex);
+  oz_emit16(x, S, Q, plane, gi * ldq + qoff + gp);
+}
+
+// By-cols operand: each thread reads 16 consecutive K values of one row.
+__global__ void __launch_bounds__(256) oz_slice_cols_kernel(long long rows, long long k, const double* __restrict__ X,
+                                                            long long ldx, int mask, long long koff,
+                                                            const int* __restrict__ e, int S, int8_t* __restrict__ Q,
+                                                            long long ldq, long long plane, long long qoff,
+                                                            long long kw) {
+  const int t = threadIdx.x;
+  const long long gi = (long long)blockIdx.x * 32 + (t >> 3), gp = (long long)blockIdx.y * 128 + (t & 7) * 16;
+  if (gi >= rows || gp >= kw) return;
+  const int ex = e[gi] < -1000 ? 0 : e[gi];
+  double x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const long long p = gp + j;
+    x[j] = (p < k && oz_keep(mask, gi, p, koff)) ? ldexp(X[p + gi * ldx], -ex) : 0.0;
+  }
+  oz_emit16(x, S, Q, plane, gi * ldq + qoff + gp);
+}
+
 // ---------------------------------------------------------------- products
+// C (M x N, column-major FP64) = alpha * sum_L 2^(eA_i + eB_j - 7L) P_L + beta * C
+// with P_L = sum_{s+t=L} QA_s QB_t^T over the tile's K-blocks [kb0, kb1).
+// tile = {m0, n0, kb0 | kOzAccumulate?, kb1}; kOzAccumulate: beta is taken
+// as 1 for this tile (a later K chunk of a product whose first chunk
+// already applied beta).
+constexpr int kOzAccumulate = 1 << 30;
+
 struct OzArgs {
-  CUtensorMap mapA;  // Q planes, box {128, 128, 1}
-  CUtensorMap mapB;  // Q planes, box {128, 256, 1}
+  CUtensorMap mapA;  // QA planes, box {128, 128, 1}
+  CUtensorMap mapB;  // QB planes, box {128, 256, 1}
   const int4* tiles;
   int num_tiles;
-  int S, KB;  // slices, K-blocks of 128
-  int n;
+  int S;
+  int kb_shift, kb_mod;  // B's K-block = kb + kb_shift (mod kb_mod when kb_mod > 0)
+  int M, N;
+  int tri;  // 1: only C(i, j) with j <= i is written
   double* C;
   long long ldc;
   double alpha, beta;
-  const int* e;
+  const int* eA;
+  const int* eB;
   int raw_level;  // >= 2: write P_raw_level (int32) to raw_out instead of folding into C
   int* raw_out;
   long long ld_raw;
@@ -141,7 +211,7 @@ struct OzArgs {
 __device__ __forceinline__ int level_pairs_begin(int L, int S) { return L - S > 1 ? L - S : 1; }
 __device__ __forceinline__ int level_pairs_end(int L, int S) { return L - 1 < S ? L - 1 : S; }
 
-__global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__ OzArgs args) {
+__global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__ OzArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOzStages * kOzStageBytes);
@@ -152,7 +222,7 @@ __global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int S = args.S, KB = args.KB;
+  const int S = args.S;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kOzStages; ++s) {
@@ -188,17 +258,20 @@ __global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__
       bool ok = true;
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
         const int4 tile = args.tiles[t];
+        const int kb0 = tile.z & (kOzAccumulate - 1), kb1 = tile.w;
         for (int L = 2; L <= S + 1 && ok; ++L)
           for (int s = level_pairs_begin(L, S); s <= level_pairs_end(L, S) && ok; ++s)
-            for (int kb = 0; kb < KB; ++kb) {
+            for (int kb = kb0; kb < kb1; ++kb) {
               if (!mbar_wait(&empty[st], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
                 ok = false;
                 break;
               }
+              int kbb = kb + args.kb_shift;
+              if (args.kb_mod > 0 && kbb >= args.kb_mod) kbb -= args.kb_mod;
               mbar_arrive_expect_tx(&full[st], kOzStageBytes);
               uint8_t* dst = smem + st * kOzStageBytes;
               tma_load_3d(dst, &args.mapA, &full[st], kb * kOzBK, tile.x, s - 1);
-              tma_load_3d(dst + kOzABytes, &args.mapB, &full[st], kb * kOzBK, tile.y, L - s - 1);
+              tma_load_3d(dst + kOzABytes, &args.mapB, &full[st], kbb * kOzBK, tile.y, L - s - 1);
               issued_mask |= 1u << st;
               phase_mask = (phase_mask & ~(1u << st)) | (ph << st);
               if (++st == kOzStages) {
@@ -224,6 +297,9 @@ __global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__
       int it = 0;
       bool ok = true, any = false;
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+        const int4 tile = args.tiles[t];
+        const int kb0 = tile.z & (kOzAccumulate - 1), kb1 = tile.w;
+        if (kb1 <= kb0) continue;  // empty product: no accumulator round trip
         for (int L = 2; L <= S + 1 && ok; ++L, ++it) {
           const int buf = it & 1;
           const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -235,7 +311,7 @@ __global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__
           const uint32_t d = tmem_base + (uint32_t)(buf * kOzBN);
           bool first = true;
           for (int s = level_pairs_begin(L, S); s <= level_pairs_end(L, S) && ok; ++s)
-            for (int kb = 0; kb < KB; ++kb) {
+            for (int kb = kb0; kb < kb1; ++kb) {
               if (!mbar_wait(&full[st], ph, abort_flag, args.err, kDevErrTimeoutMma)) {
                 ok = false;
                 break;
@@ -275,9 +351,22 @@ __global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__
     bool ok = true;
     for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
       const int4 tile = args.tiles[t];
+      const double beta = (tile.z & kOzAccumulate) ? 1.0 : args.beta;
       const long long gi = (long long)tile.x + row;
-      const bool row_ok = gi < args.n;
-      const int ei = row_ok ? (args.e[gi] < -1000 ? 0 : args.e[gi]) : 0;
+      const bool row_ok = gi < args.M;
+      const int ei = row_ok ? (args.eA[gi] < -1000 ? 0 : args.eA[gi]) : 0;
+      if (tile.w <= (tile.z & (kOzAccumulate - 1))) {
+        // empty product (K range outside the operand's support): C = beta C
+        if (row_ok && beta != 1.0 && args.raw_level < 2)
+          for (int j = 0; j < kOzBN; ++j) {
+            const long long gj = (long long)tile.y + j;
+            if (gj < args.N && (!args.tri || gj <= gi)) {
+              double* c = args.C + gi + gj * args.ldc;
+              *c = beta == 0.0 ? 0.0 : beta * *c;
+            }
+          }
+        continue;
+      }
       for (int L = 2; L <= S + 1; ++L, ++it) {
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -298,7 +387,7 @@ __global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
               const long long gj = (long long)tile.y + c0 + j;
-              if (gj < args.n && gj <= gi) args.raw_out[gi + gj * args.ld_raw] = v[j];
+              if (gj < args.N && (!args.tri || gj <= gi)) args.raw_out[gi + gj * args.ld_raw] = v[j];
             }
             continue;
           }
@@ -307,17 +396,17 @@ __global__ void __launch_bounds__(192, 1) oz_syrk_kernel(const __grid_constant__
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const long long gj = (long long)tile.y + c0 + j;
-            keep[j] = gj < args.n && gj <= gi;
+            keep[j] = gj < args.N && (!args.tri || gj <= gi);
             old[j] = 0.0;
-            if (keep[j] && (L > 2 || args.beta != 0.0)) old[j] = args.C[gi + gj * args.ldc];
+            if (keep[j] && (L > 2 || beta != 0.0)) old[j] = args.C[gi + gj * args.ldc];
           }
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             if (!keep[j]) continue;
             const long long gj = (long long)tile.y + c0 + j;
-            const int ej = args.e[gj] < -1000 ? 0 : args.e[gj];
+            const int ej = args.eB[gj] < -1000 ? 0 : args.eB[gj];
             const double scale = args.alpha * ldexp(1.0, ei + ej - 7 * L);
-            const double base = (L == 2) ? args.beta * old[j] : old[j];
+            const double base = (L == 2) ? beta * old[j] : old[j];
             args.C[gi + gj * args.ldc] = fma(scale, (double)v[j], base);
           }
         }
@@ -366,103 +455,504 @@ tb_status make_q_map(CUtensorMap* map, int8_t* Q, long long ldq, long long n, in
   return TB_SUCCESS;
 }
 
-}  // namespace
+// ---------------------------------------------------------------- host side
+// Largest K chunk whose level sums stay exact in INT32:
+// (pairs per level <= S) * K * 127^2 < 2^31.
+long long oz_kmax(int S) { return ((2147483647LL / ((long long)S * 127 * 127)) / kOzBK) * kOzBK; }
 
-// Slices A (n x k, column-major) into S int8 planes (K-major, row stride ldq)
-// and row exponents e[n].
-tb_status ozaki_slice(long long n, long long k, const double* A, long long lda, int S, int8_t* Q, long long ldq,
-                      int* e, cudaStream_t st) {
-  TB_CUDA_TRY(cudaMemsetAsync(e, 0x80, sizeof(int) * n, st));
-  TB_CUDA_TRY(cudaMemsetAsync(Q, 0, (size_t)S * n * ldq, st));  // K padding up to ldq reads as zero
-  dim3 g1((unsigned)((n + 255) / 256), (unsigned)(k < 64 ? k : 64));
-  oz_rowexp_kernel<<<g1, 256, 0, st>>>(n, k, A, lda, e);
-  TB_CUDA_TRY(cudaGetLastError());
-  note_launch();
-  dim3 g2((unsigned)((n + 31) / 32), (unsigned)((k + 127) / 128));
-  oz_slice_kernel<<<g2, 256, 0, st>>>(n, k, A, lda, e, S, Q, ldq, ldq * n);
+struct OzOperand {
+  const double* X = nullptr;
+  long long ld = 0;
+  long long rows = 0, k = 0;
+  bool by_cols = false;
+  int mask = 0;
+  long long koff = 0;
+  // the K sub-range [k0, k0 + kc) of the operand, as an operand of its own
+  OzOperand chunk(long long k0, long long kc) const {
+    OzOperand o = *this;
+    o.X = by_cols ? X + k0 : X + k0 * ld;
+    o.k = kc;
+    o.koff = koff + k0;
+    return o;
+  }
+};
+
+// Planes of one operand: S int8 planes [rows][ldq] and row exponents.
+struct OzPlanes {
+  int8_t* Q = nullptr;
+  long long ldq = 0, rows = 0;
+  int* e = nullptr;
+};
+
+tb_status oz_exponents(const OzOperand& o, int* e, cudaStream_t st) {
+  if (o.rows == 0 || o.k == 0) return TB_SUCCESS;
+  if (o.by_cols) {
+    oz_exp_cols_kernel<<<(unsigned)((o.rows + 7) / 8), 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff, e);
+  } else {
+    dim3 g((unsigned)((o.rows + 255) / 256), (unsigned)(o.k < 64 ? o.k : 64));
+    oz_exp_rows_kernel<<<g, 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff, e);
+  }
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   return TB_SUCCESS;
 }
 
-tb_status ozaki_syrk_impl(long n, long k, double alpha, const double* A, long lda, double beta, double* C, long ldc,
-                          int S, int raw_level, int* raw_out, long ld_raw, cudaStream_t st) {
-  if (n < 0 || k < 0 || lda < (n > 1 ? n : 1) || ldc < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
-  if (S < 1 || S > kOzMaxSlices) {
-    set_last_error("ozaki: slices must be in [1, %d]", kOzMaxSlices);
-    return TB_ERROR_INVALID_VALUE;
+// Writes columns [qoff, qoff + kw) of the planes (zeros beyond o.k).
+tb_status oz_slice(const OzOperand& o, const int* e, int S, const OzPlanes& q, long long qoff, long long kw,
+                   cudaStream_t st) {
+  if (o.rows == 0 || kw == 0) return TB_SUCCESS;
+  dim3 g((unsigned)((o.rows + 31) / 32), (unsigned)((kw + 127) / 128));
+  if (o.by_cols)
+    oz_slice_cols_kernel<<<g, 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff, e, S, q.Q, q.ldq, q.ldq * q.rows,
+                                            qoff, kw);
+  else
+    oz_slice_rows_kernel<<<g, 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff, e, S, q.Q, q.ldq, q.ldq * q.rows,
+                                            qoff, kw);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
+
+// Exponents + slices of one operand into fresh planes.
+tb_status oz_prepare(const OzOperand& o, int S, const OzPlanes& q, cudaStream_t st) {
+  TB_CUDA_TRY(cudaMemsetAsync(q.e, 0x80, sizeof(int) * (size_t)(o.rows > 0 ? o.rows : 1), st));
+  TB_TRY(oz_exponents(o, q.e, st));
+  return oz_slice(o, q.e, S, q, 0, q.ldq, st);
+}
+
+size_t oz_planes_bytes(long long rows, long long ldq, int S) {
+  return (size_t)round_up((long long)S * rows * ldq, 256) + (size_t)round_up(rows * 4 + 4, 256);
+}
+
+// Carves planes for `rows` x ldq out of ws (advancing it).
+OzPlanes oz_carve(char*& ws, long long rows, long long ldq, int S) {
+  OzPlanes q;
+  q.rows = rows;
+  q.ldq = ldq;
+  q.Q = reinterpret_cast<int8_t*>(ws);
+  ws += round_up((long long)S * rows * ldq, 256);
+  q.e = reinterpret_cast<int*>(ws);
+  ws += round_up(rows * 4 + 4, 256);
+  return q;
+}
+
+// Per-tile K range of a product chunk [k0, k1) of an operand pair whose
+// product vanishes outside [kbeg(m0, n0), kend(m0, n0)).
+enum class KRange {
+  kFull,       // [0, K)
+  kRowsLower,  // A lower triangular by rows:      [0, m0 + BM)
+  kRowsUpper,  // A upper triangular by rows:      [m0, K)
+  kColsLower,  // B operand lower triangular:      [0, n0 + BN)
+};
+
+std::vector<int4> oz_plan(int M, int N, bool lower_tiles, KRange kr, long long K, long long k0, long long k1,
+                          bool first_chunk) {
+  std::vector<int4> plan = lower_tiles ? plan_lower(M, kOzBN, 0, 0) : plan_rect(M, N, kOzBN, 0, 0);
+  std::vector<int4> out;
+  out.reserve(plan.size());
+  for (int4 t : plan) {
+    long long b = 0, e = K;
+    if (kr == KRange::kRowsLower) e = std::min<long long>(K, (long long)t.x + kOzBM);
+    if (kr == KRange::kRowsUpper) b = t.x;
+    if (kr == KRange::kColsLower) e = std::min<long long>(K, (long long)t.y + kOzBN);
+    // tiles whose whole range lies in an earlier chunk were written there
+    b = std::max(b, k0);
+    e = std::min(e, k1);
+    if (e <= b) {
+      if (!first_chunk) continue;
+      t.z = t.w = 0;  // empty product: the kernel only applies beta to the tile
+    } else {
+      // every tile is written by the first chunk; later chunks accumulate
+      t.z = (int)((b - k0) / kOzBK) | (first_chunk ? 0 : kOzAccumulate);
+      t.w = (int)((e - k0 + kOzBK - 1) / kOzBK);
+    }
+    out.push_back(t);
   }
-  // exactness of the INT32 level sums: (pairs per level) * k * 127^2 < 2^31
-  const double bound = (double)S * (double)k * 127.0 * 127.0;
-  if (bound >= 2147483647.0) {
-    set_last_error("ozaki: k = %ld too large for exact INT32 accumulation with %d slices", k, S);
-    return TB_ERROR_NOT_SUPPORTED;
-  }
-  if (n == 0 || k == 0) return TB_SUCCESS;
-  const long long ldq = round_up(k, 128);
-  const size_t qbytes = (size_t)S * n * ldq;
-  const size_t ebytes = (size_t)round_up(n * 4, 256);
-  char* ws = static_cast<char*>(pool_get(qbytes + ebytes));
-  if (!ws) return TB_ERROR_ALLOC;
-  int* e = reinterpret_cast<int*>(ws);
-  int8_t* Q = reinterpret_cast<int8_t*>(ws + ebytes);
-  TB_TRY(ozaki_slice(n, k, A, lda, S, Q, ldq, e, st));
-  OzArgs a;
-  memset(&a, 0, sizeof(a));
-  TB_TRY(make_q_map(&a.mapA, Q, ldq, n, S, kOzBM));
-  TB_TRY(make_q_map(&a.mapB, Q, ldq, n, S, kOzBN));
-  const std::vector<int4> plan = plan_lower((int)n, kOzBN, 0, 1);
-  a.tiles = upload_tiles(plan, st);
-  if (!a.tiles) return TB_ERROR_ALLOC;
-  a.num_tiles = (int)plan.size();
-  a.S = S;
-  a.KB = (int)(ldq / kOzBK);
-  a.n = (int)n;
-  a.C = C;
-  a.ldc = ldc;
-  a.alpha = alpha;
-  a.beta = beta;
-  a.e = e;
-  a.raw_level = raw_level;
-  a.raw_out = raw_out;
-  a.ld_raw = ld_raw;
-  a.err = device_error_word();
+  return out;
+}
+
+tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_mod, const std::vector<int4>& plan,
+                    int M, int N, int tri, double alpha, double* C, long long ldc, double beta, int S, double flops,
+                    int raw_level, int* raw_out, long long ld_raw, cudaStream_t st) {
+  if (plan.empty()) return TB_SUCCESS;
+  OzArgs g;
+  memset(&g, 0, sizeof(g));
+  TB_TRY(make_q_map(&g.mapA, a.Q, a.ldq, a.rows, S, kOzBM));
+  TB_TRY(make_q_map(&g.mapB, b.Q, b.ldq, b.rows, S, kOzBN));
+  g.tiles = upload_tiles(plan, st);
+  if (!g.tiles) return TB_ERROR_ALLOC;
+  g.num_tiles = (int)plan.size();
+  g.S = S;
+  g.kb_shift = kb_shift;
+  g.kb_mod = kb_mod;
+  g.M = M;
+  g.N = N;
+  g.tri = tri;
+  g.C = C;
+  g.ldc = ldc;
+  g.alpha = alpha;
+  g.beta = beta;
+  g.eA = a.e;
+  g.eB = b.e;
+  g.raw_level = raw_level;
+  g.raw_out = raw_out;
+  g.ld_raw = ld_raw;
+  g.err = device_error_word();
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr[dev]) {
-    TB_CUDA_TRY(cudaFuncSetAttribute(oz_syrk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzSmem));
+    TB_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzSmem));
     attr[dev] = true;
   }
-  const int grid = a.num_tiles < sm_count() ? a.num_tiles : sm_count();
+  const int grid = g.num_tiles < sm_count() ? g.num_tiles : sm_count();
   void* tok = prof_begin(st);
-  oz_syrk_kernel<<<grid, 192, kOzSmem, st>>>(a);
+  oz_gemm_kernel<<<grid, 192, kOzSmem, st>>>(g);
   TB_CUDA_TRY(cudaGetLastError());
-  prof_end(tok, st, (double)n * (double)(n + 1) * (double)k);
+  prof_end(tok, st, flops);
   note_launch();
   return TB_SUCCESS;
 }
 
+tb_status check_slices(int S) {
+  if (S < 1 || S > kOzMaxSlices) {
+    set_last_error("ozaki: slices must be in [1, %d]", kOzMaxSlices);
+    return TB_ERROR_INVALID_VALUE;
+  }
+  return TB_SUCCESS;
+}
+
+// Scratch of oz_gemm for operands of at most ra / rb rows and K.
+size_t oz_gemm_ws(long long ra, long long rb, long long K, int S) {
+  const long long ldq = round_up(std::min<long long>(std::max<long long>(K, 1), oz_kmax(S)), kOzBK);
+  return oz_planes_bytes(ra, ldq, S) + oz_planes_bytes(rb, ldq, S);
+}
+
+// C (M x N) = alpha * a (M x K) * b (N x K)^T + beta * C in FP64 on the INT8
+// tensor cores, in K chunks of at most oz_kmax(S). ws: oz_gemm_ws bytes.
+tb_status oz_gemm(const OzOperand& a, const OzOperand& b, long long K, KRange kr, bool lower_tiles, double alpha,
+                  double* C, long long ldc, double beta, int S, double flops, char* ws, cudaStream_t st) {
+  const int M = (int)a.rows, N = (int)b.rows;
+  if (M == 0 || N == 0) return TB_SUCCESS;
+  const long long kc_max = oz_kmax(S);
+  const long long ldq = round_up(std::min<long long>(std::max<long long>(K, 1), kc_max), kOzBK);
+  OzPlanes qa = oz_carve(ws, M, ldq, S);
+  OzPlanes qb = oz_carve(ws, N, ldq, S);
+  const long long K1 = K > 0 ? K : 1;  // K == 0: one all-zero chunk applies beta
+  for (long long k0 = 0; k0 < K1; k0 += kc_max) {
+    const long long kc = std::min(kc_max, K1 - k0);
+    const long long kreal = std::max(0LL, std::min(kc, K - k0));
+    TB_TRY(oz_prepare(a.chunk(k0, kreal), S, qa, st));
+    TB_TRY(oz_prepare(b.chunk(k0, kreal), S, qb, st));
+    const std::vector<int4> plan = oz_plan(M, N, lower_tiles, kr, K1, k0, k0 + kc, k0 == 0);
+    TB_TRY(oz_launch(qa, qb, 0, 0, plan, M, N, lower_tiles ? 1 : 0, alpha, C, ldc, beta, S,
+                     flops * (double)kc / (double)K1, 0, nullptr, 0, st));
+  }
+  return TB_SUCCESS;
+}
+
+}  // namespace
+
+// Slices A (n x k, column-major) into S int8 planes (K-major, row stride
+// ldq; columns [k, kw) written as zeros) and row exponents e[n].
+tb_status ozaki_slice(long long n, long long k, const double* A, long long lda, int S, int8_t* Q, long long ldq,
+                      long long kw, int* e, cudaStream_t st) {
+  OzOperand o;
+  o.X = A;
+  o.ld = lda;
+  o.rows = n;
+  o.k = k;
+  OzPlanes q;
+  q.Q = Q;
+  q.ldq = ldq;
+  q.rows = n;
+  q.e = e;
+  TB_CUDA_TRY(cudaMemsetAsync(e, 0x80, sizeof(int) * n, st));
+  TB_TRY(oz_exponents(o, e, st));
+  return oz_slice(o, e, S, q, 0, kw, st);
+}
+
+// FP64 SYRK: C(lower) = alpha A A^T + beta C, A n x k ('N') or k x n ('T').
+tb_status ozaki_syrk_impl(bool trans, long n, long k, double alpha, const double* A, long lda, double beta, double* C,
+                          long ldc, int S, int raw_level, int* raw_out, long ld_raw, cudaStream_t st) {
+  const long rows_a = trans ? k : n;
+  if (n < 0 || k < 0 || lda < (rows_a > 1 ? rows_a : 1) || ldc < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
+  TB_TRY(check_slices(S));
+  if (n == 0) return TB_SUCCESS;
+  const long long kc_max = oz_kmax(S);
+  if (raw_level >= 2 && k > kc_max) {
+    set_last_error("ozaki: level products need k <= %lld with %d slices", kc_max, S);
+    return TB_ERROR_NOT_SUPPORTED;
+  }
+  OzOperand a;
+  a.X = A;
+  a.ld = lda;
+  a.rows = n;
+  a.k = k;
+  a.by_cols = trans;
+  const long long K1 = k > 0 ? k : 1;
+  const long long ldq = round_up(std::min<long long>(K1, kc_max), kOzBK);
+  char* ws = static_cast<char*>(pool_get(oz_planes_bytes(n, ldq, S)));
+  if (!ws) return TB_ERROR_ALLOC;
+  OzPlanes q = oz_carve(ws, n, ldq, S);
+  for (long long k0 = 0; k0 < K1; k0 += kc_max) {
+    const long long kc = std::min(kc_max, K1 - k0);
+    TB_TRY(oz_prepare(a.chunk(k0, std::max(0LL, std::min(kc, (long long)k - k0))), S, q, st));
+    const std::vector<int4> plan = oz_plan((int)n, (int)n, true, KRange::kFull, K1, k0, k0 + kc, k0 == 0);
+    TB_TRY(oz_launch(q, q, 0, 0, plan, (int)n, (int)n, 1, alpha, C, ldc, beta, S,
+                     (double)n * (double)(n + 1) * (double)kc, raw_level, raw_out, ld_raw, st));
+  }
+  return TB_SUCCESS;
+}
+
+// FP64 SYR2K: C(lower) = alpha (A B^T + B A^T) + beta C, A and B n x k.
+// One product of [A | B] with [B | A]: both share the row exponents of
+// [A | B] and one set of planes; the B operand reads the planes with its K
+// halves swapped (kb_shift).
+tb_status ozaki_syr2k_impl(long n, long k, double alpha, const double* A, long lda, const double* B, long ldb,
+                           double beta, double* C, long ldc, int S, cudaStream_t st) {
+  if (n < 0 || k < 0 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) || ldc < (n > 1 ? n : 1))
+    return TB_ERROR_INVALID_VALUE;
+  TB_TRY(check_slices(S));
+  if (n == 0) return TB_SUCCESS;
+  const long long kc_max = oz_kmax(S) / 2 / kOzBK * kOzBK;  // the concatenated K is twice the chunk
+  const long long K1 = k > 0 ? k : 1;
+  const long long kh = round_up(std::min<long long>(K1, kc_max), kOzBK);
+  char* ws = static_cast<char*>(pool_get(oz_planes_bytes(n, 2 * kh, S)));
+  if (!ws) return TB_ERROR_ALLOC;
+  OzPlanes q = oz_carve(ws, n, 2 * kh, S);
+  OzOperand a, b;
+  a.X = A;
+  a.ld = lda;
+  a.rows = n;
+  a.k = k;
+  b = a;
+  b.X = B;
+  b.ld = ldb;
+  for (long long k0 = 0; k0 < K1; k0 += kc_max) {
+    const long long kc = std::min(kc_max, K1 - k0);
+    const long long kreal = std::max(0LL, std::min(kc, (long long)k - k0));
+    const OzOperand ac = a.chunk(k0, kreal), bc = b.chunk(k0, kreal);
+    TB_CUDA_TRY(cudaMemsetAsync(q.e, 0x80, sizeof(int) * n, st));
+    TB_TRY(oz_exponents(ac, q.e, st));
+    TB_TRY(oz_exponents(bc, q.e, st));
+    TB_TRY(oz_slice(ac, q.e, S, q, 0, kh, st));
+    TB_TRY(oz_slice(bc, q.e, S, q, kh, kh, st));
+    const std::vector<int4> plan = oz_plan((int)n, (int)n, true, KRange::kFull, 2 * kh, 0, 2 * kh, k0 == 0);
+    const int khb = (int)(kh / kOzBK);
+    // later chunks accumulate: oz_plan marks them only when k0 > 0 via first_chunk
+    TB_TRY(oz_launch(q, q, khb, 2 * khb, plan, (int)n, (int)n, 1, alpha, C, ldc, beta, S,
+                     2.0 * (double)n * (double)(n + 1) * (double)kc, 0, nullptr, 0, st));
+  }
+  return TB_SUCCESS;
+}
+
+// FP64 TRMM (left, out of place): C = alpha op(A) B, A m x m lower ('L') or
+// upper ('U') triangular (the other triangle is never read), B, C m x n.
+tb_status ozaki_trmm_impl(bool upper, long m, long n, double alpha, const double* A, long lda, const double* B,
+                          long ldb, double* C, long ldc, int S, cudaStream_t st) {
+  if (m < 0 || n < 0 || lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1) || ldc < (m > 1 ? m : 1))
+    return TB_ERROR_INVALID_VALUE;
+  TB_TRY(check_slices(S));
+  if (m == 0 || n == 0) return TB_SUCCESS;
+  OzOperand a, b;
+  a.X = A;
+  a.ld = lda;
+  a.rows = m;
+  a.k = m;
+  a.mask = upper ? 2 : 1;
+  b.X = B;
+  b.ld = ldb;
+  b.rows = n;
+  b.k = m;
+  b.by_cols = true;
+  char* ws = static_cast<char*>(pool_get(oz_gemm_ws(m, n, m, S)));
+  if (!ws) return TB_ERROR_ALLOC;
+  return oz_gemm(a, b, m, upper ? KRange::kRowsUpper : KRange::kRowsLower, false, alpha, C, ldc, 0.0, S,
+                 (double)m * m * n, ws, st);
+}
+
+// FP64 TRSM, A lower-triangular non-unit:
+//   right: X A^T = B (the reference's tc_ozimmu_trsm), A n x n, B m x n
+//   left : A X = B, A m x m
+// The same recursion as the FP32 driver (halving at leaf boundaries). Leaves
+// multiply by the FP64 inverse of the diagonal block (warp substitution on
+// 32x32 blocks plus column chains, all FP64); leaf products and off-diagonal
+// updates are Ozaki-scheme FP64 GEMMs on the INT8 tensor cores. Operands are
+// sliced into planes before each product, so X can overwrite B in place.
+namespace {
+struct OzTrsm {
+  bool right;
+  long m, n, nt;
+  const double* A;
+  long lda;
+  double* B;
+  long ldb;
+  int leaf;
+  double* W;
+  long long ldw, wstride;
+  int S;
+  char* ws;
+  cudaStream_t st;
+};
+
+tb_status oz_trsm_leaf(OzTrsm& c, int bidx, long s, long e) {
+  const long sz = e - s;
+  OzOperand w;  // W_b by rows: row j holds W(j, :), lower triangular
+  w.X = c.W + bidx * c.wstride;
+  w.ld = c.ldw;
+  w.rows = sz;
+  w.k = sz;
+  OzOperand x;
+  if (c.right) {
+    // B[:, s:e] = B[:, s:e] W^T: rows of B's block against rows of W
+    x.X = c.B + s * c.ldb;
+    x.ld = c.ldb;
+    x.rows = c.m;
+    x.k = sz;
+    return oz_gemm(x, w, sz, KRange::kColsLower, false, 1.0, c.B + s * c.ldb, c.ldb, 0.0, c.S,
+                   (double)c.m * sz * sz, c.ws, c.st);
+  }
+  // B[s:e, :] = W B[s:e, :]: rows of W against columns of B's block
+  x.X = c.B + s;
+  x.ld = c.ldb;
+  x.rows = c.n;
+  x.k = sz;
+  x.by_cols = true;
+  return oz_gemm(w, x, sz, KRange::kRowsLower, false, 1.0, c.B + s, c.ldb, 0.0, c.S, (double)c.n * sz * sz, c.ws,
+                 c.st);
+}
+
+tb_status oz_trsm_update(OzTrsm& c, long s, long mid, long e) {
+  const long kk = mid - s;
+  OzOperand a21;  // A[mid:e, s:mid] by rows
+  a21.X = c.A + mid + s * c.lda;
+  a21.ld = c.lda;
+  a21.rows = e - mid;
+  a21.k = kk;
+  OzOperand x;
+  if (c.right) {
+    // B[:, mid:e] -= B[:, s:mid] A[mid:e, s:mid]^T
+    x.X = c.B + s * c.ldb;
+    x.ld = c.ldb;
+    x.rows = c.m;
+    x.k = kk;
+    return oz_gemm(x, a21, kk, KRange::kFull, false, -1.0, c.B + mid * c.ldb, c.ldb, 1.0, c.S,
+                   2.0 * c.m * (e - mid) * kk, c.ws, c.st);
+  }
+  // B[mid:e, :] -= A[mid:e, s:mid] B[s:mid, :]
+  x.X = c.B + s;
+  x.ld = c.ldb;
+  x.rows = c.n;
+  x.k = kk;
+  x.by_cols = true;
+  return oz_gemm(a21, x, kk, KRange::kFull, false, -1.0, c.B + mid, c.ldb, 1.0, c.S, 2.0 * c.n * (e - mid) * kk,
+                 c.ws, c.st);
+}
+
+tb_status oz_trsm_rec(OzTrsm& c, long s, long e) {
+  if (e - s <= c.leaf) return oz_trsm_leaf(c, (int)(s / c.leaf), s, e);
+  const long nleaves = (e - s + c.leaf - 1) / c.leaf;
+  const long mid = s + ((nleaves + 1) / 2) * c.leaf;
+  TB_TRY(oz_trsm_rec(c, s, mid));
+  TB_TRY(oz_trsm_update(c, s, mid, e));
+  return oz_trsm_rec(c, mid, e);
+}
+}  // namespace
+
+tb_status ozaki_trsm_impl(bool right, long m, long n, const double* A, long lda, double* B, long ldb, long nb, int S,
+                          cudaStream_t st) {
+  if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
+  const long nt = right ? n : m;
+  if (lda < (nt > 1 ? nt : 1) || ldb < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
+  TB_TRY(check_slices(S));
+  if (m == 0 || n == 0) return TB_SUCCESS;
+  OzTrsm c;
+  c.right = right;
+  c.m = m;
+  c.n = n;
+  c.nt = nt;
+  c.A = A;
+  c.lda = lda;
+  c.B = B;
+  c.ldb = ldb;
+  c.S = S;
+  c.st = st;
+  long leaf = round_up(std::min<long>(nb, kOzLeaf), 64);
+  if (leaf > kOzLeaf) leaf = kOzLeaf;
+  c.leaf = (int)leaf;
+  std::vector<int2> leaves;
+  for (long s = 0; s < nt; s += leaf) leaves.push_back(make_int2((int)s, (int)std::min<long>(leaf, nt - s)));
+  const long nleaf = (long)leaves.size();
+  c.ldw = leaf;
+  c.wstride = leaf * leaf;
+  const long other = right ? m : n;  // extent of B across the solve
+  // largest product: other x (nt - leaf) by K <= nt / 2 + leaf
+  const size_t g_bytes = oz_gemm_ws(std::max<long>(other, nt), std::max<long>(other, nt), nt / 2 + leaf, S);
+  const size_t w_bytes = (size_t)round_up((long long)c.wstride * nleaf * 8, 256);
+  const size_t d_bytes = (size_t)round_up((nt + 31) / 32 * 1024 * 8, 256);
+  const size_t l_bytes = (size_t)round_up(nleaf * (long long)sizeof(int2), 256);
+  char* ws = static_cast<char*>(pool_get(w_bytes + d_bytes + l_bytes + g_bytes));
+  if (!ws) {
+    set_last_error("ozaki trsm: cannot allocate %zu bytes of scratch", w_bytes + d_bytes + l_bytes + g_bytes);
+    return TB_ERROR_ALLOC;
+  }
+  c.W = reinterpret_cast<double*>(ws);
+  double* D = reinterpret_cast<double*>(ws + w_bytes);
+  int2* dleaves = reinterpret_cast<int2*>(ws + w_bytes + d_bytes);
+  c.ws = ws + w_bytes + d_bytes + l_bytes;
+  TB_CUDA_TRY(cudaMemcpyAsync(dleaves, leaves.data(), nleaf * sizeof(int2), cudaMemcpyHostToDevice, st));
+  TB_TRY(trsm_leaf_inverses_f64(nt, A, lda, dleaves, (int)nleaf, (int)leaf, D, c.W, c.ldw, c.wstride, st));
+  return oz_trsm_rec(c, 0, nt);
+}
+
 }  // namespace tb
+
+// ------------------------------------------------------------------ C ABI
+namespace {
+bool is(char c, char u) { return c == u || c == u + ('a' - 'A'); }
+int slices_or_default(int s) { return s <= 0 ? 10 : s; }
+}  // namespace
 
 extern "C" tb_status tb_dsyrk_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
                                     double beta, double* C, long ldc, int slices) {
-  if (uplo != 'L' && uplo != 'l') {
+  if (!is(uplo, 'L')) {
     tb::set_last_error("tb_dsyrk_ozaki: only uplo='L' is supported");
     return TB_ERROR_NOT_SUPPORTED;
   }
-  if (trans != 'N' && trans != 'n') {
-    tb::set_last_error("tb_dsyrk_ozaki: only trans='N' is supported");
+  if (!is(trans, 'N') && !is(trans, 'T')) return TB_ERROR_INVALID_VALUE;
+  return tb::ozaki_syrk_impl(is(trans, 'T'), n, k, alpha, A, lda, beta, C, ldc, slices_or_default(slices), 0,
+                             nullptr, 0, tb::current_stream());
+}
+
+extern "C" tb_status tb_dsyr2k_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
+                                     const double* B, long ldb, double beta, double* C, long ldc, int slices) {
+  if (!is(uplo, 'L') || !is(trans, 'N')) {
+    tb::set_last_error("tb_dsyr2k_ozaki: only uplo='L', trans='N' are supported");
     return TB_ERROR_NOT_SUPPORTED;
   }
-  return tb::ozaki_syrk_impl(n, k, alpha, A, lda, beta, C, ldc, slices <= 0 ? 10 : slices, 0, nullptr, 0,
+  return tb::ozaki_syr2k_impl(n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices_or_default(slices),
+                              tb::current_stream());
+}
+
+extern "C" tb_status tb_dtrmm_ozaki(char uplo, long m, long n, double alpha, const double* A, long lda,
+                                    const double* B, long ldb, double* C, long ldc, int slices) {
+  if (!is(uplo, 'L') && !is(uplo, 'U')) return TB_ERROR_INVALID_VALUE;
+  return tb::ozaki_trmm_impl(is(uplo, 'U'), m, n, alpha, A, lda, B, ldb, C, ldc, slices_or_default(slices),
+                             tb::current_stream());
+}
+
+extern "C" tb_status tb_dtrsm_ozaki(char side, long m, long n, const double* A, long lda, double* B, long ldb,
+                                    long nb, int slices) {
+  if (!is(side, 'R') && !is(side, 'L')) return TB_ERROR_INVALID_VALUE;
+  return tb::ozaki_trsm_impl(is(side, 'R'), m, n, A, lda, B, ldb, nb, slices_or_default(slices),
                              tb::current_stream());
 }
 
 extern "C" tb_status tb_ozaki_level_product(long n, long k, const double* A, long lda, int slices, int level,
                                             int* P, long ldp) {
   if (level < 2 || level > slices + 1 || ldp < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
-  return tb::ozaki_syrk_impl(n, k, 1.0, A, lda, 0.0, nullptr, n > 1 ? n : 1, slices, level, P, ldp,
+  return tb::ozaki_syrk_impl(false, n, k, 1.0, A, lda, 0.0, nullptr, n > 1 ? n : 1, slices, level, P, ldp,
                              tb::current_stream());
 }
 
@@ -472,14 +962,37 @@ extern "C" tb_status tb_ozaki_slice(long n, long k, const double* A, long lda, i
     return TB_ERROR_INVALID_VALUE;
   if (slices < 1 || slices > 14) return TB_ERROR_INVALID_VALUE;
   if (n == 0 || k == 0) return TB_SUCCESS;
-  return tb::ozaki_slice(n, k, A, lda, slices, reinterpret_cast<int8_t*>(Q), ldq, exponents, tb::current_stream());
+  return tb::ozaki_slice(n, k, A, lda, slices, reinterpret_cast<int8_t*>(Q), ldq, tb::round_up(k, 16), exponents,
+                         tb::current_stream());
 }
 
 // ------------------------------------------------------------------ reference C++ API
 #include "../../include/TensorBLAS.h"
 
+namespace {
+void report(const char* fn, tb_status s) {
+  if (s != TB_SUCCESS) fprintf(stderr, "TensorBLAS %s: %s %s\n", fn, tb_status_string(s), tb_last_error());
+}
+}  // namespace
+
 void tc_ozimmu_syrk(cublasHandle_t, long int n, long int k, double alpha, double* A, long int lda, double beta,
                     double* C, long int ldc, long int) {
-  tb_status s = tb::ozaki_syrk_impl(n, k, alpha, A, lda, beta, C, ldc, 10, 0, nullptr, 0, tb::current_stream());
-  if (s != TB_SUCCESS) fprintf(stderr, "TensorBLAS tc_ozimmu_syrk: %s %s\n", tb_status_string(s), tb_last_error());
+  report("tc_ozimmu_syrk",
+         tb::ozaki_syrk_impl(false, n, k, alpha, A, lda, beta, C, ldc, 10, 0, nullptr, 0, tb::current_stream()));
+}
+
+void tc_ozimmu_trsm(cublasHandle_t, long int m, long int n, double* A, long int lda, double* B, long int ldb,
+                    long int nb) {
+  report("tc_ozimmu_trsm", tb::ozaki_trsm_impl(true, m, n, A, lda, B, ldb, nb, 10, tb::current_stream()));
+}
+
+void tc_ozimmu_trmm(cublasHandle_t, long int m, long int n, double alpha, double* A, long int lda, double* B,
+                    long int ldb, double* C, long int ldc, long int) {
+  report("tc_ozimmu_trmm", tb::ozaki_trmm_impl(false, m, n, alpha, A, lda, B, ldb, C, ldc, 10, tb::current_stream()));
+}
+
+void tc_ozimmu_syr2k(cublasHandle_t, long int n, long int k, double alpha, double* A, long int lda, double* B,
+                     long int ldb, double beta, double* C, long int ldc, long int) {
+  report("tc_ozimmu_syr2k",
+         tb::ozaki_syr2k_impl(n, k, alpha, A, lda, B, ldb, beta, C, ldc, 10, tb::current_stream()));
 }

@@ -36,7 +36,8 @@ constexpr int kLeafMax = 512;  // largest diagonal block inverted explicitly
 // the identity). One warp per sub-block; lane c owns column c of the inverse
 // and runs forward substitution in FP64 registers; rows of L are broadcast
 // from shared memory. Output: D[t*1024 + i + 32*c] (column-major 32x32).
-__device__ __forceinline__ void diag_inv32_body(long long n, const float* __restrict__ A, long long lda,
+template <class T>
+__device__ __forceinline__ void diag_inv32_body(long long n, const T* __restrict__ A, long long lda,
                                                 double* __restrict__ D, long long t) {
   __shared__ double L[32][33];
   const int c = threadIdx.x;
@@ -63,9 +64,10 @@ __device__ __forceinline__ void diag_inv32_body(long long n, const float* __rest
   for (int i = 0; i < 32; ++i) D[t * 1024 + i + 32 * c] = w[i];
 }
 
-__global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const float* __restrict__ A, long long lda,
+template <class T>
+__global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const T* __restrict__ A, long long lda,
                                                         double* __restrict__ D) {
-  diag_inv32_body(n, A, lda, D, blockIdx.x);
+  diag_inv32_body<T>(n, A, lda, D, blockIdx.x);
 }
 
 // Grouped form: block b belongs to the job whose [first, first + count)
@@ -81,7 +83,7 @@ __global__ void __launch_bounds__(32) diag_inv32_grouped_kernel(const DiagJob* _
       hi = mid - 1;
   }
   const DiagJob& jb = jobs[lo];
-  diag_inv32_body(jb.n, jb.A, jb.lda, jb.D, b - jb.first);
+  diag_inv32_body<float>(jb.n, jb.A, jb.lda, jb.D, b - jb.first);
 }
 
 // Column chain j of the inverse of leaf block b (rows/cols [s, s+size)):
@@ -90,13 +92,16 @@ __global__ void __launch_bounds__(32) diag_inv32_grouped_kernel(const DiagJob* _
 // sub-block of L and each Dinv_i is staged (transposed) through shared memory
 // with coalesced loads; each of the 128 threads owns a 2 x 4 block of the
 // 32x32 result so every shared-memory load feeds several FMAs. The result is
-// written as the FP16 hi/lo pair (lo scaled by 2^11) of W, column-major with
-// leading dimension ldw, zeros above the diagonal.
+// written as the FP16 hi/lo pair (lo scaled by 2^11) of W, or as FP64 W when
+// w64 is given, column-major with leading dimension ldw, zeros above the
+// diagonal.
 constexpr int kChainThreads = 128;
 
-__device__ __forceinline__ void trtri_chain_body(const float* __restrict__ A, long long lda, int s, int size,
+template <class T>
+__device__ __forceinline__ void trtri_chain_body(const T* __restrict__ A, long long lda, int s, int size,
                                                  const double* __restrict__ D, __half* __restrict__ hi,
-                                                 __half* __restrict__ lo, long long ldw, int j) {
+                                                 __half* __restrict__ lo, double* __restrict__ w64, long long ldw,
+                                                 int j) {
   extern __shared__ __align__(16) double sm[];
   __shared__ __align__(16) double LsT[32][34];  // LsT[k][r] = L(r, k) of the staged sub-block (or Dinv_i)
   __shared__ __align__(16) double Ts[32][36];   // Ts[k][c]
@@ -179,6 +184,10 @@ __device__ __forceinline__ void trtri_chain_body(const float* __restrict__ A, lo
     for (int row = lr; row < size; row += 32) {
       double v = 0.0;
       if (row >= 32 * j) v = Wp[(row - 32 * j) * 32 + c];
+      if (w64) {
+        w64[row + (long long)gc * ldw] = v;
+        continue;
+      }
       const __half h = __float2half_rn((float)v);
       hi[row + (long long)gc * ldw] = h;
       lo[row + (long long)gc * ldw] = __float2half_rn((float)((v - (double)__half2float(h)) * 2048.0));
@@ -192,36 +201,27 @@ __global__ void __launch_bounds__(kChainThreads) trtri_chain_kernel(const float*
                                                                     __half* __restrict__ Whi, __half* __restrict__ Wlo,
                                                                     long long ldw, long long wstride) {
   const int2 leaf = leaves[blockIdx.y];  // {s, size}
-  trtri_chain_body(A, lda, leaf.x, leaf.y, D, Whi + (long long)blockIdx.y * wstride,
-                   Wlo + (long long)blockIdx.y * wstride, ldw, blockIdx.x);
+  trtri_chain_body<float>(A, lda, leaf.x, leaf.y, D, Whi + (long long)blockIdx.y * wstride,
+                          Wlo + (long long)blockIdx.y * wstride, nullptr, ldw, blockIdx.x);
+}
+
+// FP64 operand, FP64 inverse (the Ozaki-scheme FP64 TRSM's leaves).
+__global__ void __launch_bounds__(kChainThreads) trtri_chain_f64_kernel(const double* __restrict__ A, long long lda,
+                                                                        const int2* __restrict__ leaves,
+                                                                        const double* __restrict__ D,
+                                                                        double* __restrict__ W, long long ldw,
+                                                                        long long wstride) {
+  const int2 leaf = leaves[blockIdx.y];
+  trtri_chain_body<double>(A, lda, leaf.x, leaf.y, D, nullptr, nullptr, W + (long long)blockIdx.y * wstride, ldw,
+                           blockIdx.x);
 }
 
 // Grouped form: one job per (instance, leaf) along blockIdx.y.
 __global__ void __launch_bounds__(kChainThreads) trtri_chain_grouped_kernel(const ChainJob* __restrict__ jobs) {
   const ChainJob& jb = jobs[blockIdx.y];
-  trtri_chain_body(jb.A, jb.lda, jb.s, jb.size, jb.D, jb.Whi, jb.Wlo, jb.ldw, blockIdx.x);
+  trtri_chain_body<float>(jb.A, jb.lda, jb.s, jb.size, jb.D, jb.Whi, jb.Wlo, nullptr, jb.ldw, blockIdx.x);
 }
 
-struct TrsmCtx {
-  bool right;
-  long m, n;  // B is m x n
-  long nt;    // order of A (n for right, m for left)
-  float* B;
-  long ldb;
-  Split split;
-  int leaf;  // leaf block size (multiple of 64)
-  // FP16 copies
-  __half *ah, *al;  // A (nt x nt, MN-major, lda_h)
-  long long lda_h;
-  __half *xh, *xl;  // X: right: m x n col-major (ld ldx, MN-major operand)
-                    //    left : m x n col-major (ld ldx, K-major operand, rows = n)
-  long long ldx;
-  __half *wh, *wl;  // per-leaf inverses (ldw x leaf each)
-  long long ldw, wstride;
-  __half *rh, *rl;  // current leaf block of B
-  long long ldr;
-  cudaStream_t st;
-};
 
 // Leaf block [s, e): X_b = B_b * W^T (right) or W * B_b (left), W = inv(A_bb),
 // as a split-FP16 product. W is lower triangular, so each output tile only
@@ -375,19 +375,92 @@ tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblo
   return TB_SUCCESS;
 }
 
-tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float* B, long ldb, long nb, Split split,
-                    cudaStream_t st) {
+// FP64 inverses of the diagonal leaf blocks of an FP64 lower-triangular
+// matrix (order nt): leaf b = {s_b, size_b} (s_b a multiple of 32, size_b <=
+// 512) gets W_b = inv(A[s_b:, s_b:]) at W + b * wstride (ld ldw, zeros above
+// the diagonal). D: (nt + 31) / 32 * 1024 doubles of scratch; d_leaves: the
+// leaves in device memory.
+tb_status trsm_leaf_inverses_f64(long nt, const double* A, long lda, const int2* d_leaves, int nleaf, int max_size,
+                                 double* D, double* W, long long ldw, long long wstride, cudaStream_t st) {
+  const long nsub = (nt + 31) / 32;
+  diag_inv32_kernel<double><<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  const int max_chain = (max_size + 31) / 32;
+  const size_t smem = (size_t)max_chain * 1024 * sizeof(double);
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_done[dev]) {
+    TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kLeafMax / 32 * 1024 * sizeof(double))));
+    attr_done[dev] = true;
+  }
+  trtri_chain_f64_kernel<<<dim3((unsigned)max_chain, (unsigned)nleaf), kChainThreads, smem, st>>>(A, lda, d_leaves, D,
+                                                                                                 W, ldw, wstride);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
+
+// Set-up shared by every right-hand side of one triangular operand: scratch
+// for B blocks of at most `m` rows (right side) / `n` columns (left side),
+// the FP16 copy of A's lower part and the FP64 leaf inverses as FP16 hi/lo.
+// `scratch`: device memory of trsm_scratch_bytes(...) bytes, or nullptr to
+// take it from the pool.
+namespace {
+struct TrsmLayout {
+  size_t o_ah, o_al, o_xh, o_xl, o_wh, o_wl, o_rh, o_rl, o_d, o_lv, total;
+};
+
+TrsmLayout trsm_layout(TrsmCtx& c, long nleaf) {
+  const long nt = c.nt;
+  const bool hilo = c.split == Split::kHiLo;
+  c.lda_h = round_up(nt, 64);
+  // X copy: right: m x n, MN-major rows m; left: m x n col-major, K-major (K = m rows)
+  c.ldx = round_up(c.m, 64);
+  c.ldw = c.leaf;
+  c.wstride = c.ldw * c.leaf;
+  c.ldr = c.right ? round_up(c.m, 64) : c.leaf;
+  const size_t a_bytes = (size_t)c.lda_h * nt * 2;
+  const size_t x_bytes = (size_t)c.ldx * c.n * 2;
+  const size_t w_bytes = (size_t)c.wstride * nleaf * 2;
+  const size_t r_bytes = (size_t)c.ldr * (c.right ? c.leaf : c.n) * 2;
+  const size_t d_bytes = (size_t)((nt + 31) / 32) * 1024 * sizeof(double);
+  const size_t l_bytes = (size_t)nleaf * sizeof(int2);
+  TrsmLayout L;
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t o = off;
+    off += round_up((long long)b, 256);
+    return o;
+  };
+  L.o_ah = take(a_bytes);
+  L.o_al = hilo ? take(a_bytes) : 0;
+  L.o_xh = take(x_bytes);
+  L.o_xl = hilo ? take(x_bytes) : 0;
+  L.o_wh = take(w_bytes);
+  L.o_wl = take(w_bytes);
+  L.o_rh = take(r_bytes);
+  L.o_rl = take(r_bytes);
+  L.o_d = take(d_bytes);
+  L.o_lv = take(l_bytes);
+  L.total = off;
+  return L;
+}
+}  // namespace
+
+tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long nb, Split split, cudaStream_t st,
+                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start) {
   if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
   const long nt = right ? n : m;
-  if (lda < (nt > 1 ? nt : 1) || ldb < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
-  if (m == 0 || n == 0) return TB_SUCCESS;
-  TrsmCtx c;
+  if (lda < (nt > 1 ? nt : 1)) return TB_ERROR_INVALID_VALUE;
   c.right = right;
   c.m = m;
   c.n = n;
   c.nt = nt;
-  c.B = B;
-  c.ldb = ldb;
+  c.B = nullptr;
+  c.ldb = 0;
   // The reference's chunk planner (util/mat_size.cu:31-55) sends an order
   // below 2048 to FP32 cublasStrsm with no FP16 step at all
   // (BLAS/tc_trsm.cu:103-112); the plain form keeps that accuracy contract
@@ -399,59 +472,36 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   c.leaf = (int)leaf;
   const bool hilo = c.split == Split::kHiLo;
 
-  std::vector<long> leaf_start;
+  leaf_start.clear();
   std::vector<int2> leaves;
   for (long s = 0; s < nt; s += leaf) {
     leaf_start.push_back(s);
     leaves.push_back(make_int2((int)s, (int)std::min<long>(leaf, nt - s)));
   }
   const long nleaf = (long)leaves.size();
-
-  c.lda_h = round_up(nt, 64);
-  // X copy: right: m x n, MN-major rows m; left: m x n col-major, K-major (K = m rows)
-  c.ldx = round_up(m, 64);
-  c.ldw = leaf;
-  c.wstride = c.ldw * leaf;
-  c.ldr = right ? round_up(m, 64) : leaf;
-  const size_t a_bytes = (size_t)c.lda_h * nt * 2;
-  const size_t x_bytes = (size_t)c.ldx * n * 2;
-  const size_t w_bytes = (size_t)c.wstride * nleaf * 2;
-  const size_t r_bytes = (size_t)c.ldr * (right ? leaf : n) * 2;
-  const size_t d_bytes = (size_t)((nt + 31) / 32) * 1024 * sizeof(double);
-  const size_t l_bytes = (size_t)nleaf * sizeof(int2);
-  size_t off = 0;
-  auto take = [&](size_t b) {
-    size_t o = off;
-    off += round_up((long long)b, 256);
-    return o;
-  };
-  const size_t o_ah = take(a_bytes), o_al = hilo ? take(a_bytes) : 0;
-  const size_t o_xh = take(x_bytes), o_xl = hilo ? take(x_bytes) : 0;
-  const size_t o_wh = take(w_bytes), o_wl = take(w_bytes);
-  const size_t o_rh = take(r_bytes), o_rl = take(r_bytes);
-  const size_t o_d = take(d_bytes), o_lv = take(l_bytes);
-  char* ws = static_cast<char*>(pool_get(off));
+  const TrsmLayout L = trsm_layout(c, nleaf);
+  char* ws = static_cast<char*>(scratch ? scratch : pool_get(L.total));
   if (!ws) {
-    set_last_error("trsm: cannot allocate %zu bytes of scratch", off);
+    set_last_error("trsm: cannot allocate %zu bytes of scratch", L.total);
     return TB_ERROR_ALLOC;
   }
-  c.ah = reinterpret_cast<__half*>(ws + o_ah);
-  c.al = hilo ? reinterpret_cast<__half*>(ws + o_al) : nullptr;
-  c.xh = reinterpret_cast<__half*>(ws + o_xh);
-  c.xl = hilo ? reinterpret_cast<__half*>(ws + o_xl) : nullptr;
-  c.wh = reinterpret_cast<__half*>(ws + o_wh);
-  c.wl = reinterpret_cast<__half*>(ws + o_wl);
-  c.rh = reinterpret_cast<__half*>(ws + o_rh);
-  c.rl = reinterpret_cast<__half*>(ws + o_rl);
-  double* D = reinterpret_cast<double*>(ws + o_d);
-  int2* dleaves = reinterpret_cast<int2*>(ws + o_lv);
-  TB_CUDA_TRY(cudaMemcpyAsync(dleaves, leaves.data(), l_bytes, cudaMemcpyHostToDevice, st));
+  c.ah = reinterpret_cast<__half*>(ws + L.o_ah);
+  c.al = hilo ? reinterpret_cast<__half*>(ws + L.o_al) : nullptr;
+  c.xh = reinterpret_cast<__half*>(ws + L.o_xh);
+  c.xl = hilo ? reinterpret_cast<__half*>(ws + L.o_xl) : nullptr;
+  c.wh = reinterpret_cast<__half*>(ws + L.o_wh);
+  c.wl = reinterpret_cast<__half*>(ws + L.o_wl);
+  c.rh = reinterpret_cast<__half*>(ws + L.o_rh);
+  c.rl = reinterpret_cast<__half*>(ws + L.o_rl);
+  double* D = reinterpret_cast<double*>(ws + L.o_d);
+  int2* dleaves = reinterpret_cast<int2*>(ws + L.o_lv);
+  TB_CUDA_TRY(cudaMemcpyAsync(dleaves, leaves.data(), nleaf * sizeof(int2), cudaMemcpyHostToDevice, st));
 
   // 1. FP16 copy of A's lower part (only off-diagonal leaf blocks are read)
   if (nleaf > 1) TB_TRY(convert_f32_f16(nt, nt, A, lda, c.ah, c.al, c.lda_h, 2048.f, 2, st));
   // 2. inverses of the diagonal leaf blocks (FP64), as FP16 hi/lo
   const long nsub = (nt + 31) / 32;
-  diag_inv32_kernel<<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D);
+  diag_inv32_kernel<float><<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   const int max_chain = (int)(leaf / 32);
@@ -468,8 +518,45 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   trtri_chain_kernel<<<grid, kChainThreads, smem, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
-  // 3. recursion
-  return recurse(c, 0, nt, leaf_start);
+  return TB_SUCCESS;
+}
+
+size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split) {
+  TrsmCtx c;
+  c.right = right;
+  c.m = m;
+  c.n = n;
+  c.nt = right ? n : m;
+  c.split = (split == Split::kPlain && c.nt < 2048) ? Split::kHiLo : split;
+  long leaf = round_up(std::min<long>(nb, kLeafMax), 64);
+  c.leaf = (int)(leaf > kLeafMax ? kLeafMax : leaf);
+  return trsm_layout(c, (c.nt + c.leaf - 1) / c.leaf).total;
+}
+
+// Solves one right-hand side block with a prepared context: B is m' x n
+// (right side, m' <= the set-up m) or m x n' (left side, n' <= the set-up n).
+tb_status trsm_solve(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols) {
+  if (ldb < (rows > 1 ? rows : 1)) return TB_ERROR_INVALID_VALUE;
+  if (rows == 0 || cols == 0) return TB_SUCCESS;
+  c.B = B;
+  c.ldb = ldb;
+  if (c.right)
+    c.m = rows;
+  else
+    c.n = cols;
+  return recurse(c, 0, c.nt, leaf_start);
+}
+
+tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float* B, long ldb, long nb, Split split,
+                    cudaStream_t st) {
+  if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
+  const long nt = right ? n : m;
+  if (lda < (nt > 1 ? nt : 1) || ldb < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
+  if (m == 0 || n == 0) return TB_SUCCESS;
+  TrsmCtx c;
+  std::vector<long> leaf_start;
+  TB_TRY(trsm_setup(right, m, n, A, lda, nb, split, st, nullptr, c, leaf_start));
+  return trsm_solve(c, leaf_start, B, ldb, m, n);
 }
 
 }  // namespace tb

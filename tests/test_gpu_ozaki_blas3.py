@@ -1,0 +1,247 @@
+"""FP64 SYR2K / TRMM / TRSM (and transposed / K-chunked SYRK) on the INT8
+tensor cores (Ozaki scheme), against long-double and FP64 evaluations, the
+truncated-sum model of the oracle, and the reference's native-FP64 outputs.
+
+Reference interfaces: tc_ozimmu_syr2k (BLAS/tc_ozimmu_syr2k.cu:97-123),
+tc_ozimmu_trmm (BLAS/tc_ozimmu_trmm.cu:118-149), tc_ozimmu_trsm
+(BLAS/tc_ozimmu_trsm.cu:103-136), tc_ozimmu_syrk (BLAS/tc_ozimmu_syrk.cu).
+"""
+import ctypes
+import json
+import os
+import struct
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+import tb_oracle as orc
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+if GOLDEN not in sys.path:
+    sys.path.insert(0, GOLDEN)
+import golden_inputs as gi  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+P = ctypes.c_void_p
+L = ctypes.c_long
+D = ctypes.c_double
+
+
+def _lib(tblas):
+    lib = tblas.lib
+    lib.tb_dsyrk_ozaki.argtypes = [ctypes.c_char, ctypes.c_char, L, L, D, P, L, D, P, L, ctypes.c_int]
+    lib.tb_dsyr2k_ozaki.argtypes = [ctypes.c_char, ctypes.c_char, L, L, D, P, L, P, L, D, P, L, ctypes.c_int]
+    lib.tb_dtrmm_ozaki.argtypes = [ctypes.c_char, L, L, D, P, L, P, L, P, L, ctypes.c_int]
+    lib.tb_dtrsm_ozaki.argtypes = [ctypes.c_char, L, L, P, L, P, L, L, ctypes.c_int]
+    return lib
+
+
+def _dev(x):
+    """Column-major device copy of a host matrix."""
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(x, np.float64).T)).cuda()
+
+
+def _host(d):
+    return d.cpu().numpy().T
+
+
+def _rel(got, ref, mask=None):
+    d = (np.asarray(got, np.longdouble) - ref).astype(np.float64)
+    r = np.asarray(ref).astype(np.float64)
+    if mask is not None:
+        d, r = d[mask], r[mask]
+    return float(np.linalg.norm(d) / np.linalg.norm(r))
+
+
+def _wide(seed, shape, phi):
+    g = np.random.Generator(np.random.PCG64(seed))
+    return g.standard_normal(shape) * np.exp(phi * g.standard_normal(shape))
+
+
+@pytest.mark.parametrize("n,k,S", [(300, 500, 10), (128, 129, 12), (70, 1, 10)])
+def test_dsyr2k(tblas, n, k, S):
+    lib = _lib(tblas)
+    A, B = _wide(n + k, (n, k), 0.5), _wide(n * k, (n, k), 0.5)
+    C0 = np.random.default_rng(3).standard_normal((n, n))
+    dA, dB, dC = _dev(A), _dev(B), _dev(C0)
+    tblas._check(lib.tb_dsyr2k_ozaki(b"L", b"N", n, k, -1.5, dA.data_ptr(), n, dB.data_ptr(), n, 0.5, dC.data_ptr(),
+                                     n, S))
+    tblas.synchronize()
+    C = _host(dC)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    ex = -1.5 * (orc.gemm_extended(A, B) + orc.gemm_extended(B, A)) + 0.5 * C0.astype(np.longdouble)
+    model = -1.5 * orc.ozaki_gemm_model(np.hstack([A, B]), np.hstack([B, A]), S) + 0.5 * C0.astype(np.longdouble)
+    e_ex, e_model = _rel(C, ex, low), _rel(C, model, low)
+    print(f"dsyr2k n={n} k={k} S={S}: vs long double {e_ex:.3e}, vs model {e_model:.3e}")
+    assert e_model <= 1e-15
+    assert e_ex <= 1e-14
+    assert np.array_equal(np.triu(C, 1), np.triu(C0, 1))
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("m,n", [(384, 200), (257, 33), (1000, 130)])
+def test_dtrmm(tblas, uplo, m, n):
+    lib = _lib(tblas)
+    A = _wide(m + 7 * n, (m, m), 0.5)
+    B = _wide(m * n, (m, n), 0.5)
+    At = np.tril(A) if uplo == "L" else np.triu(A)
+    Ag = A.copy()
+    Ag[(np.triu(np.ones((m, m)), 1) if uplo == "L" else np.tril(np.ones((m, m)), -1)).astype(bool)] = np.nan
+    dA, dB = _dev(Ag), _dev(B)
+    dC = torch.full((n, m), 7.0, dtype=torch.float64, device="cuda")
+    tblas._check(lib.tb_dtrmm_ozaki(uplo.encode(), m, n, 2.0, dA.data_ptr(), m, dB.data_ptr(), m, dC.data_ptr(), m,
+                                    10))
+    tblas.synchronize()
+    C = _host(dC)
+    ex = 2.0 * orc.gemm_extended(At, B.T)
+    model = 2.0 * orc.ozaki_gemm_model(At, B.T, 10)
+    e_ex, e_model = _rel(C, ex), _rel(C, model)
+    print(f"dtrmm {uplo} m={m} n={n}: vs long double {e_ex:.3e}, vs model {e_model:.3e}")
+    assert np.all(np.isfinite(C))
+    assert e_model <= 1e-15
+    assert e_ex <= 1e-14
+
+
+@pytest.mark.parametrize("side", ["R", "L"])
+@pytest.mark.parametrize("m,n,nb", [(512, 1024, 256), (300, 700, 128), (1000, 64, 512), (64, 1537, 512)])
+def test_dtrsm(tblas, side, m, n, nb):
+    from scipy.linalg import solve_triangular
+
+    lib = _lib(tblas)
+    nt = n if side == "R" else m
+    g = np.random.Generator(np.random.PCG64(m + 3 * n + nb))
+    A = np.tril(g.uniform(-1, 1, (nt, nt)) / np.sqrt(nt), -1) + np.diag(g.uniform(1, 2, nt))
+    B = g.uniform(-1, 1, (m, n))
+    Ag = A.copy()
+    Ag[np.triu(np.ones((nt, nt), dtype=bool), 1)] = np.nan  # never read
+    dA, dB = _dev(Ag), _dev(B)
+    tblas._check(lib.tb_dtrsm_ozaki(side.encode(), m, n, dA.data_ptr(), nt, dB.data_ptr(), m, nb, 10))
+    tblas.synchronize()
+    X = _host(dB)
+    ref = solve_triangular(A, B.T, lower=True).T if side == "R" else solve_triangular(A, B, lower=True)
+    resid = (X @ A.T - B) if side == "R" else (A @ X - B)
+    err = float(np.linalg.norm(X - ref) / np.linalg.norm(ref))
+    res = float(np.linalg.norm(resid) / np.linalg.norm(B))
+    print(f"dtrsm {side} m={m} n={n} nb={nb}: vs FP64 solve {err:.3e}, residual {res:.3e}")
+    assert err <= 1e-13
+    assert res <= 1e-14
+
+
+def test_dsyrk_trans_and_k_chunks(tblas):
+    """trans 'T' (A k x n) and k above the INT32-exact chunk (14 slices:
+    k <= 9472 per chunk) both reach FP64 accuracy."""
+    lib = _lib(tblas)
+    n, k, S = 96, 10000, 14
+    A = _wide(9, (n, k), 0.5)
+    dAt = torch.from_numpy(np.ascontiguousarray(A)).cuda()  # column-major k x n = A^T
+    dC = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+    tblas._check(lib.tb_dsyrk_ozaki(b"L", b"T", n, k, 1.0, dAt.data_ptr(), k, 0.0, dC.data_ptr(), n, S))
+    tblas.synchronize()
+    C = _host(dC)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    e = _rel(C, orc.gemm_extended(A, A), low)
+    print(f"dsyrk trans, k={k} in two chunks: vs long double {e:.3e}")
+    assert e <= 1e-15
+
+
+def _load(name):
+    z = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+    return z, json.loads(str(z["meta"]))
+
+
+def test_fp64_family_vs_reference(tblas):
+    """Direct parity with the reference's tc_ozimmu_trsm / _trmm / _syr2k
+    outputs (native FP64 there) on the recorded seeded inputs."""
+    lib = _lib(tblas)
+    z, meta = _load("dtrsm_small")
+    m, n, nb = meta["m"], meta["n"], meta["nb"]
+    A = gi.lower_tri(meta["seed"], n).astype(np.float64)
+    B = gi.rng(meta["seed"] + 1).uniform(-1, 1, (m, n))
+    dA, dB = _dev(A), _dev(B)
+    tblas._check(lib.tb_dtrsm_ozaki(b"R", m, n, dA.data_ptr(), n, dB.data_ptr(), m, nb, 10))
+    tblas.synchronize()
+    e = float(np.linalg.norm(_host(dB) - z["X"]) / np.linalg.norm(z["X"]))
+    print(f"dtrsm vs reference {e:.3e}")
+    assert e <= 1e-13
+
+    z, meta = _load("dtrmm_small")
+    m, n = meta["m"], meta["n"]
+    g = gi.rng(meta["seed"])
+    A = np.tril(g.standard_normal((m, m)))
+    B = g.standard_normal((m, n))
+    dA, dB = _dev(A), _dev(B)
+    dC = torch.zeros(n, m, dtype=torch.float64, device="cuda")
+    tblas._check(lib.tb_dtrmm_ozaki(b"L", m, n, 1.0, dA.data_ptr(), m, dB.data_ptr(), m, dC.data_ptr(), m, 10))
+    tblas.synchronize()
+    e = float(np.linalg.norm(_host(dC) - z["C"]) / np.linalg.norm(z["C"]))
+    print(f"dtrmm vs reference {e:.3e}")
+    assert e <= 1e-14
+
+    z, meta = _load("dsyr2k_small")
+    n, k = meta["n"], meta["k"]
+    g = gi.rng(meta["seed"])
+    A = g.standard_normal((n, k))
+    B = g.standard_normal((n, k))
+    dA, dB = _dev(A), _dev(B)
+    dC = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+    tblas._check(lib.tb_dsyr2k_ozaki(b"L", b"N", n, k, 1.0, dA.data_ptr(), n, dB.data_ptr(), n, 0.0,
+                                     dC.data_ptr(), n, 10))
+    tblas.synchronize()
+    low = np.tril(np.ones((n, n), dtype=bool))
+    C = _host(dC)
+    ex = orc.gemm_extended(A, B) + orc.gemm_extended(B, A)
+    e_ex = _rel(C, ex, low)
+    # The reference's FP64 SYR2K reads the 4-byte float &sone as its FP64
+    # beta (BLAS/tc_ozimmu_syr2k.cu; 8 bytes = two 1.0f = 0.0078125018...)
+    # and returns B A^T + 0.0078125 A B^T. Parity modulo that defect: our
+    # result with A B^T re-weighted the same way equals the reference's.
+    beta_read = struct.unpack("<d", struct.pack("<ff", 1.0, 1.0))[0]
+    as_ref = C - (1.0 - beta_read) * (A @ B.T)
+    e_ref = float(np.linalg.norm((as_ref - z["C"])[low]) / np.linalg.norm(z["C"][low]))
+    print(f"dsyr2k vs long double {e_ex:.3e}; vs reference (its beta defect applied) {e_ref:.3e}")
+    assert e_ex <= 1e-15
+    assert e_ref <= 1e-13
+
+
+def test_cxx_entry_points_match_c_abi(tblas):
+    """tc_ozimmu_trsm / _trmm / _syr2k (the reference's C++ signatures,
+    include/TensorBLAS.h:151,157,163) give the same bits as the C ABI."""
+    lib = _lib(tblas)
+    f_trsm = lib["_Z14tc_ozimmu_trsmP13cublasContextllPdlS1_ll"]
+    f_trsm.argtypes = [P, L, L, P, L, P, L, L]
+    f_trmm = lib["_Z14tc_ozimmu_trmmP13cublasContextlldPdlS1_lS1_ll"]
+    f_trmm.argtypes = [P, L, L, D, P, L, P, L, P, L, L]
+    f_syr2k = lib["_Z15tc_ozimmu_syr2kP13cublasContextlldPdlS1_ldS1_ll"]
+    f_syr2k.argtypes = [P, L, L, D, P, L, P, L, D, P, L, L]
+    for f in (f_trsm, f_trmm, f_syr2k):
+        f.restype = None
+    g = np.random.Generator(np.random.PCG64(77))
+    m, n = 200, 600
+    A = np.tril(g.uniform(-1, 1, (n, n)) / np.sqrt(n), -1) + np.diag(g.uniform(1, 2, n))
+    B = g.uniform(-1, 1, (m, n))
+    dA, dB1, dB2 = _dev(A), _dev(B), _dev(B)
+    f_trsm(None, m, n, dA.data_ptr(), n, dB1.data_ptr(), m, 256)
+    tblas._check(lib.tb_dtrsm_ozaki(b"R", m, n, dA.data_ptr(), n, dB2.data_ptr(), m, 256, 10))
+    tblas.synchronize()
+    assert torch.equal(dB1, dB2)
+    T = np.tril(g.standard_normal((m, m)))
+    Bm = g.standard_normal((m, 70))
+    dT, dBm = _dev(T), _dev(Bm)
+    c1 = torch.zeros(70, m, dtype=torch.float64, device="cuda")
+    c2 = torch.zeros_like(c1)
+    f_trmm(None, m, 70, 1.0, dT.data_ptr(), m, dBm.data_ptr(), m, c1.data_ptr(), m, 64)
+    tblas._check(lib.tb_dtrmm_ozaki(b"L", m, 70, 1.0, dT.data_ptr(), m, dBm.data_ptr(), m, c2.data_ptr(), m, 10))
+    tblas.synchronize()
+    assert torch.equal(c1, c2)
+    X, Y = g.standard_normal((m, 90)), g.standard_normal((m, 90))
+    dX, dY = _dev(X), _dev(Y)
+    s1 = torch.zeros(m, m, dtype=torch.float64, device="cuda")
+    s2 = torch.zeros_like(s1)
+    f_syr2k(None, m, 90, 1.0, dX.data_ptr(), m, dY.data_ptr(), m, 0.0, s1.data_ptr(), m, 64)
+    tblas._check(lib.tb_dsyr2k_ozaki(b"L", b"N", m, 90, 1.0, dX.data_ptr(), m, dY.data_ptr(), m, 0.0, s2.data_ptr(), m,
+                                     10))
+    tblas.synchronize()
+    assert torch.equal(s1, s2)

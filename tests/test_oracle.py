@@ -2,6 +2,7 @@
 outputs recorded in tests/golden/ (planner: util/mat_size.cu; SYRK/TRSM:
 BLAS/tc_syrk.cu, BLAS/tc_trsm.cu run on a B200 by make_golden.py)."""
 import json
+import struct
 import os
 import sys
 
@@ -206,3 +207,55 @@ def test_ozaki_slicing_reconstructs_exactly():
         rec = sum(Q[s].astype(np.float64) * 2.0 ** (-7 * (s + 1)) for s in range(S)) * np.ldexp(1.0, e)[:, None]
         assert np.all(np.abs(rec - A) <= np.ldexp(1.0, e)[:, None] * 2.0 ** (-7 * S))
         assert np.abs(Q).max() <= 127
+
+
+def test_ozaki_gemm_model_accuracy():
+    """The truncated two-operand Ozaki sum approximates A B^T to FP64 level
+    once 7S covers 53 bits plus the in-row exponent spread, and degrades
+    (as it must) when the slices are too few."""
+    g = gi.rng(6)
+    A = g.standard_normal((48, 300)) * np.exp(0.5 * g.standard_normal((48, 300)))
+    B = g.standard_normal((40, 300)) * np.exp(0.5 * g.standard_normal((40, 300)))
+    ex = orc.gemm_extended(A, B)
+    err = lambda C: float(np.linalg.norm((C - ex).astype(np.float64)) / np.linalg.norm(ex.astype(np.float64)))  # noqa
+    assert err(orc.ozaki_gemm_model(A, B, 10)) <= 1e-15
+    assert err(orc.ozaki_gemm_model(A, B, 3)) >= 1e-7
+
+
+def test_fp64_golden_pins():
+    """The reference's native-FP64 tc_ozimmu_trsm / _trmm / _syr2k outputs
+    (recorded on a B200) agree with FP64/long-double evaluations of the same
+    seeded inputs: the fixtures the FP64 GPU parity tests compare against."""
+    from scipy.linalg import solve_triangular
+
+    z, meta = load("dtrsm_small")
+    m, n = meta["m"], meta["n"]
+    A = gi.lower_tri(meta["seed"], n).astype(np.float64)
+    B = gi.rng(meta["seed"] + 1).uniform(-1, 1, (m, n))
+    X = solve_triangular(A, B.T, lower=True).T  # X A^T = B
+    assert np.linalg.norm(z["X"] - X) / np.linalg.norm(X) <= 1e-13
+
+    z, meta = load("dtrmm_small")
+    m, n = meta["m"], meta["n"]
+    g = gi.rng(meta["seed"])
+    A = np.tril(g.standard_normal((m, m)))
+    B = g.standard_normal((m, n))
+    ex = orc.gemm_extended(A, B.T)
+    assert np.linalg.norm((z["C"] - ex).astype(np.float64)) / np.linalg.norm(ex.astype(np.float64)) <= 1e-15
+
+    # tc_ozimmu_syr2k passes &sone, a 4-byte float (include/TensorBLAS.h:169),
+    # as the beta of its second FP64 cublasGemmEx (BLAS/tc_ozimmu_syr2k.cu,
+    # the rest_n / nn branches): the GEMM reads 8 bytes, two adjacent 1.0f,
+    # i.e. beta = 0x3F8000003F800000 = 0.0078125018..., so the reference
+    # returns B A^T + 0.0078125 A B^T instead of A B^T + B A^T. The fixture
+    # pins that defect exactly; the library computes the correct sum.
+    z, meta = load("dsyr2k_small")
+    n, k = meta["n"], meta["k"]
+    g = gi.rng(meta["seed"])
+    A = g.standard_normal((n, k))
+    B = g.standard_normal((n, k))
+    beta_read = struct.unpack("<d", struct.pack("<ff", 1.0, 1.0))[0]
+    ex = orc.gemm_extended(B, A) + beta_read * orc.gemm_extended(A, B)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    d = (z["C"] - ex)[low].astype(np.float64)
+    assert np.linalg.norm(d) / np.linalg.norm(ex[low].astype(np.float64)) <= 1e-15
