@@ -110,6 +110,23 @@ TB_API tb_status tb_ssymm(char uplo, long m, long n, float alpha, const float* A
                           float beta, float* C, long ldc, int precision);
 
 /*
+ * Host-memory forms (no single reference counterpart: the reference's
+ * callers copy whole operands to the device around tc_syrk / tc_trsm, e.g.
+ * python/TensorBLAS.py:11-68, testing/testing_syrk.cu). A, B and C are host
+ * pointers (page-locked memory gives full PCIe speed; pageable memory works
+ * but its copies do not overlap). The call streams them through device
+ * staging buffers in panels, overlapping host->device copies, the tensor-core
+ * work and device->host copies on two internal copy streams; only the
+ * referenced triangle of A (TRSM) and of C (SYRK) crosses the bus. Arguments
+ * and results are those of tb_ssyrk ('L', 'N'; k > 0, alpha != 0) and
+ * tb_strsm. Synchronous: returns when the results are in host memory.
+ */
+TB_API tb_status tb_ssyrk_host(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
+                               float beta, float* C, long ldc, long nb, int precision);
+TB_API tb_status tb_strsm_host(char side, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
+                               int precision);
+
+/*
  * tb_ssyrk_noalloc: tb_ssyrk for callers that cannot allocate device memory
  * (no counterpart in the reference library). Same arguments and results as
  * tb_ssyrk, but every byte of scratch comes from one static 64 MiB device

@@ -66,7 +66,8 @@ tb_status syr2k_impl(long n, long k, float alpha, const float* A, long lda, cons
   c.beta = beta;
   c.tri = 1;
   c.flops = 2.0 * (double)n * (double)(n + 1) * (double)k;
-  return run(c, plan_lower((int)n, gemm_bn(split), 0, (int)((2 * k + kGemmBK - 1) / kGemmBK)), st);
+  c.kblocks = (int)((2 * k + kGemmBK - 1) / kGemmBK);
+  return run(c, plan_lower((int)n, gemm_bn(split, c.kblocks), 0, c.kblocks), st);
 }
 
 tb_status trmm_impl(bool upper, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
@@ -100,7 +101,9 @@ tb_status trmm_impl(bool upper, long m, long n, float alpha, const float* A, lon
   c.beta = 0.f;
   c.flops = (double)m * m * n;
   const int kb = (int)((m + kGemmBK - 1) / kGemmBK);
-  std::vector<int4> plan = plan_rect((int)m, (int)n, gemm_bn(split), 0, kb);
+  c.kblocks = kb;
+  const int bn = gemm_bn(split, kb);
+  std::vector<int4> plan = plan_rect((int)m, (int)n, bn, 0, kb);
   for (int4& t : plan) {
     if (upper) {
       t.z = t.x / kGemmBK;  // A(i, p) = 0 for p < i
@@ -142,7 +145,8 @@ tb_status symm_impl(bool lower, long m, long n, float alpha, const float* A, lon
   c.alpha = alpha;
   c.beta = beta;
   c.flops = 2.0 * (double)m * m * n;
-  return run(c, plan_rect((int)m, (int)n, gemm_bn(split), 0, (int)((m + kGemmBK - 1) / kGemmBK)), st);
+  c.kblocks = (int)((m + kGemmBK - 1) / kGemmBK);
+  return run(c, plan_rect((int)m, (int)n, gemm_bn(split, c.kblocks), 0, c.kblocks), st);
 }
 
 }  // namespace tb

@@ -118,10 +118,14 @@ tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t strea
 }  // namespace
 
 int gemm_bn(Split s) { return s == Split::kPlain ? 256 : 128; }
+int gemm_bn(Split s, int kblocks) {
+  const bool pf = kblocks > 0 && kblocks <= kGemmPfMaxKb;
+  return (s == Split::kPlain && !pf) ? 256 : 128;
+}
 
 tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
   const bool split = c.split == Split::kHiLo;
-  const int bn = gemm_bn(c.split);
+  const int bn = gemm_bn(c.split, c.kblocks);
   GemmArgs& a = *out;
   memset(&a, 0, sizeof(a));
   TB_TRY(make_map(&a.mapA[0], c.a_hi, kGemmBM));
@@ -170,6 +174,19 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   TB_TRY(gemm_build_args(c, &a));
   const bool split = c.split == Split::kHiLo;
   const bool amn = c.a_hi.mn_major, bmn = c.b_hi.mn_major;
+  if (c.kblocks > 0 && c.kblocks <= kGemmPfMaxKb) {
+    if (!split) {
+      if (amn && bmn) return launch_variant<GemmCfg<128, 1, true, true, true>, false>(a, c.num_tiles, stream, c.flops);
+      if (amn && !bmn) return launch_variant<GemmCfg<128, 1, true, false, true>, false>(a, c.num_tiles, stream, c.flops);
+      if (!amn && !bmn)
+        return launch_variant<GemmCfg<128, 1, false, false, true>, false>(a, c.num_tiles, stream, c.flops);
+      return launch_variant<GemmCfg<128, 1, false, true, true>, false>(a, c.num_tiles, stream, c.flops);
+    }
+    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true, true>, false>(a, c.num_tiles, stream, c.flops);
+    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false, true>, false>(a, c.num_tiles, stream, c.flops);
+    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false, true>, false>(a, c.num_tiles, stream, c.flops);
+    return launch_variant<GemmCfg<128, 3, false, true, true>, false>(a, c.num_tiles, stream, c.flops);
+  }
   if (!split) {
     if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>, false>(a, c.num_tiles, stream, c.flops);
     if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>, false>(a, c.num_tiles, stream, c.flops);

@@ -89,22 +89,31 @@ __device__ __forceinline__ const GemmArgs& tile_problem(const GemmArgs& args, in
   }
 }
 
-template <int BN_, int NSPLIT_, bool A_MN_, bool B_MN_>
+// PF (prefetch) variants serve launches whose tiles have few K-blocks: there
+// the epilogue, not the MMA, bounds the tile, so they trade pipeline stages
+// for one shared-memory slot per 32-column chunk of the tile. The whole C
+// tile is requested by TMA as soon as the previous tile's stores have left
+// shared memory -- while this tile's MMAs still run -- instead of one chunk
+// at a time inside the epilogue; fp16 side copies get two staging buffers.
+template <int BN_, int NSPLIT_, bool A_MN_, bool B_MN_, bool PF_ = false>
 struct GemmCfg {
   static constexpr int BM = 128, BN = BN_, BK = 64;
   static constexpr int NSPLIT = NSPLIT_;
   static constexpr bool A_MN = A_MN_, B_MN = B_MN_;
+  static constexpr bool PF = PF_;
   static constexpr int NOPS = (NSPLIT == 1) ? 1 : 2;  // copies per operand (hi[, lo])
   static constexpr int A_BYTES = BM * BK * 2;
   static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE_BYTES = NOPS * (A_BYTES + B_BYTES);
-  static constexpr int STAGES = (STAGE_BYTES <= 48 * 1024) ? 4 : 3;
+  static constexpr int STAGES = PF ? (NSPLIT == 1 ? 4 : 2) : ((STAGE_BYTES <= 48 * 1024) ? 4 : 3);
   static constexpr int NACC = (NSPLIT == 1) ? 1 : 2;
   static constexpr int ACC_COLS = NACC * BN;  // TMEM columns per accumulation buffer
   static constexpr int TMEM_COLS = 2 * ACC_COLS;
   static_assert(TMEM_COLS <= 512, "TMEM budget");
   static constexpr int EPI_CHUNK_BYTES = 128 * 32 * 4;  // one staged 128 x 32 fp32 chunk
-  static constexpr int EPI_BYTES = 2 * EPI_CHUNK_BYTES;
+  static constexpr int C_SLOTS = PF ? BN / 32 : 2;      // C-chunk staging slots (and their load barriers)
+  static constexpr int SIDE_BYTES = PF ? 2 * EPI_CHUNK_BYTES : 0;  // PF: two fp16 hi/lo side buffers
+  static constexpr int EPI_BYTES = C_SLOTS * EPI_CHUNK_BYTES + SIDE_BYTES;
   static constexpr int BAR_BYTES = 256;
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + BAR_BYTES;
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
@@ -243,6 +252,68 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
   ++es.chunk;
 }
 
+// PF epilogue, one 128 x 32 chunk (index c of the tile, columns gj0..gj0+31).
+// Its C values (when needed) were requested into slot c at the start of the
+// tile; the result is combined in place and stored from the same slot. Side
+// copies alternate between two fp16 buffers. All 128 epilogue threads call
+// it together; pf.lphase / pf.side stay identical across them.
+struct PfState {
+  uint32_t lphase;  // per-slot phase bits of the C-load barriers
+  int side;         // side-copy chunks written so far (selects the buffer)
+};
+
+__device__ __forceinline__ void epilogue_chunk_pf(const GemmArgs& args, float* slots, __half* side_base,
+                                                  uint64_t* cload, PfState& pf, const float* v, int m0, int gj0,
+                                                  int c, int row, bool need_load, bool issuer,
+                                                  volatile int* abort_flag) {
+  const bool side = args.tma_out != 0 && gj0 < args.out_n && m0 < args.out_m;
+  float* S = slots + c * (128 * 32);
+  __half* Hs = side_base + (pf.side & 1) * (2 * 128 * 32);
+  __half* Ls = Hs + 128 * 32;
+  // the side buffer's previous store (two side chunks ago) has read it
+  if (side && issuer) bulk_wait_read<1>();
+  named_bar_sync(1, 128);
+  const long long gi = (long long)m0 + row;
+  float r[32];
+  if (need_load) {
+    mbar_wait(&cload[c], (pf.lphase >> c) & 1u, abort_flag, args.err, kDevErrTimeoutEpilogue);
+    pf.lphase ^= 1u << c;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float old = S[j * 128 + row];
+      const bool masked = args.tri && (gi - (long long)(gj0 + j)) < args.diag;
+      r[j] = masked ? old : fmaf(args.beta, old, args.alpha * v[j]);
+      S[j * 128 + row] = r[j];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      r[j] = args.alpha * v[j];
+      S[j * 128 + row] = r[j];
+    }
+  }
+  if (side) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const __half hv = __float2half_rn(r[j]);
+      Hs[j * 128 + row] = hv;
+      Ls[j * 128 + row] = __float2half_rn((r[j] - __half2float(hv)) * args.out_lo_scale);
+    }
+  }
+  fence_proxy_async_smem();
+  named_bar_sync(1, 128);
+  if (issuer) {
+    tma_store_2d(&args.mapC, S, m0, gj0);
+    if (side) {
+      tma_store_2d(&args.mapOut[0], Hs, m0, gj0);
+      if (args.out_lo) tma_store_2d(&args.mapOut[1], Ls, m0, gj0);
+    }
+    bulk_commit();
+  }
+  if (!args.tma_out && args.out_hi && gi < args.out_m) store_fp16_copies(args, r, gi, gj0);
+  if (side) ++pf.side;
+}
+
 template <class Cfg, bool GROUPED>
 __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ GemmArgs args) {
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
@@ -254,8 +325,8 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
   uint64_t* tfull = empty + STAGES;  // [2]
   uint64_t* tempty = tfull + 2;      // [2]
   uint64_t* drain = tempty + 2;      // [1] teardown barrier for the MMA issuer
-  uint64_t* cload = drain + 1;       // [2] C-chunk loads of the TMA epilogue
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + 2);
+  uint64_t* cload = drain + 1;       // [C_SLOTS] C-chunk loads of the TMA epilogue
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + Cfg::C_SLOTS);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5;
@@ -269,8 +340,8 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4);
-      mbar_init(&cload[b], 1);
     }
+    for (int b = 0; b < Cfg::C_SLOTS; ++b) mbar_init(&cload[b], 1);
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -421,6 +492,109 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
     EpiState es{0, 0u};
     int it = 0;
     bool ok = true;
+    if constexpr (Cfg::PF) {
+      PfState pf{0u, 0};
+      uint32_t pending = 0;  // issuer: slots whose C load is in flight and not yet consumed
+      __half* side_base = reinterpret_cast<__half*>(stage_c + Cfg::C_SLOTS * (128 * 32));
+      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+        const int4 tile = args.tiles[t];
+        const GemmArgs& P = tile_problem<GROUPED>(args, t);
+        const long long gi = (long long)tile.x + row;
+        const bool row_ok = gi < P.M;
+        const bool tile_masked = P.tri && ((long long)tile.x - (long long)(tile.y + BN - 1)) < P.diag;
+        const bool need_load = P.tma_c && (P.beta != 0.0f || tile_masked);
+        // request this tile's C while its MMAs run; slots are free once the
+        // previous tile's stores have read them
+        if (issuer && P.tma_c) {
+          bulk_wait_read<0>();
+          if (need_load)
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c)
+              if (tile.y + 32 * c < P.N) {
+                mbar_arrive_expect_tx(&cload[c], Cfg::EPI_CHUNK_BYTES);
+                tma_load_2d(stage_c + c * (128 * 32), &P.mapC, &cload[c], tile.x, tile.y + 32 * c);
+                pending |= 1u << c;
+              }
+        }
+        if constexpr (Cfg::NSPLIT == 1) {
+          const int buf = it & 1;
+          const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+          ++it;
+          if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+#pragma unroll 1
+          for (int c0 = 0; c0 < BN; c0 += 32) {
+            float v[32];
+            tmem_ld32(tacc + c0, v);
+            if (c0 == BN - 32) {
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&tempty[buf]);
+            }
+            if (tile.y + c0 >= P.N) continue;
+            if (P.tma_c) {
+              epilogue_chunk_pf(P, stage_c, side_base, cload, pf, v, tile.x, tile.y + c0, c0 / 32, row, need_load,
+                                issuer, abort_flag);
+              pending &= ~(1u << (c0 / 32));
+            } else if (row_ok)
+              epilogue_store32(P, v, gi, (long long)tile.y + c0);
+          }
+        } else {
+          float acc[BN];
+#pragma unroll
+          for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+          for (int c0k = tile.z; c0k < tile.w; c0k += args.kchunk) {
+            const int buf = it & 1;
+            const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+            ++it;
+            if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+#pragma unroll
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+              float v[32], w[32];
+              tmem_ld32(tacc + c0, v);
+              tmem_ld32(tacc + BN + c0, w);
+#pragma unroll
+              for (int j = 0; j < 32; ++j) acc[c0 + j] += fmaf(args.corr_scale, w[j], v[j]);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[buf]);
+          }
+          if (!ok) break;
+#pragma unroll
+          for (int c0 = 0; c0 < BN; c0 += 32) {
+            if (tile.y + c0 >= P.N) continue;
+            if (P.tma_c) {
+              epilogue_chunk_pf(P, stage_c, side_base, cload, pf, acc + c0, tile.x, tile.y + c0, c0 / 32, row,
+                                need_load, issuer, abort_flag);
+              pending &= ~(1u << (c0 / 32));
+            } else if (row_ok)
+              epilogue_store32(P, acc + c0, gi, (long long)tile.y + c0);
+          }
+        }
+      }
+      if (issuer && pending) {
+        // abort path: C loads still in flight must land before the CTA exits
+        for (int c = 0; c < Cfg::C_SLOTS; ++c) {
+          if (!((pending >> c) & 1u)) continue;
+          const uint64_t t0 = globaltimer_ns();
+          while (!mbar_try_wait(&cload[c], (pf.lphase >> c) & 1u))
+            if (globaltimer_ns() - t0 > 1000000000ull) {
+              if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
+              break;
+            }
+        }
+      }
+    } else
     for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
       const int4 tile = args.tiles[t];
       const GemmArgs& P = tile_problem<GROUPED>(args, t);

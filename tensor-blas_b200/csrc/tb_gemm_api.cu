@@ -46,8 +46,8 @@ tb_status gemm_impl(bool ta, bool tb_, long m, long n, long k, float alpha, cons
   c.b_hi.mn_major = tb_;
   c.b_lo = c.b_hi;
   c.b_lo.ptr = bl;
-  const int bn = gemm_bn(split);
-  const std::vector<int4> plan = plan_rect((int)m, (int)n, bn, 0, (int)((k + kGemmBK - 1) / kGemmBK));
+  c.kblocks = (int)((k + kGemmBK - 1) / kGemmBK);
+  const std::vector<int4> plan = plan_rect((int)m, (int)n, gemm_bn(split, c.kblocks), 0, c.kblocks);
   c.tiles = upload_tiles(plan, st);
   if (!c.tiles) return TB_ERROR_ALLOC;
   c.num_tiles = (int)plan.size();

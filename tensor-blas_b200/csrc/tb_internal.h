@@ -28,9 +28,12 @@ void set_last_error(const char* fmt, ...);
 
 // ------------------------------------------------------------------ streams / pool
 cudaStream_t current_stream();
-// Device scratch owned by the library (grow-only, per device). Returns
-// nullptr on allocation failure. Growing synchronises the device.
-void* pool_get(size_t bytes);
+// Device scratch owned by the library (grow-only, per device and slot).
+// Slot 0 serves the routines' own scratch; slot 1 the host-memory entry
+// points' staging buffers, which live across routine calls. Returns nullptr
+// on allocation failure. Growing synchronises the device.
+constexpr int kPoolSlots = 2;
+void* pool_get(size_t bytes, int slot = 0);
 // Device error word used by bounded waits inside kernels (per device).
 int* device_error_word();
 // Reads and clears the device error word (synchronises `stream`).
@@ -77,14 +80,19 @@ struct GemmCall {
   long long ld_out = 0;
   float out_lo_scale = 2048.0f;
   int out_m = -1, out_n = -1;  // side-copy region (default: all of C)
+  int kblocks = 0;   // most K-blocks (64) of any tile; 0 < kblocks <= kGemmPfMaxKb selects the prefetch variants
   double flops = 0;  // algorithmic flops of this launch (profiling only)
   int* err = nullptr;  // device error word (nullptr: the library's per-device word)
 };
 
-// Tile width along N used by the engine for a given split mode.
-int gemm_bn(Split s);
+// Tile width along N used by the engine for a given split mode (and, with
+// kblocks = the most K-blocks of any tile, for the prefetch variants that
+// launches with short K ranges use: plain tiles are then 128 wide).
 constexpr int kGemmBM = 128;
 constexpr int kGemmBK = 64;
+constexpr int kGemmPfMaxKb = 32;
+int gemm_bn(Split s);
+int gemm_bn(Split s, int kblocks);
 
 tb_status gemm_launch(const GemmCall& call, cudaStream_t stream);
 

@@ -18,8 +18,8 @@ cudaStream_t g_stream = nullptr;
 
 constexpr int kMaxDevices = 64;
 struct DeviceState {
-  void* pool = nullptr;
-  size_t pool_bytes = 0;
+  void* pool[kPoolSlots] = {nullptr, nullptr};
+  size_t pool_bytes[kPoolSlots] = {0, 0};
   int* err = nullptr;
   int sms = 0;
 };
@@ -104,26 +104,26 @@ int sm_count() {
   return s->sms;
 }
 
-void* pool_get(size_t bytes) {
+void* pool_get(size_t bytes, int slot) {
   std::lock_guard<std::mutex> lk(g_mu);
   DeviceState* s = state();
-  if (!s) return nullptr;
+  if (!s || slot < 0 || slot >= kPoolSlots) return nullptr;
   if (bytes == 0) bytes = 256;
-  if (s->pool_bytes >= bytes) return s->pool;
-  if (s->pool) {
+  if (s->pool_bytes[slot] >= bytes) return s->pool[slot];
+  if (s->pool[slot]) {
     cudaDeviceSynchronize();  // work queued on the old buffer must finish
-    cudaFree(s->pool);
-    s->pool = nullptr;
-    s->pool_bytes = 0;
+    cudaFree(s->pool[slot]);
+    s->pool[slot] = nullptr;
+    s->pool_bytes[slot] = 0;
   }
   size_t want = (size_t)round_up((long long)bytes, 1 << 20);
-  if (cudaMalloc(&s->pool, want) != cudaSuccess) {
+  if (cudaMalloc(&s->pool[slot], want) != cudaSuccess) {
     cudaGetLastError();
-    s->pool = nullptr;
+    s->pool[slot] = nullptr;
     return nullptr;
   }
-  s->pool_bytes = want;
-  return s->pool;
+  s->pool_bytes[slot] = want;
+  return s->pool[slot];
 }
 
 int* device_error_word() {

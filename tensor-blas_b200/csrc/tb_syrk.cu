@@ -63,8 +63,8 @@ tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, lon
   Operand opl = op;
   opl.ptr = lo;
 
-  const int bn = gemm_bn(split);
   const int kb = (int)((k + kGemmBK - 1) / kGemmBK);
+  const int bn = gemm_bn(split, kb);
   const int4* tiles = upload_tiles(plan_lower((int)n, bn, 0, kb), st);
   if (!tiles) return TB_ERROR_ALLOC;
   GemmCall c;
@@ -73,6 +73,7 @@ tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, lon
   c.split = split;
   c.tiles = tiles;
   c.num_tiles = (int)plan_lower((int)n, bn, 0, kb).size();
+  c.kblocks = kb;
   c.C = C;
   c.ldc = ldc;
   c.M = (int)n;

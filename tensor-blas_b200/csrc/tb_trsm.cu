@@ -266,8 +266,9 @@ tb_status leaf_solve(TrsmCtx& c, int bidx, long s, long e) {
   g.alpha = 1.f;
   g.beta = 0.f;
   g.flops = (double)g.M * g.N * nbl;  // triangular solve of the leaf: other * nbl^2 flops
-  const int bn = gemm_bn(g.split);
-  std::vector<int4> plan = plan_rect(g.M, g.N, bn, 0, (int)((nbl + kGemmBK - 1) / kGemmBK));
+  g.kblocks = (int)((nbl + kGemmBK - 1) / kGemmBK);
+  const int bn = gemm_bn(g.split, g.kblocks);
+  std::vector<int4> plan = plan_rect(g.M, g.N, bn, 0, g.kblocks);
   for (int4& t : plan) {  // K (= columns of W) beyond the tile's last W row is zero
     const long lim = c.right ? (long)t.y + bn : (long)t.x + kGemmBM;
     const long kmax = lim < nbl ? lim : nbl;
@@ -322,7 +323,8 @@ tb_status update(TrsmCtx& c, long s, long mid, long e) {
   else
     g.out_m = (int)next;
   g.flops = 2.0 * g.M * g.N * kk;
-  const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split), 0, (int)((kk + kGemmBK - 1) / kGemmBK));
+  g.kblocks = (int)((kk + kGemmBK - 1) / kGemmBK);
+  const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split, g.kblocks), 0, g.kblocks);
   g.tiles = upload_tiles(plan, c.st);
   if (!g.tiles) return TB_ERROR_ALLOC;
   g.num_tiles = (int)plan.size();

@@ -63,6 +63,10 @@ lib.tb_ssyrk.argtypes = [ctypes.c_char, ctypes.c_char, _c_long, _c_long, ctypes.
 lib.tb_ssyrk.restype = ctypes.c_int
 lib.tb_strsm.argtypes = [ctypes.c_char, _c_long, _c_long, _fp, _c_long, _fp, _c_long, _c_long, ctypes.c_int]
 lib.tb_strsm.restype = ctypes.c_int
+lib.tb_ssyrk_host.argtypes = lib.tb_ssyrk.argtypes
+lib.tb_ssyrk_host.restype = ctypes.c_int
+lib.tb_strsm_host.argtypes = lib.tb_strsm.argtypes
+lib.tb_strsm_host.restype = ctypes.c_int
 
 
 class TensorBLASError(RuntimeError):
@@ -133,6 +137,31 @@ def ssyrk(A_cm, C_cm, n, k, lda, ldc, alpha=1.0, beta=0.0, trans="N", nb=256, pr
 def strsm(side, A_cm, B_cm, m, n, lda, ldb, nb=512, precision=PLAIN):
     """Raw column-major STRSM (lower, non-unit); side 'R': X A^T = B, 'L': A X = B."""
     _check(lib.tb_strsm(side.encode(), m, n, A_cm.data_ptr(), lda, B_cm.data_ptr(), ldb, nb, precision))
+
+
+def _host_f32(t, name):
+    if t.device.type != "cpu" or t.dtype != torch.float32 or not t.is_contiguous():
+        raise TypeError(f"{name} must be a contiguous float32 CPU tensor (page-locked for full speed)")
+
+
+def ssyrk_host(A_cm, C_cm, n, k, lda, ldc, alpha=1.0, beta=0.0, nb=256, precision=PLAIN):
+    """Column-major SSYRK (lower, 'N') with A and C in host memory; the call
+    overlaps the copies with the tensor-core work and returns when C is
+    written (see tb_ssyrk_host)."""
+    _host_f32(A_cm, "A")
+    _host_f32(C_cm, "C")
+    lib.tb_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    _check(lib.tb_ssyrk_host(b"L", b"N", n, k, alpha, A_cm.data_ptr(), lda, beta, C_cm.data_ptr(), ldc, nb,
+                             precision))
+
+
+def strsm_host(side, A_cm, B_cm, m, n, lda, ldb, nb=512, precision=PLAIN):
+    """Column-major STRSM (lower, non-unit) with A and B in host memory; B is
+    overwritten by X (see tb_strsm_host)."""
+    _host_f32(A_cm, "A")
+    _host_f32(B_cm, "B")
+    lib.tb_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    _check(lib.tb_strsm_host(side.encode(), m, n, A_cm.data_ptr(), lda, B_cm.data_ptr(), ldb, nb, precision))
 
 
 def syrk(A, alpha=1.0, beta=0.0, C=None, nb=256, precision=PLAIN):
