@@ -90,7 +90,7 @@ struct GemmCall {
 // launches with short K ranges use: plain tiles are then 128 wide).
 constexpr int kGemmBM = 128;
 constexpr int kGemmBK = 64;
-constexpr int kGemmPfMaxKb = 32;
+constexpr int kGemmPfMaxKb = 16;
 int gemm_bn(Split s);
 int gemm_bn(Split s, int kblocks);
 
