@@ -254,6 +254,17 @@ def run_mine(args, world, rank, local):
     step(TB.SPLIT)
     TB.synchronize()
     err_split = fp64_errors(n, A, C, T, B0, Bw) if rank == 0 else None
+    # ---- TRSM alone in each precision, with the refinement sweep (plain
+    # solve + split-product residual + plain correction) beside plain / split
+    trsm_only = {}
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split"), (TB.REFINE, "refine")):
+        ms_t = _median_ms(lambda: TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, prec), 5,  # noqa: B023
+                          lambda: Bw.copy_(B0))
+        Bw.copy_(B0)
+        TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, prec)
+        TB.synchronize()
+        e = fp64_errors(n, A, C, T, B0, Bw)["trsm"] if rank == 0 else None
+        trsm_only[name] = {"ms": ms_t, "tflops": float(n) ** 3 / (ms_t * 1e-3) / 1e12, "errors_vs_fp64": e}
 
     value = world * args.steps * flops_step / (ms_plain * 1e-3) / 1e12
     value_split = world * args.steps * flops_step / (ms_split * 1e-3) / 1e12
@@ -322,6 +333,7 @@ def run_mine(args, world, rank, local):
         "chosen": {"precision": "split (FP16 hi + scaled lo, 3 products, RN folds)", "value": value_split,
                    "ms_per_step": ms_split / args.steps, "ratio_vs_plain": value_split / value,
                    "errors_vs_fp64": err_split},
+        "trsm_16384_by_precision": trsm_only,
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "steps": args.e2e_steps, "ms_per_step": ms_e2e / args.e2e_steps,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "api": "TensorBLAS.ssyrk_host / TensorBLAS.strsm_host (tb_ssyrk_host / tb_strsm_host) on page-locked "
@@ -362,8 +374,8 @@ def _median_ms(fn, reps, prep=None):
 
 def blas3_config(TB, ref_lib):
     """SYR2K n=16384 k=4096, TRMM left/upper m=n=16384 and SYMM left/lower
-    m=n=16384 with entries N(0,1) * 2^U(-8,8): plain and split, each with a
-    sampled FP64 error, beside the reference's tc_syr2k / tc_trmm / tc_symm
+    m=n=16384 with entries N(0,1) * 2^U(-8,8): plain, split and FP8-e4m3
+    (per-128x128-block scaled), each with a sampled FP64 error, beside the reference's tc_syr2k / tc_trmm / tc_symm
     on inputs of the same shape (its TRMM is lower-only; the flops are the
     same). Flop conventions: SYR2K 2 n^2 k, TRMM m^2 n, SYMM 2 m^2 n."""
     import ctypes
@@ -380,7 +392,8 @@ def blas3_config(TB, ref_lib):
 
     def err(got, ref):
         d = np.abs(got - ref)
-        return float(np.linalg.norm(d) / np.linalg.norm(ref))
+        return {"norm_rel": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+                "max_rel": float(np.max(d / np.maximum(np.abs(ref), 1e-300)))}
 
     out = {}
     n, k = 16384, 4096
@@ -393,12 +406,12 @@ def blas3_config(TB, ref_lib):
     lo, hi = np.maximum(i, j), np.minimum(i, j)
     ref = np.einsum("pk,pk->k", Ah[:, lo], Bh[:, hi]) + np.einsum("pk,pk->k", Bh[:, lo], Ah[:, hi])
     entry = {"n": n, "k": k, "flops": 2.0 * n * n * k}
-    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split")):
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split"), (TB.FP8, "fp8")):
         run = lambda: TB._check(lib.tb_ssyr2k(b"L", b"N", n, k, 1.0, A.data_ptr(), n, B.data_ptr(), n,  # noqa: E731
                                               0.0, C.data_ptr(), n, 256, prec))
         ms = _median_ms(run, 5)
         got = C.cpu().numpy()[hi, lo].astype(np.float64)
-        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "err_vs_fp64": err(got, ref)}
+        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "errors_vs_fp64": err(got, ref)}
     if ref_lib is not None:
         t = ref_lib.ref_time_syr2k(n, k, 256, A.cpu().numpy().ctypes.data_as(P), B.cpu().numpy().ctypes.data_as(P),
                                    1, 3)
@@ -417,12 +430,12 @@ def blas3_config(TB, ref_lib):
     # TRMM upper: C(i, j) = sum_{p >= i} A(i, p) B(p, j)
     ref = np.array([np.dot(An[ii:, ii].astype(np.float64), Bn[jj, ii:].astype(np.float64)) for ii, jj in zip(i, j)])
     entry = {"m": m, "n": n, "uplo": "U", "flops": float(m) * m * n}
-    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split")):
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split"), (TB.FP8, "fp8")):
         run = lambda: TB._check(lib.tb_strmm(b"U", m, n, 1.0, A.data_ptr(), m, B.data_ptr(), m,  # noqa: E731
                                              C.data_ptr(), m, 256, prec))
         ms = _median_ms(run, 5)
         got = C.cpu().numpy()[j, i].astype(np.float64)
-        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "err_vs_fp64": err(got, ref)}
+        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "errors_vs_fp64": err(got, ref)}
     if ref_lib is not None:
         t = ref_lib.ref_time_trmm(m, n, 256, An.ctypes.data_as(P), Bn.ctypes.data_as(P), 1, 3)
         entry["reference_plain_ms"] = t
@@ -436,12 +449,12 @@ def blas3_config(TB, ref_lib):
         ref.append(np.dot(row, Bn[jj, :].astype(np.float64)))
     ref = np.array(ref)
     entry = {"m": m, "n": n, "uplo": "L", "flops": 2.0 * m * m * n}
-    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split")):
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split"), (TB.FP8, "fp8")):
         run = lambda: TB._check(lib.tb_ssymm(b"L", m, n, 1.0, A.data_ptr(), m, B.data_ptr(), m, 0.0,  # noqa: E731
                                              C.data_ptr(), m, prec))
         ms = _median_ms(run, 5)
         got = C.cpu().numpy()[j, i].astype(np.float64)
-        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "err_vs_fp64": err(got, ref)}
+        entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "errors_vs_fp64": err(got, ref)}
     if ref_lib is not None:
         t = ref_lib.ref_time_symm(m, n, An.ctypes.data_as(P), Bn.ctypes.data_as(P), 1, 3)
         entry["reference_plain_ms"] = t

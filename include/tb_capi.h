@@ -33,7 +33,14 @@ typedef enum {
   /* FP16 hi + scaled-lo split of both operands, 3 tensor-core products with
    * the correction in a separate FP32 accumulator: FP32-level accuracy (the
    * role of the reference's tc_cumpsgemm_* / CUMPSGEMM_FP16TCEC). */
-  TB_PREC_SPLIT = 1
+  TB_PREC_SPLIT = 1,
+  /* e4m3 operands scaled per 128 x 128 block, FP32 accumulation (normwise
+   * error ~1e-2 on wide-range data): SYRK, SYR2K, TRMM, SYMM and GEMM only. */
+  TB_PREC_FP8 = 2,
+  /* TRSM only: plain solve plus one refinement sweep (residual with the
+   * split products, correction with a second plain solve): FP32-level
+   * accuracy from the FP16 path. */
+  TB_PREC_REFINE = 3
 } tb_precision;
 
 /* Library/stream control. `stream` is a cudaStream_t (NULL = default). */
@@ -64,8 +71,9 @@ TB_API tb_status tb_sgemm(char transa, char transb, long m, long n, long k, floa
                           const float* B, long ldb, float beta, float* C, long ldc, int precision);
 
 /*
- * SYRK: C = alpha * op(A) * op(A)^T + beta * C, lower triangle of C written
- * (diagonal included); the strict upper triangle is left untouched.
+ * SYRK: C = alpha * op(A) * op(A)^T + beta * C, the `uplo` triangle of C
+ * ('L' lower, 'U' upper, diagonal included) written; the other strict
+ * triangle is left untouched.
  *   trans 'N': A is n x k (lda >= n).   trans 'T': A is k x n (lda >= k).
  * Replaces tc_syrk (BLAS/tc_syrk.cu:126-157, include/TensorBLAS.h:139) and,
  * with TB_PREC_SPLIT, tc_cumpsgemm_syrk (BLAS/tc_cumpsgemm_syrk.cu:3-125).
@@ -86,6 +94,20 @@ TB_API tb_status tb_strsm(char side, long m, long n, const float* A, long lda, f
                           int precision);
 
 /*
+ * General TRSM, B overwritten by X, BLAS flag meanings (no single reference
+ * counterpart: the reference solves right/lower/transpose/non-unit only):
+ *   side 'L': op(A) X = B, A m x m;   side 'R': X op(A) = B, A n x n
+ *   uplo 'L'/'U': the triangle of A that is read; transa 'N'/'T': op(A) = A / A^T;
+ *   diag 'N'/'U': stored or unit diagonal (a unit diagonal is never read).
+ * The six forms other than left/lower/'N' and right/lower/'T' run on those
+ * two through a remapped copy of A's triangle (transposed and/or order-
+ * reversed) and, where the order is reversed, an in-place reversal of B's
+ * rows (left) or columns (right) around the solve.
+ */
+TB_API tb_status tb_strsm_ex(char side, char uplo, char transa, char diag, long m, long n, const float* A, long lda,
+                             float* B, long ldb, long nb, int precision);
+
+/*
  * SYR2K: C = alpha (A B^T + B A^T) + beta C, lower triangle written, A and B
  * n x k (trans 'N'). Replaces tc_syr2k (BLAS/tc_syr2k.cu:116-152) and, with
  * TB_PREC_SPLIT, tc_cumpsgemm_syr2k (BLAS/tc_cumpsgemm_syr2k.cu).
@@ -100,6 +122,16 @@ TB_API tb_status tb_ssyr2k(char uplo, char trans, long n, long k, float alpha, c
  */
 TB_API tb_status tb_strmm(char uplo, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
                           float* C, long ldc, long nb, int precision);
+
+/*
+ * General TRMM, out of place, BLAS flag meanings (no single reference
+ * counterpart: the reference has left/lower/no-trans/non-unit only):
+ *   side 'L': C = alpha op(A) B, A m x m;   side 'R': C = alpha B op(A), A n x n
+ *   uplo 'L'/'U': the triangle of A that is read; transa 'N'/'T': op(A) = A / A^T;
+ *   diag 'N'/'U': stored or unit diagonal. B and C are m x n.
+ */
+TB_API tb_status tb_strmm_ex(char side, char uplo, char transa, char diag, long m, long n, float alpha,
+                             const float* A, long lda, const float* B, long ldb, float* C, long ldc, int precision);
 
 /*
  * SYMM (left): C = alpha A B + beta C, A m x m symmetric with triangle `uplo`
@@ -153,8 +185,9 @@ TB_API tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, float a
  * 7 * slices exceeds 53 bits plus the in-row exponent spread. The reference's
  * tc_ozimmu_* drivers run native FP64 cuBLAS GEMMs instead.
  *
- * SYRK: C = alpha op(A) op(A)^T + beta C, lower triangle; A n x k ('N') or
- * k x n ('T'). Replaces tc_ozimmu_syrk (BLAS/tc_ozimmu_syrk.cu:108-143).
+ * SYRK: C = alpha op(A) op(A)^T + beta C, the `uplo` triangle ('L' or 'U');
+ * A n x k ('N') or k x n ('T'). Replaces tc_ozimmu_syrk
+ * (BLAS/tc_ozimmu_syrk.cu:108-143).
  */
 TB_API tb_status tb_dsyrk_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
                                 double beta, double* C, long ldc, int slices);

@@ -259,3 +259,52 @@ def syrk_extended(A, rows, cols):
     the higher-than-FP64 oracle for the FP64-emulation checks."""
     Al = np.asarray(A, dtype=np.float64).astype(np.longdouble)
     return np.einsum("ij,ij->i", Al[rows], Al[cols])
+
+
+def e4m3(y):
+    """Round float values to FP8 e4m3 (round to nearest even, saturating at
+    +-448; normal exponents -6..8, subnormal step 2^-9), as float64."""
+    y = np.asarray(y, dtype=np.float64)
+    a = np.abs(y)
+    _, E = np.frexp(np.where(a > 0, a, 1.0))
+    e = np.maximum(E - 1, -6)                  # exponent of the binade (subnormals share -6)
+    step = np.ldexp(1.0, e - 3)                # 3 stored mantissa bits
+    q = np.round(a / step) * step              # numpy rounds half to even
+    q = np.minimum(q, 448.0)
+    return np.where(a > 0, np.sign(y) * q, 0.0)
+
+
+def fp8_quantize(X, block=128):
+    """Per-(128-row, 128-deep) block scaled e4m3 copy of an operand X (rows x
+    K, row i = one K-vector): s = float32(max|x| / 448) (1 for an all-zero
+    block), q = e4m3(float32(x / s)). Returns (Q float64 rows x K, S [rb, kb])."""
+    X = np.asarray(X, dtype=np.float32)
+    rows, K = X.shape
+    rb, kb = -(-rows // block), -(-K // block)
+    Q = np.zeros((rows, K))
+    S = np.ones((rb, kb), dtype=np.float32)
+    for i in range(rb):
+        for j in range(kb):
+            blk = X[i * block:(i + 1) * block, j * block:(j + 1) * block]
+            m = np.float32(np.max(np.abs(blk))) if blk.size else np.float32(0)
+            s = np.float32(m / np.float32(448.0)) if m > 0 else np.float32(1.0)
+            S[i, j] = s
+            Q[i * block:(i + 1) * block, j * block:(j + 1) * block] = e4m3((blk / s).astype(np.float32))
+    return Q, S
+
+
+def fp8_product_model(A, B, block=128):
+    """sum over 128-deep K blocks of s_A s_B (Q_A Q_B^T) for A (M x K) and
+    B (N x K), in float64: what the FP8 engine computes before rounding."""
+    QA, SA = fp8_quantize(A, block)
+    QB, SB = fp8_quantize(B, block)
+    M, K = QA.shape
+    N = QB.shape[0]
+    C = np.zeros((M, N))
+    for kb in range(SA.shape[1]):
+        ks = slice(kb * block, (kb + 1) * block)
+        P = QA[:, ks] @ QB[:, ks].T
+        sa = np.repeat(SA[:, kb].astype(np.float64), block)[:M]
+        sb = np.repeat(SB[:, kb].astype(np.float64), block)[:N]
+        C += P * sa[:, None] * sb[None, :]
+    return C

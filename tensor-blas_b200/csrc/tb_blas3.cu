@@ -27,12 +27,7 @@ void* scratch(void* ws, size_t ws_bytes, size_t need) {
   return (ws && ws_bytes >= need) ? ws : pool_get(need);
 }
 
-tb_status run(GemmCall& c, const std::vector<int4>& plan, cudaStream_t st) {
-  c.tiles = upload_tiles(plan, st);
-  if (!c.tiles) return TB_ERROR_ALLOC;
-  c.num_tiles = (int)plan.size();
-  return gemm_launch(c, st);
-}
+tb_status run(GemmCall& c, const std::vector<int4>& plan, cudaStream_t st) { return gemm_launch_plan(c, plan, st); }
 
 }  // namespace
 
@@ -70,14 +65,21 @@ tb_status syr2k_impl(long n, long k, float alpha, const float* A, long lda, cons
   return run(c, plan_lower((int)n, gemm_bn(split, c.kblocks), 0, c.kblocks), st);
 }
 
-tb_status trmm_impl(bool upper, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
-                    float* C, long ldc, long nb, Split split, void* ws, size_t ws_bytes, cudaStream_t st) {
-  if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
-  if (lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1) || ldc < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
+// General TRMM, out of place: C = alpha op(A) B (left, A m x m) or
+// C = alpha B op(A) (right, A n x n); op(A) = A or A^T, A lower or upper
+// triangular (the other triangle is never read), unit or stored diagonal.
+// The triangle becomes a per-tile K range; op(A) is read from one FP16 copy
+// of A in whichever orientation the product needs.
+tb_status trmm_ex_impl(bool right, bool upper, bool trans, bool unit, long m, long n, float alpha, const float* A,
+                       long lda, const float* B, long ldb, float* C, long ldc, Split split, void* ws, size_t ws_bytes,
+                       cudaStream_t st, float beta) {
+  const long na = right ? n : m;  // order of A
+  if (m < 0 || n < 0) return TB_ERROR_INVALID_VALUE;
+  if (lda < (na > 1 ? na : 1) || ldb < (m > 1 ? m : 1) || ldc < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
   if (m == 0 || n == 0) return TB_SUCCESS;
   const bool hilo = split == Split::kHiLo;
-  const long long ldh = round_up(m, 64);
-  const size_t abytes = (size_t)ldh * m * 2, bbytes = (size_t)ldh * n * 2;
+  const long long lda_h = round_up(na, 64), ldb_h = round_up(m, 64);
+  const size_t abytes = (size_t)round_up(lda_h * na * 2, 256), bbytes = (size_t)round_up(ldb_h * n * 2, 256);
   const size_t need = (abytes + bbytes) * (hilo ? 2 : 1);
   char* buf = static_cast<char*>(scratch(ws, ws_bytes, need));
   if (!buf) return TB_ERROR_ALLOC;
@@ -85,34 +87,62 @@ tb_status trmm_impl(bool upper, long m, long n, float alpha, const float* A, lon
   __half* bh = reinterpret_cast<__half*>(buf + abytes);
   __half* al = hilo ? reinterpret_cast<__half*>(buf + abytes + bbytes) : nullptr;
   __half* bl = hilo ? reinterpret_cast<__half*>(buf + 2 * abytes + bbytes) : nullptr;
-  TB_TRY(convert_f32_f16(m, m, A, lda, ah, al, ldh, 2048.f, upper ? 3 : 1, st));
-  TB_TRY(convert_f32_f16(m, n, B, ldb, bh, bl, ldh, 2048.f, 0, st));
+  TB_TRY(convert_f32_f16(na, na, A, lda, ah, al, lda_h, 2048.f, upper ? 3 : 1, st));
+  if (unit) TB_TRY(set_unit_diag(na, ah, al, lda_h, st));
+  TB_TRY(convert_f32_f16(m, n, B, ldb, bh, bl, ldb_h, 2048.f, 0, st));
+  const bool op_lower = upper == trans;  // op(A) lower triangular
   GemmCall c;
   c.split = split;
-  c.a_hi = {ah, m, m, ldh, true};
-  c.a_lo = {al, m, m, ldh, true};
-  c.b_hi = {bh, n, m, ldh, false};  // B(p, j): K-major with rows = n
-  c.b_lo = {bl, n, m, ldh, false};
+  if (!right) {
+    // C(i, j) = sum_p op(A)(i, p) B(p, j): op(A) rows from the copy (MN-major
+    // for A, K-major for A^T); B as K-major rows j
+    c.a_hi = {ah, m, m, lda_h, !trans};
+    c.a_lo = {al, m, m, lda_h, !trans};
+    c.b_hi = {bh, n, m, ldb_h, false};
+    c.b_lo = {bl, n, m, ldb_h, false};
+  } else {
+    // C(i, j) = sum_p B(i, p) op(A)(p, j): B MN-major; op(A)^T rows j (K-major
+    // for A, MN-major for A^T)
+    c.a_hi = {bh, m, n, ldb_h, true};
+    c.a_lo = {bl, m, n, ldb_h, true};
+    c.b_hi = {ah, n, n, lda_h, trans};
+    c.b_lo = {al, n, n, lda_h, trans};
+  }
   c.C = C;
   c.ldc = ldc;
   c.M = (int)m;
   c.N = (int)n;
   c.alpha = alpha;
-  c.beta = 0.f;
-  c.flops = (double)m * m * n;
-  const int kb = (int)((m + kGemmBK - 1) / kGemmBK);
+  c.beta = beta;
+  c.flops = (double)m * n * na;
+  const int kb = (int)((na + kGemmBK - 1) / kGemmBK);
   c.kblocks = kb;
   const int bn = gemm_bn(split, kb);
   std::vector<int4> plan = plan_rect((int)m, (int)n, bn, 0, kb);
   for (int4& t : plan) {
-    if (upper) {
-      t.z = t.x / kGemmBK;  // A(i, p) = 0 for p < i
+    if (!right) {
+      if (op_lower) {
+        const long lim = (long)t.x + kGemmBM < na ? (long)t.x + kGemmBM : na;
+        t.w = (int)((lim + kGemmBK - 1) / kGemmBK);  // op(A)(i, p) = 0 for p > i
+      } else {
+        t.z = t.x / kGemmBK;  // op(A)(i, p) = 0 for p < i
+      }
     } else {
-      const long lim = (long)t.x + kGemmBM < m ? (long)t.x + kGemmBM : m;
-      t.w = (int)((lim + kGemmBK - 1) / kGemmBK);  // A(i, p) = 0 for p > i
+      if (op_lower) {
+        t.z = t.y / kGemmBK;  // op(A)(p, j) = 0 for p < j
+      } else {
+        const long lim = (long)t.y + bn < na ? (long)t.y + bn : na;
+        t.w = (int)((lim + kGemmBK - 1) / kGemmBK);  // op(A)(p, j) = 0 for p > j
+      }
     }
   }
   return run(c, plan, st);
+}
+
+tb_status trmm_impl(bool upper, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
+                    float* C, long ldc, long nb, Split split, void* ws, size_t ws_bytes, cudaStream_t st) {
+  if (nb <= 0) return TB_ERROR_INVALID_VALUE;
+  return trmm_ex_impl(false, upper, false, false, m, n, alpha, A, lda, B, ldb, C, ldc, split, ws, ws_bytes, st);
 }
 
 tb_status symm_impl(bool lower, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
@@ -165,6 +195,13 @@ extern "C" tb_status tb_ssyr2k(char uplo, char trans, long n, long k, float alph
     tb::set_last_error("tb_ssyr2k: only trans='N' is supported");
     return TB_ERROR_NOT_SUPPORTED;
   }
+  if (precision == TB_PREC_FP8) {
+    if (n < 0 || k < 0 || nb <= 0 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) || ldc < (n > 1 ? n : 1))
+      return TB_ERROR_INVALID_VALUE;
+    if (n == 0) return TB_SUCCESS;
+    if (k > 0 && alpha != 0.f) return tb::syr2k_fp8(n, k, alpha, A, lda, B, ldb, beta, C, ldc, tb::current_stream());
+    precision = TB_PREC_PLAIN;  // k == 0 / alpha == 0: C = beta C, no products
+  }
   if (!prec_ok(precision)) return TB_ERROR_INVALID_VALUE;
   return tb::syr2k_impl(n, k, alpha, A, lda, B, ldb, beta, C, ldc, nb, to_split(precision), nullptr, 0,
                         tb::current_stream());
@@ -179,9 +216,44 @@ extern "C" tb_status tb_strmm(char uplo, long m, long n, float alpha, const floa
     upper = true;
   else
     return TB_ERROR_INVALID_VALUE;
+  if (precision == TB_PREC_FP8) {
+    if (m < 0 || n < 0 || nb <= 0 || lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1) || ldc < (m > 1 ? m : 1))
+      return TB_ERROR_INVALID_VALUE;
+    if (m == 0 || n == 0) return TB_SUCCESS;
+    return tb::trmm_fp8(false, upper, false, false, m, n, alpha, A, lda, B, ldb, C, ldc, tb::current_stream());
+  }
   if (!prec_ok(precision)) return TB_ERROR_INVALID_VALUE;
   return tb::trmm_impl(upper, m, n, alpha, A, lda, B, ldb, C, ldc, nb, to_split(precision), nullptr, 0,
                        tb::current_stream());
+}
+
+extern "C" tb_status tb_strmm_ex(char side, char uplo, char transa, char diag, long m, long n, float alpha,
+                                 const float* A, long lda, const float* B, long ldb, float* C, long ldc, int precision) {
+  auto flag = [](char c, char a, char b, bool* v) {
+    if (c == a || c == a + ('a' - 'A')) {
+      *v = false;
+      return true;
+    }
+    if (c == b || c == b + ('a' - 'A')) {
+      *v = true;
+      return true;
+    }
+    return false;
+  };
+  bool right, upper, trans, unit;
+  if (!flag(side, 'L', 'R', &right) || !flag(uplo, 'L', 'U', &upper) || !flag(diag, 'N', 'U', &unit))
+    return TB_ERROR_INVALID_VALUE;
+  if (!flag(transa, 'N', 'T', &trans) && !flag(transa, 'N', 'C', &trans)) return TB_ERROR_INVALID_VALUE;
+  if (precision == TB_PREC_FP8) {
+    const long na = right ? n : m;
+    if (m < 0 || n < 0 || lda < (na > 1 ? na : 1) || ldb < (m > 1 ? m : 1) || ldc < (m > 1 ? m : 1))
+      return TB_ERROR_INVALID_VALUE;
+    if (m == 0 || n == 0) return TB_SUCCESS;
+    return tb::trmm_fp8(right, upper, trans, unit, m, n, alpha, A, lda, B, ldb, C, ldc, tb::current_stream());
+  }
+  if (!prec_ok(precision)) return TB_ERROR_INVALID_VALUE;
+  return tb::trmm_ex_impl(right, upper, trans, unit, m, n, alpha, A, lda, B, ldb, C, ldc, to_split(precision),
+                          nullptr, 0, tb::current_stream());
 }
 
 extern "C" tb_status tb_ssymm(char uplo, long m, long n, float alpha, const float* A, long lda, const float* B,
@@ -193,6 +265,12 @@ extern "C" tb_status tb_ssymm(char uplo, long m, long n, float alpha, const floa
     lower = false;
   else
     return TB_ERROR_INVALID_VALUE;
+  if (precision == TB_PREC_FP8) {
+    if (m < 0 || n < 0 || lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1) || ldc < (m > 1 ? m : 1))
+      return TB_ERROR_INVALID_VALUE;
+    if (m == 0 || n == 0) return TB_SUCCESS;
+    return tb::symm_fp8(lower, m, n, alpha, A, lda, B, ldb, beta, C, ldc, tb::current_stream());
+  }
   if (!prec_ok(precision)) return TB_ERROR_INVALID_VALUE;
   return tb::symm_impl(lower, m, n, alpha, A, lda, B, ldb, beta, C, ldc, to_split(precision), nullptr, 0,
                        tb::current_stream());

@@ -151,4 +151,22 @@ tb_status convert_f32_f16(long long rows, long long cols, const float* src, long
   return TB_SUCCESS;
 }
 
+namespace {
+__global__ void unit_diag_kernel(long long n, __half* hi, __half* lo, long long ld) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  hi[i + i * ld] = __float2half_rn(1.f);
+  if (lo) lo[i + i * ld] = __float2half_rn(0.f);
+}
+}  // namespace
+
+// Unit diagonal in an FP16 copy (hi = 1, lo = 0) for diag = 'U' operands.
+tb_status set_unit_diag(long long n, __half* hi, __half* lo, long long ld, cudaStream_t stream) {
+  if (n <= 0) return TB_SUCCESS;
+  unit_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(n, hi, lo, ld);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
+
 }  // namespace tb

@@ -1,6 +1,7 @@
 // Host side of the tcgen05 GEMM engine: tensor-map encoding, tile planning,
 // variant dispatch and launch.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -67,6 +68,32 @@ tb_status make_map(CUtensorMap* map, const Operand& op, int box_rows) {
   return TB_SUCCESS;
 }
 
+// Tensor map for a K-major e4m3 operand (one byte per element): box
+// {128 (K), box_rows}, 128B swizzle.
+tb_status make_map8(CUtensorMap* map, const Operand& op, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_last_error("cuTensorMapEncodeTiled unavailable");
+    return TB_ERROR_CUDA;
+  }
+  if (op.mn_major || (reinterpret_cast<uintptr_t>(op.ptr) & 15) != 0 || op.ld % 16 != 0) {
+    set_last_error("fp8 operand must be K-major, 16-byte aligned, ld a multiple of 16 (ld=%lld)", op.ld);
+    return TB_ERROR_INVALID_VALUE;
+  }
+  cuuint64_t dims[2] = {(cuuint64_t)op.cols, (cuuint64_t)op.rows};
+  cuuint64_t strides[1] = {(cuuint64_t)op.ld};
+  cuuint32_t box[2] = {128, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(op.ptr), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled (fp8) failed (%d)", (int)r);
+    return TB_ERROR_CUDA;
+  }
+  return TB_SUCCESS;
+}
+
 // Tensor map for the fp32 output C (rows x cols, column-major, ldc), box
 // {128 rows, 32 cols}, used by the TMA epilogue for loads and stores.
 bool make_c_map(CUtensorMap* map, float* C, long long rows, long long cols, long long ldc) {
@@ -94,6 +121,26 @@ bool make_half_out_map(CUtensorMap* map, __half* p, long long rows, long long co
   return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <class Cfg>
+tb_status launch_pair(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops) {
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    TB_CUDA_TRY(cudaFuncSetAttribute(gemm_pair_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     Cfg::SMEM_BYTES));
+    attr_set[dev] = true;
+  }
+  const int pairs_max = sm_count() / 2;
+  const int pairs = num_tiles < pairs_max ? num_tiles : pairs_max;
+  void* tok = prof_begin(stream);
+  gemm_pair_kernel<Cfg><<<2 * pairs, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(args);
+  TB_CUDA_TRY(cudaGetLastError());
+  prof_end(tok, stream, flops);
+  note_launch();
+  return TB_SUCCESS;
 }
 
 template <class Cfg, bool GROUPED>
@@ -124,12 +171,25 @@ int gemm_bn(Split s, int kblocks) {
 }
 
 tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
-  const bool split = c.split == Split::kHiLo;
-  const int bn = gemm_bn(c.split, c.kblocks);
+  const bool split = c.split == Split::kHiLo && !c.fp8;
+  // pair launches: each CTA loads 128 of the tile's 256 B rows
+  const int bn = c.fp8 ? kGemmBNFp8 : (c.pair ? 128 : gemm_bn(c.split, c.kblocks));
   GemmArgs& a = *out;
   memset(&a, 0, sizeof(a));
-  TB_TRY(make_map(&a.mapA[0], c.a_hi, kGemmBM));
-  TB_TRY(make_map(&a.mapB[0], c.b_hi, bn));
+  if (c.fp8) {
+    if ((c.a_off % 128) != 0 || (c.b_off % 128) != 0 || (c.k_off % 128) != 0) {
+      set_last_error("fp8 operand offsets must be multiples of the 128-wide scale blocks");
+      return TB_ERROR_INVALID_VALUE;
+    }
+    TB_TRY(make_map8(&a.mapA[0], c.a_hi, kGemmBM));
+    TB_TRY(make_map8(&a.mapB[0], c.b_hi, bn));
+    a.scale_a = c.scale_a;
+    a.scale_b = c.scale_b;
+    a.scale_ld = c.scale_ld;
+  } else {
+    TB_TRY(make_map(&a.mapA[0], c.a_hi, kGemmBM));
+    TB_TRY(make_map(&a.mapB[0], c.b_hi, bn));
+  }
   if (split) {
     TB_TRY(make_map(&a.mapA[1], c.a_lo, kGemmBM));
     TB_TRY(make_map(&a.mapB[1], c.b_lo, bn));
@@ -148,7 +208,7 @@ tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
   a.tri = c.tri;
   a.diag = c.diag;
   a.corr_scale = c.corr_scale;
-  a.kchunk = c.kchunk > 0 ? c.kchunk : 1;
+  a.kchunk = c.fp8 ? 1 : (c.kchunk > 0 ? c.kchunk : 1);
   a.tma_c = make_c_map(&a.mapC, c.C, c.M, c.N, c.ldc) ? 1 : 0;
   a.out_hi = c.out_hi;
   a.out_lo = c.out_lo;
@@ -174,6 +234,14 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   TB_TRY(gemm_build_args(c, &a));
   const bool split = c.split == Split::kHiLo;
   const bool amn = c.a_hi.mn_major, bmn = c.b_hi.mn_major;
+  if (c.fp8) return launch_variant<GemmCfg<kGemmBNFp8, 1, false, false, false, true>, false>(a, c.num_tiles, stream,
+                                                                                            c.flops);
+  if (c.pair) {
+    if (amn && bmn) return launch_pair<PairCfg<true, true>>(a, c.num_tiles, stream, c.flops);
+    if (amn && !bmn) return launch_pair<PairCfg<true, false>>(a, c.num_tiles, stream, c.flops);
+    if (!amn && !bmn) return launch_pair<PairCfg<false, false>>(a, c.num_tiles, stream, c.flops);
+    return launch_pair<PairCfg<false, true>>(a, c.num_tiles, stream, c.flops);
+  }
   if (c.kblocks > 0 && c.kblocks <= kGemmPfMaxKb) {
     if (!split) {
       if (amn && bmn) return launch_variant<GemmCfg<128, 1, true, true, true>, false>(a, c.num_tiles, stream, c.flops);
@@ -198,6 +266,50 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
     if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>, false>(a, c.num_tiles, stream, c.flops);
     return launch_variant<GemmCfg<128, 3, false, true>, false>(a, c.num_tiles, stream, c.flops);
   }
+}
+
+// TB_GEMM_PAIR=1 in the environment runs large plain launches on CTA pairs
+// (read once).
+bool pair_engine_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("TB_GEMM_PAIR");
+    on = (e && e[0] == '1') ? 1 : 0;
+  }
+  return on == 1;
+}
+
+tb_status gemm_launch_plan(GemmCall& c, const std::vector<int4>& plan, cudaStream_t stream) {
+  const bool pf = c.kblocks > 0 && c.kblocks <= kGemmPfMaxKb;
+  c.pair = !c.fp8 && c.split == Split::kPlain && !pf && c.M >= 512 && c.N >= 512 && pair_engine_enabled();
+  if (!c.pair) {
+    c.tiles = upload_tiles(plan, stream);
+    if (!c.tiles) return TB_ERROR_ALLOC;
+    c.num_tiles = (int)plan.size();
+    return gemm_launch(c, stream);
+  }
+  // merge vertically adjacent 128-row tiles into 256-row pair tiles (the K
+  // range of a pair tile spans both halves; products outside an operand's
+  // support multiply stored zeros, and masked outputs are never written)
+  std::vector<int4> merged;
+  std::map<std::pair<int, int>, size_t> where;
+  merged.reserve(plan.size());
+  for (const int4& t : plan) {
+    const std::pair<int, int> key((t.x >> 8) << 8, t.y);
+    auto it = where.find(key);
+    if (it == where.end()) {
+      where.emplace(key, merged.size());
+      merged.push_back(make_int4(key.first, key.second, t.z, t.w));
+    } else {
+      int4& m = merged[it->second];
+      m.z = t.z < m.z ? t.z : m.z;
+      m.w = t.w > m.w ? t.w : m.w;
+    }
+  }
+  c.tiles = upload_tiles(merged, stream);
+  if (!c.tiles) return TB_ERROR_ALLOC;
+  c.num_tiles = (int)merged.size();
+  return gemm_launch(c, stream);
 }
 
 // Kernel attributes of the grouped variants, set outside any stream capture.
@@ -255,6 +367,20 @@ std::vector<int4> plan_lower(int n, int bn, int kb0, int kb1) {
       for (int j = g; j < ge; ++j) {
         const int m0 = i * kGemmBM, n0 = j * bn;
         if (m0 + kGemmBM - 1 >= n0) t.push_back(make_int4(m0, n0, kb0, kb1));
+      }
+  }
+  return t;
+}
+
+std::vector<int4> plan_upper(int n, int bn, int kb0, int kb1) {
+  std::vector<int4> t;
+  const int mt = (n + kGemmBM - 1) / kGemmBM, nt = (n + bn - 1) / bn;
+  for (int g = 0; g < nt; g += kGroup) {
+    const int ge = g + kGroup < nt ? g + kGroup : nt;
+    for (int i = 0; i < mt; ++i)
+      for (int j = g; j < ge; ++j) {
+        const int m0 = i * kGemmBM, n0 = j * bn;
+        if (n0 + bn - 1 >= m0) t.push_back(make_int4(m0, n0, kb0, kb1));
       }
   }
   return t;

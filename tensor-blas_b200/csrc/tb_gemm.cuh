@@ -58,7 +58,7 @@ struct GemmArgs {
   float* C;
   long long ldc;
   float alpha, beta;
-  int tri;   // 1: write only (i - j) >= diag (lower triangle)
+  int tri;   // 1: write only (i - j) >= diag (lower triangle); 2: only (j - i) >= diag (upper)
   int diag;
   float corr_scale;  // weight of the correction accumulator
   int kchunk;        // split mode: K-blocks per round-to-nearest fold
@@ -72,6 +72,11 @@ struct GemmArgs {
   int out_m, out_n;  // side copies only for rows < out_m and columns < out_n
   int tma_out;       // 1: side copies through mapOut (requires tma_c and tri == 0)
   int* err;
+  // FP8: per-(128-row block, 128-deep K block) scales of the A and B
+  // operands, row-block-major with scale_ld K blocks per row block.
+  const float* scale_a;
+  const float* scale_b;
+  int scale_ld;
   // Grouped launches: per-tile problem index into a device array of
   // GemmArgs (64-byte aligned; their tensor maps are read from global memory).
   const struct GemmArgs* problems;
@@ -95,17 +100,24 @@ __device__ __forceinline__ const GemmArgs& tile_problem(const GemmArgs& args, in
 // tile is requested by TMA as soon as the previous tile's stores have left
 // shared memory -- while this tile's MMAs still run -- instead of one chunk
 // at a time inside the epilogue; fp16 side copies get two staging buffers.
-template <int BN_, int NSPLIT_, bool A_MN_, bool B_MN_, bool PF_ = false>
+// FP8 variant: e4m3 K-major operands scaled per 128 x 128 block; the
+// accumulator is folded into fp32 registers after every 128-deep K block
+// with the product of the two blocks' scales.
+template <int BN_, int NSPLIT_, bool A_MN_, bool B_MN_, bool PF_ = false, bool FP8_ = false>
 struct GemmCfg {
-  static constexpr int BM = 128, BN = BN_, BK = 64;
+  static constexpr bool FP8 = FP8_;
+  static constexpr int ELEM = FP8 ? 1 : 2;       // operand bytes per element
+  static constexpr int BM = 128, BN = BN_, BK = 128 / ELEM;  // one 128-byte swizzle row of K per stage
+  static constexpr int KSTEPS = 4;               // MMAs per stage (K = 16 fp16 / 32 fp8 each)
   static constexpr int NSPLIT = NSPLIT_;
   static constexpr bool A_MN = A_MN_, B_MN = B_MN_;
   static constexpr bool PF = PF_;
+  static constexpr bool FOLD = NSPLIT > 1 || FP8;  // accumulate in registers across TMEM rounds
   static constexpr int NOPS = (NSPLIT == 1) ? 1 : 2;  // copies per operand (hi[, lo])
-  static constexpr int A_BYTES = BM * BK * 2;
-  static constexpr int B_BYTES = BN * BK * 2;
+  static constexpr int A_BYTES = BM * BK * ELEM;
+  static constexpr int B_BYTES = BN * BK * ELEM;
   static constexpr int STAGE_BYTES = NOPS * (A_BYTES + B_BYTES);
-  static constexpr int STAGES = PF ? (NSPLIT == 1 ? 4 : 2) : ((STAGE_BYTES <= 48 * 1024) ? 4 : 3);
+  static constexpr int STAGES = FP8 ? 6 : PF ? (NSPLIT == 1 ? 4 : 2) : ((STAGE_BYTES <= 48 * 1024) ? 4 : 3);
   static constexpr int NACC = (NSPLIT == 1) ? 1 : 2;
   static constexpr int ACC_COLS = NACC * BN;  // TMEM columns per accumulation buffer
   static constexpr int TMEM_COLS = 2 * ACC_COLS;
@@ -140,6 +152,16 @@ __device__ __forceinline__ uint64_t operand_desc(uint32_t base, int kk) {
   }
 }
 
+// Output triangle mask: tri 1 writes only (i - j) >= diag (lower), tri 2
+// only (j - i) >= diag (upper); masked elements keep their old value.
+__device__ __forceinline__ bool out_masked(const GemmArgs& a, long long gi, long long gj) {
+  return a.tri == 1 ? (gi - gj) < a.diag : (a.tri == 2 ? (gj - gi) < a.diag : false);
+}
+// Whether a BM x BN tile at (m0, n0) reaches into the masked region.
+__device__ __forceinline__ bool tile_reaches_mask(const GemmArgs& a, long long m0, long long n0, int bm, int bn) {
+  return a.tri == 1 ? (m0 - (n0 + bn - 1)) < a.diag : (a.tri == 2 ? (n0 - (m0 + bm - 1)) < a.diag : false);
+}
+
 // Fused fp16 hi[/lo] copies of 32 result values of one row.
 __device__ __forceinline__ void store_fp16_copies(const GemmArgs& args, const float* r, long long gi, long long gj0) {
   __half* hrow = args.out_hi + gi + gj0 * args.ld_out;
@@ -147,7 +169,7 @@ __device__ __forceinline__ void store_fp16_copies(const GemmArgs& args, const fl
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    if (gj >= args.out_n || (args.tri && (gi - gj) < args.diag)) continue;
+    if (gj >= args.out_n || out_masked(args, gi, gj)) continue;
     const __half h = __float2half_rn(r[j]);
     hrow[(long long)j * args.ld_out] = h;
     if (lrow) lrow[(long long)j * args.ld_out] = __float2half_rn((r[j] - __half2float(h)) * args.out_lo_scale);
@@ -163,7 +185,7 @@ __device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const flo
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    keep[j] = gj < args.N && !(args.tri && (gi - gj) < args.diag);
+    keep[j] = gj < args.N && !out_masked(args, gi, gj);
   }
   float r[32];
   if (args.beta != 0.0f) {
@@ -219,7 +241,7 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       const float old = S[j * 128 + row];
-      const bool masked = args.tri && (gi - (long long)(gj0 + j)) < args.diag;
+      const bool masked = out_masked(args, gi, (long long)(gj0 + j));
       r[j] = masked ? old : fmaf(args.beta, old, args.alpha * v[j]);
       S[j * 128 + row] = r[j];
     }
@@ -281,7 +303,7 @@ __device__ __forceinline__ void epilogue_chunk_pf(const GemmArgs& args, float* s
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       const float old = S[j * 128 + row];
-      const bool masked = args.tri && (gi - (long long)(gj0 + j)) < args.diag;
+      const bool masked = out_masked(args, gi, (long long)(gj0 + j));
       r[j] = masked ? old : fmaf(args.beta, old, args.alpha * v[j]);
       S[j * 128 + row] = r[j];
     }
@@ -425,7 +447,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
       int it = 0;  // chunk counter (selects TMEM buffer and phase)
       bool ok = true;
       bool any = false;
-      const int kc = (Cfg::NSPLIT > 1) ? args.kchunk : (1 << 30);
+      const int kc = Cfg::FOLD ? args.kchunk : (1 << 30);
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
         const int4 tile = args.tiles[t];
         for (int c0 = tile.z; c0 < tile.w && ok; c0 += kc, ++it) {
@@ -447,11 +469,14 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
             const uint32_t st = smem_u32(smem + s * Cfg::STAGE_BYTES);
             const uint32_t a_hi = st, b_hi = st + Cfg::NOPS * Cfg::A_BYTES;
 #pragma unroll
-            for (int kk = 0; kk < BK / 16; ++kk) {
+            for (int kk = 0; kk < Cfg::KSTEPS; ++kk) {
               const uint32_t acc = (kb > c0 || kk > 0) ? 1u : 0u;
               const uint64_t da = operand_desc<Cfg::A_MN>(a_hi, kk);
               const uint64_t db = operand_desc<Cfg::B_MN>(b_hi, kk);
-              umma_f16(d0, da, db, Cfg::IDESC, acc);
+              if constexpr (Cfg::FP8)
+                umma_f8(d0, da, db, Cfg::IDESC, acc);
+              else
+                umma_f16(d0, da, db, Cfg::IDESC, acc);
               if constexpr (Cfg::NSPLIT > 1) {
                 const uint64_t da_lo = operand_desc<Cfg::A_MN>(a_hi + Cfg::A_BYTES, kk);
                 const uint64_t db_lo = operand_desc<Cfg::B_MN>(b_hi + Cfg::B_BYTES, kk);
@@ -501,7 +526,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
         const GemmArgs& P = tile_problem<GROUPED>(args, t);
         const long long gi = (long long)tile.x + row;
         const bool row_ok = gi < P.M;
-        const bool tile_masked = P.tri && ((long long)tile.x - (long long)(tile.y + BN - 1)) < P.diag;
+        const bool tile_masked = tile_reaches_mask(P, tile.x, tile.y, BM, BN);
         const bool need_load = P.tma_c && (P.beta != 0.0f || tile_masked);
         // request this tile's C while its MMAs run; slots are free once the
         // previous tile's stores have read them
@@ -516,7 +541,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
                 pending |= 1u << c;
               }
         }
-        if constexpr (Cfg::NSPLIT == 1) {
+        if constexpr (!Cfg::FOLD) {
           const int buf = it & 1;
           const uint32_t tph = (uint32_t)(it >> 1) & 1u;
           ++it;
@@ -601,8 +626,8 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
       const long long gi = (long long)tile.x + row;
       const bool row_ok = gi < P.M;
       // the tile crosses the masked (upper) region: min(i - j) < diag
-      const bool tile_masked = P.tri && ((long long)tile.x - (long long)(tile.y + BN - 1)) < P.diag;
-      if constexpr (Cfg::NSPLIT == 1) {
+      const bool tile_masked = tile_reaches_mask(P, tile.x, tile.y, BM, BN);
+      if constexpr (!Cfg::FOLD) {
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
         ++it;
@@ -640,13 +665,27 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
           }
           tc_fence_after();
           const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+          if constexpr (Cfg::FP8) {
+            // this round is K block c0k (kchunk = 1): scale by both blocks' scales
+            const int kbs = (P.k_off >> 7) + c0k;
+            const float sc = P.scale_a[(long long)((P.a_off + tile.x) >> 7) * P.scale_ld + kbs] *
+                             P.scale_b[(long long)((P.b_off + tile.y) >> 7) * P.scale_ld + kbs];
 #pragma unroll
-          for (int c0 = 0; c0 < BN; c0 += 32) {
-            float v[32], w[32];
-            tmem_ld32(tacc + c0, v);
-            tmem_ld32(tacc + BN + c0, w);
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+              float v[32];
+              tmem_ld32(tacc + c0, v);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) acc[c0 + j] += fmaf(args.corr_scale, w[j], v[j]);
+              for (int j = 0; j < 32; ++j) acc[c0 + j] = fmaf(sc, v[j], acc[c0 + j]);
+            }
+          } else {
+#pragma unroll
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+              float v[32], w[32];
+              tmem_ld32(tacc + c0, v);
+              tmem_ld32(tacc + BN + c0, w);
+#pragma unroll
+              for (int j = 0; j < 32; ++j) acc[c0 + j] += fmaf(args.corr_scale, w[j], v[j]);
+            }
           }
           tc_fence_before();
           __syncwarp();
@@ -672,6 +711,247 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
   __syncthreads();
   tc_fence_after();
   if (warp == 1) tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// Pair variant (plain FP16): a cluster of two CTAs computes 256 x 256 output
+// tiles with tcgen05.mma.cta_group::2. CTA r of the pair loads rows
+// [m0 + 128r, +128) of A and rows [n0 + 128r, +128) of B (half of the tile's
+// columns) into its own shared memory; the leader (r = 0) issues the 256-row
+// MMA, which reads both CTAs' halves, and each CTA's TMEM receives its 128
+// accumulator rows. Per SM, one 64-deep K slab moves 32 KB from L2 instead of
+// the single-CTA tile's 48 KB for the same MMA work.
+//   full[s]   leader only: both CTAs' loads complete_tx on it, the leader's
+//             producer arms it with both CTAs' bytes;
+//   empty[s]  both CTAs: the leader's commit multicasts to the pair;
+//   tfull[b]  both CTAs: the leader's commit multicasts to the pair;
+//   tempty[b] leader only: the 8 epilogue warps of the pair arrive remotely.
+// Every wait is bounded like the single-CTA kernel's; a cluster barrier
+// before TMEM is freed keeps either CTA from leaving while the pair's MMAs
+// or remote arrivals may still touch it.
+template <bool A_MN_, bool B_MN_>
+struct PairCfg {
+  static constexpr int BM = 128, BN = 256, BK = 64;  // BM: rows per CTA; BN: the pair tile's columns
+  static constexpr bool A_MN = A_MN_, B_MN = B_MN_;
+  static constexpr int A_BYTES = BM * BK * 2;
+  static constexpr int B_BYTES = (BN / 2) * BK * 2;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int STAGES = 6;
+  static constexpr int ACC_COLS = BN;
+  static constexpr int TMEM_COLS = 2 * ACC_COLS;
+  static constexpr int EPI_BYTES = 2 * 128 * 32 * 4;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + 256;
+  static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+  static constexpr uint32_t IDESC = idesc_f16(2 * BM, BN, false, A_MN, B_MN);
+  static constexpr int THREADS = 192;
+};
+
+template <bool MN, int ROWS>
+__device__ __forceinline__ void load_operand_pair(uint8_t* dst, const CUtensorMap* map, uint32_t leader_bar, int row0,
+                                                  int k) {
+  if constexpr (MN) {
+#pragma unroll
+    for (int j = 0; j < ROWS / 64; ++j) tma_load_2d_pair(dst + j * 8192, map, leader_bar, row0 + 64 * j, k);
+  } else {
+    tma_load_2d_pair(dst, map, leader_bar, k, row0);
+  }
+}
+
+template <class Cfg>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+    gemm_pair_kernel(const __grid_constant__ GemmArgs args) {
+  constexpr int BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  float* stage_c = reinterpret_cast<float*>(smem + STAGES * Cfg::STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * Cfg::STAGE_BYTES + Cfg::EPI_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* tfull = empty + STAGES;  // [2]
+  uint64_t* tempty = tfull + 2;      // [2]
+  uint64_t* drain = tempty + 2;      // [1]
+  uint64_t* cload = drain + 1;       // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 8);
+      mbar_init(&cload[b], 1);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_map(&args.mapA[0]);
+    tma_prefetch_map(&args.mapB[0]);
+    if (args.tma_c) tma_prefetch_map(&args.mapC);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(tmem_slot, Cfg::TMEM_COLS);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // the peer's barriers exist before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const uint32_t full_leader = mapa_shared(smem_u32(full), 0);
+  const uint32_t tempty_leader = mapa_shared(smem_u32(tempty), 0);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producers (both CTAs)
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      uint32_t issued_mask = 0, phase_mask = 0;
+      bool ok = true;
+      for (int t = pair; t < args.num_tiles && ok; t += npairs) {
+        const int4 tile = args.tiles[t];
+        for (int kb = tile.z; kb < tile.w; ++kb) {
+          if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
+            ok = false;
+            break;
+          }
+          if (leader) mbar_arrive_expect_tx(&full[s], 2 * Cfg::STAGE_BYTES);
+          uint8_t* st = smem + s * Cfg::STAGE_BYTES;
+          const int k = args.k_off + kb * BK;
+          const uint32_t bar = full_leader + 8u * (uint32_t)s;
+          load_operand_pair<Cfg::A_MN, 128>(st, &args.mapA[0], bar, args.a_off + tile.x + 128 * (int)rank, k);
+          load_operand_pair<Cfg::B_MN, 128>(st + Cfg::A_BYTES, &args.mapB[0], bar, args.b_off + tile.y + 128 * (int)rank,
+                                            k);
+          issued_mask |= 1u << s;
+          phase_mask = (phase_mask & ~(1u << s)) | (ph << s);
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+      if (!ok) {
+        // Abort path: the leader sees its loads land on its own barriers; the
+        // peer's loads report to the leader, so the peer waits a bounded time.
+        if (leader) {
+          for (int i = 0; i < STAGES; ++i) {
+            if (!((issued_mask >> i) & 1u)) continue;
+            const uint64_t t0 = globaltimer_ns();
+            while (!mbar_try_wait(&full[i], (phase_mask >> i) & 1u))
+              if (globaltimer_ns() - t0 > 1000000000ull) break;
+          }
+        } else {
+          const uint64_t t0 = globaltimer_ns();
+          while (globaltimer_ns() - t0 < 2000000ull) {
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer (leader)
+    if (leader && lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int it = 0;
+      bool ok = true, any = false;
+      for (int t = pair; t < args.num_tiles && ok; t += npairs, ++it) {
+        const int4 tile = args.tiles[t];
+        const int buf = it & 1;
+        const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+        if (!mbar_wait(&tempty[buf], tph ^ 1u, abort_flag, args.err, kDevErrTimeoutMma)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d0 = tmem_base + (uint32_t)(buf * Cfg::ACC_COLS);
+        for (int kb = tile.z; kb < tile.w; ++kb) {
+          if (!mbar_wait(&full[s], ph, abort_flag, args.err, kDevErrTimeoutMma)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a = smem_u32(smem + s * Cfg::STAGE_BYTES), b = a + Cfg::A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk)
+            umma_f16_pair(d0, operand_desc<Cfg::A_MN>(a, kk), operand_desc<Cfg::B_MN>(b, kk), Cfg::IDESC,
+                          (kb > tile.z || kk > 0) ? 1u : 0u);
+          any = true;
+          tc_commit_pair(&empty[s], 3);
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+        if (!ok) break;
+        tc_commit_pair(&tfull[buf], 3);
+      }
+      if (!ok && any) {
+        tc_commit_pair(drain, 1);
+        const uint64_t t0 = globaltimer_ns();
+        while (!mbar_try_wait(drain, 0)) {
+          if (globaltimer_ns() - t0 > 1000000000ull) {
+            if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
+            break;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue (both CTAs)
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    const bool issuer = (warp == 2 && lane == 0);
+    EpiState es{0, 0u};
+    int it = 0;
+    for (int t = pair; t < args.num_tiles; t += npairs, ++it) {
+      const int4 tile = args.tiles[t];
+      const int m0 = tile.x + 128 * (int)rank;
+      const long long gi = (long long)m0 + row;
+      const bool row_ok = gi < args.M;
+      const bool tile_masked = tile_reaches_mask(args, m0, tile.y, 128, BN);
+      const int buf = it & 1;
+      const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+      if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) break;
+      tc_fence_after();
+      const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        float v[32];
+        tmem_ld32(tacc + c0, v);
+        if (c0 == BN - 32) {  // this CTA's half of the accumulator is read: tell the leader
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
+        }
+        if (args.tma_c) {
+          if (tile.y + c0 < args.N && m0 < args.M)
+            epilogue_chunk_tma(args, stage_c, cload, es, v, m0, tile.y + c0, row, args.beta != 0.0f || tile_masked,
+                               issuer, abort_flag, false);
+        } else if (row_ok) {
+          epilogue_store32(args, v, gi, (long long)tile.y + c0);
+        }
+      }
+    }
+    if (issuer) bulk_wait<0>();
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // the pair's MMAs, remote arrivals and TMEM reads are over
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc_pair(tmem_base, Cfg::TMEM_COLS);
 }
 
 }  // namespace tb

@@ -48,9 +48,6 @@ tb_status gemm_impl(bool ta, bool tb_, long m, long n, long k, float alpha, cons
   c.b_lo.ptr = bl;
   c.kblocks = (int)((k + kGemmBK - 1) / kGemmBK);
   const std::vector<int4> plan = plan_rect((int)m, (int)n, gemm_bn(split, c.kblocks), 0, c.kblocks);
-  c.tiles = upload_tiles(plan, st);
-  if (!c.tiles) return TB_ERROR_ALLOC;
-  c.num_tiles = (int)plan.size();
   c.C = C;
   c.ldc = ldc;
   c.M = (int)m;
@@ -58,7 +55,7 @@ tb_status gemm_impl(bool ta, bool tb_, long m, long n, long k, float alpha, cons
   c.alpha = alpha;
   c.beta = beta;
   c.flops = 2.0 * m * n * k;
-  return gemm_launch(c, st);
+  return gemm_launch_plan(c, plan, st);
 }
 
 }  // namespace tb
@@ -79,7 +76,14 @@ extern "C" tb_status tb_sgemm(char transa, char transb, long m, long n, long k, 
                               const float* B, long ldb, float beta, float* C, long ldc, int precision) {
   bool ta, tbb;
   if (!parse_trans(transa, &ta) || !parse_trans(transb, &tbb)) return TB_ERROR_INVALID_VALUE;
-  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT) return TB_ERROR_INVALID_VALUE;
+  if (precision == TB_PREC_FP8 && m > 0 && n > 0 && k > 0 && alpha != 0.f) {
+    if (lda < ((ta ? k : m) > 1 ? (ta ? k : m) : 1) || ldb < ((tbb ? n : k) > 1 ? (tbb ? n : k) : 1) ||
+        ldc < (m > 1 ? m : 1))
+      return TB_ERROR_INVALID_VALUE;
+    return tb::gemm_fp8(ta, tbb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tb::current_stream());
+  }
+  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT && precision != TB_PREC_FP8)
+    return TB_ERROR_INVALID_VALUE;
   return tb::gemm_impl(ta, tbb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
                        precision == TB_PREC_SPLIT ? tb::Split::kHiLo : tb::Split::kPlain, tb::current_stream());
 }

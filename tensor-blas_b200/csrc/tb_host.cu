@@ -164,9 +164,6 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
     c.a_off = (int)r0;
     c.split = split;
     c.kblocks = kb;
-    c.tiles = upload_tiles(plan, cs);
-    if (!c.tiles) return TB_ERROR_ALLOC;
-    c.num_tiles = (int)plan.size();
     c.C = cb[s];
     c.ldc = P;
     c.M = (int)pr;
@@ -176,7 +173,7 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
     c.tri = 1;
     c.diag = (int)-r0;  // global row r0 + i >= column j
     c.flops = (double)pr * (double)(r0 + r1 + 1) * (double)k;
-    TB_TRY(gemm_launch(c, cs));
+    TB_TRY(gemm_launch_plan(c, plan, cs));
     TB_CUDA_TRY(cudaEventRecord(p.ev[kEvGemm + s], cs));
     // C rows [r0, r1), columns [0, r1) -> host
     TB_CUDA_TRY(cudaStreamWaitEvent(p.d2h, p.ev[kEvGemm + s], 0));

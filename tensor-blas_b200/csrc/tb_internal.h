@@ -81,6 +81,14 @@ struct GemmCall {
   float out_lo_scale = 2048.0f;
   int out_m = -1, out_n = -1;  // side-copy region (default: all of C)
   int kblocks = 0;   // most K-blocks (64) of any tile; 0 < kblocks <= kGemmPfMaxKb selects the prefetch variants
+  // FP8 (e4m3) operands: K-major byte matrices (Operand.ld in bytes), K
+  // blocks of 128, per-(128-row block, K block) scales (row-block-major,
+  // scale_ld K blocks per row block); tiles 128 x 128.
+  bool pair = false;  // set by gemm_launch_plan: 256 x 256 tiles on CTA pairs (cta_group::2)
+  bool fp8 = false;
+  const float* scale_a = nullptr;
+  const float* scale_b = nullptr;
+  int scale_ld = 0;
   double flops = 0;  // algorithmic flops of this launch (profiling only)
   int* err = nullptr;  // device error word (nullptr: the library's per-device word)
 };
@@ -91,10 +99,14 @@ struct GemmCall {
 constexpr int kGemmBM = 128;
 constexpr int kGemmBK = 64;
 constexpr int kGemmPfMaxKb = 16;
+constexpr int kGemmBNFp8 = 128;  // FP8 tiles: 128 x 128, K blocks of 128
 int gemm_bn(Split s);
 int gemm_bn(Split s, int kblocks);
 
 tb_status gemm_launch(const GemmCall& call, cudaStream_t stream);
+// Uploads `plan` (128-row tiles) and launches; plain launches that are large
+// enough run on CTA pairs, with the plan merged into 256-row tiles.
+tb_status gemm_launch_plan(GemmCall& call, const std::vector<int4>& plan, cudaStream_t stream);
 
 // Grouped launches: each problem's descriptor is built on the host by
 // gemm_build_args (tensor maps included), copied to a 64-byte aligned device
@@ -108,6 +120,7 @@ tb_status gemm_launch_grouped(Split split, const GemmArgs* d_problems, const int
 // cached on the device by `upload_tiles`.
 std::vector<int4> plan_rect(int M, int N, int bn, int kb0, int kb1);
 std::vector<int4> plan_lower(int n, int bn, int kb0, int kb1);
+std::vector<int4> plan_upper(int n, int bn, int kb0, int kb1);
 const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
 
 // ------------------------------------------------------------------ conversion
@@ -118,6 +131,8 @@ const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
 //   tri == 3: zero the strict lower triangle.
 tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
                           long long ldd, float lo_scale, int tri, cudaStream_t stream);
+// Unit diagonal in an FP16 copy (hi = 1, lo = 0) for diag = 'U' operands.
+tb_status set_unit_diag(long long n, __half* hi, __half* lo, long long ld, cudaStream_t stream);
 // ------------------------------------------------------------------ grouped TRSM pieces
 // 32x32 diagonal-block inverses of one triangular matrix: sub-blocks
 // [first, first + ceil(n/32)) of a grouped launch write D[0 ..].
@@ -144,7 +159,8 @@ tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblo
 // size <= 512) of an FP64 lower-triangular matrix of order nt; W_b at
 // W + b * wstride, leading dimension ldw. D: (nt + 31) / 32 * 1024 doubles.
 tb_status trsm_leaf_inverses_f64(long nt, const double* A, long lda, const int2* d_leaves, int nleaf, int max_size,
-                                 double* D, double* W, long long ldw, long long wstride, cudaStream_t st);
+                                 double* D, double* W, long long ldw, long long wstride, cudaStream_t st,
+                                 bool unit = false);
 // FP32 TRSM with its triangular operand prepared once (FP16 copy, leaf
 // inverses) and applied to one or more right-hand-side blocks.
 struct TrsmCtx {
@@ -167,16 +183,34 @@ struct TrsmCtx {
   long long ldr;
   cudaStream_t st;
 };
+// unit: A's diagonal is taken as 1 (diag = 'U'); the stored diagonal is never read.
 tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long nb, Split split, cudaStream_t st,
-                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start);
+                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit = false);
 size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split);
 tb_status trsm_solve(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
 // One-time kernel attribute set-up for the grouped launches (not capturable).
 tb_status gemm_prepare_grouped();
 tb_status trsm_prepare_grouped();
 
-// C(lower) *= beta (C = 0 when beta == 0).
-tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st);
+// General TRMM (side, uplo, trans, unit diagonal), tb_blas3.cu.
+// beta != 0 gives C = alpha op(A) B + beta C (the TRSM refinement residual).
+tb_status trmm_ex_impl(bool right, bool upper, bool trans, bool unit, long m, long n, float alpha, const float* A,
+                       long lda, const float* B, long ldb, float* C, long ldc, Split split, void* ws, size_t ws_bytes,
+                       cudaStream_t st, float beta = 0.f);
+// FP8-e4m3 (per-128x128-block scaled) forms, tb_fp8.cu.
+tb_status syrk_fp8(bool trans, long n, long k, float alpha, const float* A, long lda, float beta, float* C, long ldc,
+                   cudaStream_t st, bool upper = false);
+tb_status syr2k_fp8(long n, long k, float alpha, const float* A, long lda, const float* B, long ldb, float beta,
+                    float* C, long ldc, cudaStream_t st);
+tb_status trmm_fp8(bool right, bool upper, bool trans, bool unit, long m, long n, float alpha, const float* A,
+                   long lda, const float* B, long ldb, float* C, long ldc, cudaStream_t st);
+tb_status symm_fp8(bool lower, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
+                   float beta, float* C, long ldc, cudaStream_t st);
+tb_status gemm_fp8(bool ta, bool tb_, long m, long n, long k, float alpha, const float* A, long lda, const float* B,
+                   long ldb, float beta, float* C, long ldc, cudaStream_t st);
+
+// C(lower) (or C(upper)) *= beta (C = 0 when beta == 0).
+tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st, bool upper = false);
 // Full symmetric FP16 copy of an n x n matrix with one stored triangle.
 tb_status convert_sym_f32_f16(long long n, const float* A, long long lda, bool lower, __half* hi, __half* lo,
                               long long ldd, float lo_scale, cudaStream_t stream);

@@ -196,7 +196,7 @@ struct OzArgs {
   int S;
   int kb_shift, kb_mod;  // B's K-block = kb + kb_shift (mod kb_mod when kb_mod > 0)
   int M, N;
-  int tri;  // 1: only C(i, j) with j <= i is written
+  int tri;  // 1: only C(i, j) with j <= i is written; 2: only j >= i
   double* C;
   long long ldc;
   double alpha, beta;
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
         if (row_ok && beta != 1.0 && args.raw_level < 2)
           for (int j = 0; j < kOzBN; ++j) {
             const long long gj = (long long)tile.y + j;
-            if (gj < args.N && (!args.tri || gj <= gi)) {
+            if (gj < args.N && (args.tri == 0 || (args.tri == 1 ? gj <= gi : gj >= gi))) {
               double* c = args.C + gi + gj * args.ldc;
               *c = beta == 0.0 ? 0.0 : beta * *c;
             }
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
               const long long gj = (long long)tile.y + c0 + j;
-              if (gj < args.N && (!args.tri || gj <= gi)) args.raw_out[gi + gj * args.ld_raw] = v[j];
+              if (gj < args.N && (args.tri == 0 || (args.tri == 1 ? gj <= gi : gj >= gi))) args.raw_out[gi + gj * args.ld_raw] = v[j];
             }
             continue;
           }
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const long long gj = (long long)tile.y + c0 + j;
-            keep[j] = gj < args.N && (!args.tri || gj <= gi);
+            keep[j] = gj < args.N && (args.tri == 0 || (args.tri == 1 ? gj <= gi : gj >= gi));
             old[j] = 0.0;
             if (keep[j] && (L > 2 || beta != 0.0)) old[j] = args.C[gi + gj * args.ldc];
           }
@@ -545,9 +545,12 @@ enum class KRange {
   kColsLower,  // B operand lower triangular:      [0, n0 + BN)
 };
 
-std::vector<int4> oz_plan(int M, int N, bool lower_tiles, KRange kr, long long K, long long k0, long long k1,
+// tiles: 0 all tiles of M x N, 1 those meeting the lower triangle, 2 the upper.
+std::vector<int4> oz_plan(int M, int N, int tiles, KRange kr, long long K, long long k0, long long k1,
                           bool first_chunk) {
-  std::vector<int4> plan = lower_tiles ? plan_lower(M, kOzBN, 0, 0) : plan_rect(M, N, kOzBN, 0, 0);
+  std::vector<int4> plan = tiles == 1   ? plan_lower(M, kOzBN, 0, 0)
+                           : tiles == 2 ? plan_upper(M, kOzBN, 0, 0)
+                                        : plan_rect(M, N, kOzBN, 0, 0);
   std::vector<int4> out;
   out.reserve(plan.size());
   for (int4 t : plan) {
@@ -644,7 +647,7 @@ tb_status oz_gemm(const OzOperand& a, const OzOperand& b, long long K, KRange kr
     const long long kreal = std::max(0LL, std::min(kc, K - k0));
     TB_TRY(oz_prepare(a.chunk(k0, kreal), S, qa, st));
     TB_TRY(oz_prepare(b.chunk(k0, kreal), S, qb, st));
-    const std::vector<int4> plan = oz_plan(M, N, lower_tiles, kr, K1, k0, k0 + kc, k0 == 0);
+    const std::vector<int4> plan = oz_plan(M, N, lower_tiles ? 1 : 0, kr, K1, k0, k0 + kc, k0 == 0);
     TB_TRY(oz_launch(qa, qb, 0, 0, plan, M, N, lower_tiles ? 1 : 0, alpha, C, ldc, beta, S,
                      flops * (double)kc / (double)K1, 0, nullptr, 0, st));
   }
@@ -674,7 +677,8 @@ tb_status ozaki_slice(long long n, long long k, const double* A, long long lda, 
 
 // FP64 SYRK: C(lower) = alpha A A^T + beta C, A n x k ('N') or k x n ('T').
 tb_status ozaki_syrk_impl(bool trans, long n, long k, double alpha, const double* A, long lda, double beta, double* C,
-                          long ldc, int S, int raw_level, int* raw_out, long ld_raw, cudaStream_t st) {
+                          long ldc, int S, int raw_level, int* raw_out, long ld_raw, cudaStream_t st,
+                          bool upper = false) {
   const long rows_a = trans ? k : n;
   if (n < 0 || k < 0 || lda < (rows_a > 1 ? rows_a : 1) || ldc < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
   TB_TRY(check_slices(S));
@@ -698,8 +702,8 @@ tb_status ozaki_syrk_impl(bool trans, long n, long k, double alpha, const double
   for (long long k0 = 0; k0 < K1; k0 += kc_max) {
     const long long kc = std::min(kc_max, K1 - k0);
     TB_TRY(oz_prepare(a.chunk(k0, std::max(0LL, std::min(kc, (long long)k - k0))), S, q, st));
-    const std::vector<int4> plan = oz_plan((int)n, (int)n, true, KRange::kFull, K1, k0, k0 + kc, k0 == 0);
-    TB_TRY(oz_launch(q, q, 0, 0, plan, (int)n, (int)n, 1, alpha, C, ldc, beta, S,
+    const std::vector<int4> plan = oz_plan((int)n, (int)n, upper ? 2 : 1, KRange::kFull, K1, k0, k0 + kc, k0 == 0);
+    TB_TRY(oz_launch(q, q, 0, 0, plan, (int)n, (int)n, upper ? 2 : 1, alpha, C, ldc, beta, S,
                      (double)n * (double)(n + 1) * (double)kc, raw_level, raw_out, ld_raw, st));
   }
   return TB_SUCCESS;
@@ -738,7 +742,7 @@ tb_status ozaki_syr2k_impl(long n, long k, double alpha, const double* A, long l
     TB_TRY(oz_exponents(bc, q.e, st));
     TB_TRY(oz_slice(ac, q.e, S, q, 0, kh, st));
     TB_TRY(oz_slice(bc, q.e, S, q, kh, kh, st));
-    const std::vector<int4> plan = oz_plan((int)n, (int)n, true, KRange::kFull, 2 * kh, 0, 2 * kh, k0 == 0);
+    const std::vector<int4> plan = oz_plan((int)n, (int)n, 1, KRange::kFull, 2 * kh, 0, 2 * kh, k0 == 0);
     const int khb = (int)(kh / kOzBK);
     // later chunks accumulate: oz_plan marks them only when k0 > 0 via first_chunk
     TB_TRY(oz_launch(q, q, khb, 2 * khb, plan, (int)n, (int)n, 1, alpha, C, ldc, beta, S,
@@ -916,13 +920,10 @@ int slices_or_default(int s) { return s <= 0 ? 10 : s; }
 
 extern "C" tb_status tb_dsyrk_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
                                     double beta, double* C, long ldc, int slices) {
-  if (!is(uplo, 'L')) {
-    tb::set_last_error("tb_dsyrk_ozaki: only uplo='L' is supported");
-    return TB_ERROR_NOT_SUPPORTED;
-  }
+  if (!is(uplo, 'L') && !is(uplo, 'U')) return TB_ERROR_INVALID_VALUE;
   if (!is(trans, 'N') && !is(trans, 'T')) return TB_ERROR_INVALID_VALUE;
   return tb::ozaki_syrk_impl(is(trans, 'T'), n, k, alpha, A, lda, beta, C, ldc, slices_or_default(slices), 0,
-                             nullptr, 0, tb::current_stream());
+                             nullptr, 0, tb::current_stream(), is(uplo, 'U'));
 }
 
 extern "C" tb_status tb_dsyr2k_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,

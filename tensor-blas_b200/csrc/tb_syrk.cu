@@ -16,30 +16,33 @@
 namespace tb {
 
 namespace {
-__global__ void scale_lower_kernel(long long n, float beta, float* C, long long ldc) {
-  for (long long j = blockIdx.y; j < n; j += gridDim.y)
-    for (long long i = j + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+__global__ void scale_lower_kernel(long long n, float beta, float* C, long long ldc, bool upper) {
+  for (long long j = blockIdx.y; j < n; j += gridDim.y) {
+    const long long i0 = upper ? 0 : j, i1 = upper ? j + 1 : n;
+    for (long long i = i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < i1;
          i += (long long)gridDim.x * blockDim.x)
       C[i + j * ldc] = beta == 0.f ? 0.f : beta * C[i + j * ldc];
+  }
 }
 }  // namespace
 
-// C(lower) *= beta (C = 0 when beta == 0), the k == 0 / alpha == 0 case.
-tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st) {
+// C(lower) (or C(upper)) *= beta (C = 0 when beta == 0), the k == 0 /
+// alpha == 0 case.
+tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st, bool upper) {
   dim3 g((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)(n < 65535 ? n : 65535));
-  scale_lower_kernel<<<g, 256, 0, st>>>(n, beta, C, ldc);
+  scale_lower_kernel<<<g, 256, 0, st>>>(n, beta, C, ldc, upper);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   return TB_SUCCESS;
 }
 
 tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, long lda, float beta, float* C, long ldc,
-                    long nb, Split split, void* ws, size_t ws_bytes, cudaStream_t st) {
+                    long nb, Split split, void* ws, size_t ws_bytes, cudaStream_t st, bool upper = false) {
   if (n < 0 || k < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
   if (ldc < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
   if (lda < ((trans ? k : n) > 1 ? (trans ? k : n) : 1)) return TB_ERROR_INVALID_VALUE;
   if (n == 0) return TB_SUCCESS;
-  if (k == 0 || alpha == 0.f) return beta == 1.f ? TB_SUCCESS : scale_lower(n, beta, C, ldc, st);
+  if (k == 0 || alpha == 0.f) return beta == 1.f ? TB_SUCCESS : scale_lower(n, beta, C, ldc, st, upper);
   const bool hilo = split == Split::kHiLo;
   const long long rows = trans ? k : n, cols = trans ? n : k;
   const long long ldh = round_up(rows, 64);
@@ -65,14 +68,11 @@ tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, lon
 
   const int kb = (int)((k + kGemmBK - 1) / kGemmBK);
   const int bn = gemm_bn(split, kb);
-  const int4* tiles = upload_tiles(plan_lower((int)n, bn, 0, kb), st);
-  if (!tiles) return TB_ERROR_ALLOC;
+  const std::vector<int4> plan = upper ? plan_upper((int)n, bn, 0, kb) : plan_lower((int)n, bn, 0, kb);
   GemmCall c;
   c.a_hi = c.b_hi = op;
   c.a_lo = c.b_lo = opl;
   c.split = split;
-  c.tiles = tiles;
-  c.num_tiles = (int)plan_lower((int)n, bn, 0, kb).size();
   c.kblocks = kb;
   c.C = C;
   c.ldc = ldc;
@@ -80,26 +80,29 @@ tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, lon
   c.N = (int)n;
   c.alpha = alpha;
   c.beta = beta;
-  c.tri = 1;
+  c.tri = upper ? 2 : 1;
   c.diag = 0;
-  c.flops = (double)n * (double)(n + 1) * (double)k;  // lower triangle incl. diagonal, 2 flops per MAC
-  return gemm_launch(c, st);
+  c.flops = (double)n * (double)(n + 1) * (double)k;  // one triangle incl. diagonal, 2 flops per MAC
+  return gemm_launch_plan(c, plan, st);
 }
 
 }  // namespace tb
 
 extern "C" tb_status tb_ssyrk(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
                               float beta, float* C, long ldc, long nb, int precision) {
-  if (uplo != 'L' && uplo != 'l') {
-    tb::set_last_error("tb_ssyrk: only uplo='L' is supported");
-    return TB_ERROR_NOT_SUPPORTED;
-  }
+  const bool upper = (uplo == 'U' || uplo == 'u');
+  if (!upper && uplo != 'L' && uplo != 'l') return TB_ERROR_INVALID_VALUE;
   const bool t = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');
   if (!t && trans != 'N' && trans != 'n') return TB_ERROR_INVALID_VALUE;
-  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT) return TB_ERROR_INVALID_VALUE;
+  if (precision == TB_PREC_FP8 && n > 0 && k > 0 && alpha != 0.f) {
+    if (nb <= 0 || ldc < (n > 1 ? n : 1) || lda < ((t ? k : n) > 1 ? (t ? k : n) : 1)) return TB_ERROR_INVALID_VALUE;
+    return tb::syrk_fp8(t, n, k, alpha, A, lda, beta, C, ldc, tb::current_stream(), upper);
+  }
+  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT && precision != TB_PREC_FP8)
+    return TB_ERROR_INVALID_VALUE;
   return tb::syrk_impl(t, n, k, alpha, A, lda, beta, C, ldc, nb,
                        precision == TB_PREC_SPLIT ? tb::Split::kHiLo : tb::Split::kPlain, nullptr, 0,
-                       tb::current_stream());
+                       tb::current_stream(), upper);
 }
 
 // ------------------------------------------------------------------ reference C++ API

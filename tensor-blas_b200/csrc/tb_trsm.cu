@@ -38,7 +38,7 @@ constexpr int kLeafMax = 512;  // largest diagonal block inverted explicitly
 // from shared memory. Output: D[t*1024 + i + 32*c] (column-major 32x32).
 template <class T>
 __device__ __forceinline__ void diag_inv32_body(long long n, const T* __restrict__ A, long long lda,
-                                                double* __restrict__ D, long long t) {
+                                                double* __restrict__ D, long long t, bool unit = false) {
   __shared__ double L[32][33];
   const int c = threadIdx.x;
   const long long base = t * 32;
@@ -46,7 +46,7 @@ __device__ __forceinline__ void diag_inv32_body(long long n, const T* __restrict
     const long long gi = base + i, gj = base + c;
     double v;
     if (gi < n && gj < n)
-      v = (i >= c) ? (double)A[gi + gj * lda] : 0.0;
+      v = (i > c || (i == c && !unit)) ? (double)A[gi + gj * lda] : (i == c ? 1.0 : 0.0);
     else
       v = (i == c) ? 1.0 : 0.0;
     L[i][c] = v;
@@ -66,8 +66,8 @@ __device__ __forceinline__ void diag_inv32_body(long long n, const T* __restrict
 
 template <class T>
 __global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const T* __restrict__ A, long long lda,
-                                                        double* __restrict__ D) {
-  diag_inv32_body<T>(n, A, lda, D, blockIdx.x);
+                                                        double* __restrict__ D, bool unit) {
+  diag_inv32_body<T>(n, A, lda, D, blockIdx.x, unit);
 }
 
 // Grouped form: block b belongs to the job whose [first, first + count)
@@ -325,10 +325,7 @@ tb_status update(TrsmCtx& c, long s, long mid, long e) {
   g.flops = 2.0 * g.M * g.N * kk;
   g.kblocks = (int)((kk + kGemmBK - 1) / kGemmBK);
   const std::vector<int4> plan = plan_rect(g.M, g.N, gemm_bn(g.split, g.kblocks), 0, g.kblocks);
-  g.tiles = upload_tiles(plan, c.st);
-  if (!g.tiles) return TB_ERROR_ALLOC;
-  g.num_tiles = (int)plan.size();
-  return gemm_launch(g, c.st);
+  return gemm_launch_plan(g, plan, c.st);
 }
 
 tb_status recurse(TrsmCtx& c, long s, long e, const std::vector<long>& leaf_start) {
@@ -383,9 +380,9 @@ tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblo
 // the diagonal). D: (nt + 31) / 32 * 1024 doubles of scratch; d_leaves: the
 // leaves in device memory.
 tb_status trsm_leaf_inverses_f64(long nt, const double* A, long lda, const int2* d_leaves, int nleaf, int max_size,
-                                 double* D, double* W, long long ldw, long long wstride, cudaStream_t st) {
+                                 double* D, double* W, long long ldw, long long wstride, cudaStream_t st, bool unit) {
   const long nsub = (nt + 31) / 32;
-  diag_inv32_kernel<double><<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D);
+  diag_inv32_kernel<double><<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D, unit);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   const int max_chain = (max_size + 31) / 32;
@@ -453,7 +450,7 @@ TrsmLayout trsm_layout(TrsmCtx& c, long nleaf) {
 }  // namespace
 
 tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long nb, Split split, cudaStream_t st,
-                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start) {
+                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit) {
   if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
   const long nt = right ? n : m;
   if (lda < (nt > 1 ? nt : 1)) return TB_ERROR_INVALID_VALUE;
@@ -503,7 +500,7 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
   if (nleaf > 1) TB_TRY(convert_f32_f16(nt, nt, A, lda, c.ah, c.al, c.lda_h, 2048.f, 2, st));
   // 2. inverses of the diagonal leaf blocks (FP64), as FP16 hi/lo
   const long nsub = (nt + 31) / 32;
-  diag_inv32_kernel<float><<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D);
+  diag_inv32_kernel<float><<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D, unit);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   const int max_chain = (int)(leaf / 32);
@@ -561,6 +558,138 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   return trsm_solve(c, leaf_start, B, ldb, m, n);
 }
 
+
+// ------------------------------------------------------------------ all BLAS flag combinations
+// The two solved forms (left/lower/no-trans and right/lower/trans) cover the
+// other six through index maps: with J the order reversal,
+//   op(A) lower in a left solve  -> L = op(A)           (A^T copied when op(A) = U^T)
+//   op(A) upper in a left solve  -> J op(A) J is lower: J X = solve(J op(A) J, J B)
+//   op(A) upper in a right solve -> A' = op(A)^T lower  (native when op(A) = L^T)
+//   op(A) lower in a right solve -> X J (J op(A) J) = B J with J op(A) J = A'^T,
+//                                   A' = J op(A)^T J lower
+// The remapped lower triangle is copied once into scratch; B's rows (left)
+// or columns (right) are reversed in place around the solve when J appears.
+namespace {
+__global__ void tri_remap_kernel(long long n, const float* __restrict__ src, long long lds, float* __restrict__ dst,
+                                 long long ldd, int transpose, int reverse) {
+  for (long long j = blockIdx.y; j < n; j += gridDim.y)
+    for (long long i = j + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+      const long long si = reverse ? n - 1 - i : i, sj = reverse ? n - 1 - j : j;
+      dst[i + j * ldd] = transpose ? src[sj + si * lds] : src[si + sj * lds];
+    }
+}
+
+// Reverses the order of the rows (cols == 0) or the columns (cols == 1) of
+// an m x n column-major matrix in place.
+__global__ void reverse_kernel(long long m, long long n, float* __restrict__ B, long long ldb, int cols) {
+  const long long pairs = cols ? n / 2 : m / 2, other = cols ? m : n;
+  for (long long q = blockIdx.y; q < other; q += gridDim.y)
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
+         p += (long long)gridDim.x * blockDim.x) {
+      float* x = cols ? B + q + p * ldb : B + p + q * ldb;
+      float* y = cols ? B + q + (n - 1 - p) * ldb : B + (m - 1 - p) + q * ldb;
+      const float t = *x;
+      *x = *y;
+      *y = t;
+    }
+}
+
+tb_status reverse(long long m, long long n, float* B, long long ldb, bool cols, cudaStream_t st) {
+  const long long pairs = cols ? n / 2 : m / 2, other = cols ? m : n;
+  if (pairs == 0 || other == 0) return TB_SUCCESS;
+  dim3 g((unsigned)std::min<long long>((pairs + 255) / 256, 256), (unsigned)std::min<long long>(other, 65535));
+  reverse_kernel<<<g, 256, 0, st>>>(m, n, B, ldb, cols ? 1 : 0);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
+}  // namespace
+
+// Plain solve plus one refinement sweep: X0 = plain TRSM(B); R = B - op(A) X0
+// with the FP32-accurate split products (the residual is ~1e-4 of B, so its
+// own error stays ~1e-7 of B); D = plain TRSM(R); X = X0 + D. The correction
+// carries the plain solve's relative error (~1e-4) on a quantity ~1e-4 the
+// size of X, so X reaches FP32-level accuracy.
+namespace {
+__global__ void add_kernel(long long m, long long n, float* __restrict__ X, long long ldx, const float* __restrict__ D,
+                           long long ldd) {
+  for (long long j = blockIdx.y; j < n; j += gridDim.y)
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+      X[i + j * ldx] += D[i + j * ldd];
+}
+}  // namespace
+
+tb_status trsm_refine_impl(bool right, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
+                           cudaStream_t st) {
+  if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
+  const long nt = right ? n : m;
+  if (lda < (nt > 1 ? nt : 1) || ldb < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
+  if (m == 0 || n == 0) return TB_SUCCESS;
+  const size_t bytes = (size_t)m * n * sizeof(float);
+  float* R = static_cast<float*>(pool_get(bytes, 1));
+  if (!R) {
+    set_last_error("trsm refine: cannot allocate %zu bytes for the residual", bytes);
+    return TB_ERROR_ALLOC;
+  }
+  TB_CUDA_TRY(cudaMemcpy2DAsync(R, (size_t)m * 4, B, (size_t)ldb * 4, (size_t)m * 4, (size_t)n,
+                                cudaMemcpyDeviceToDevice, st));
+  TB_TRY(trsm_impl(right, m, n, A, lda, B, ldb, nb, Split::kPlain, st));
+  // R = B0 - op(A) X0 (left: A X0; right: X0 A^T)
+  TB_TRY(trmm_ex_impl(right, false, right, false, m, n, -1.f, A, lda, B, ldb, R, m, Split::kHiLo, nullptr, 0, st,
+                      1.f));
+  TB_TRY(trsm_impl(right, m, n, A, lda, R, m, nb, Split::kPlain, st));
+  dim3 g((unsigned)std::min<long long>((m + 255) / 256, 64), (unsigned)std::min<long>(n, 65535));
+  add_kernel<<<g, 256, 0, st>>>(m, n, B, ldb, R, m);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
+
+tb_status trsm_ex_impl(bool right, bool upper, bool trans, bool unit, long m, long n, const float* A, long lda,
+                       float* B, long ldb, long nb, Split split, cudaStream_t st) {
+  if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
+  const long nt = right ? n : m;
+  if (lda < (nt > 1 ? nt : 1) || ldb < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
+  if (m == 0 || n == 0) return TB_SUCCESS;
+  const bool op_lower = upper == trans;
+  bool tr = false, rev = false;  // how A' is read from A
+  if (!right) {
+    tr = trans;  // (L,N): as is; (U,T): A^T; (U,N): J A J; (L,T): J A^T J
+    rev = !op_lower;
+  } else {
+    tr = !trans;  // (L,T): as is; (U,N): A^T; (L,N): J A^T J; (U,T): J A J
+    rev = op_lower;
+  }
+  const bool copy = tr || rev;
+  const long long ldc_ = round_up(nt, 4);
+  const size_t copy_bytes = copy ? (size_t)round_up(ldc_ * nt * 4, 256) : 0;
+  const size_t need = copy_bytes + trsm_scratch_bytes(right, m, n, nb, split);
+  char* ws = static_cast<char*>(pool_get(need));
+  if (!ws) {
+    set_last_error("trsm: cannot allocate %zu bytes of scratch", need);
+    return TB_ERROR_ALLOC;
+  }
+  const float* Ause = A;
+  long ldause = lda;
+  if (copy) {
+    float* Ac = reinterpret_cast<float*>(ws);
+    dim3 g((unsigned)std::min<long long>((nt + 255) / 256, 64), (unsigned)std::min<long long>(nt, 65535));
+    tri_remap_kernel<<<g, 256, 0, st>>>(nt, A, lda, Ac, ldc_, tr ? 1 : 0, rev ? 1 : 0);
+    TB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    Ause = Ac;
+    ldause = (long)ldc_;
+  }
+  if (rev) TB_TRY(reverse(m, n, B, ldb, right, st));
+  TrsmCtx c;
+  std::vector<long> leaf_start;
+  TB_TRY(trsm_setup(right, m, n, Ause, ldause, nb, split, st, ws + copy_bytes, c, leaf_start, unit));
+  TB_TRY(trsm_solve(c, leaf_start, B, ldb, m, n));
+  if (rev) TB_TRY(reverse(m, n, B, ldb, right, st));
+  return TB_SUCCESS;
+}
+
 }  // namespace tb
 
 extern "C" tb_status tb_strsm(char side, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
@@ -572,9 +701,32 @@ extern "C" tb_status tb_strsm(char side, long m, long n, const float* A, long ld
     right = false;
   else
     return TB_ERROR_INVALID_VALUE;
+  if (precision == TB_PREC_REFINE) return tb::trsm_refine_impl(right, m, n, A, lda, B, ldb, nb, tb::current_stream());
   if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT) return TB_ERROR_INVALID_VALUE;
   return tb::trsm_impl(right, m, n, A, lda, B, ldb, nb,
                        precision == TB_PREC_SPLIT ? tb::Split::kHiLo : tb::Split::kPlain, tb::current_stream());
+}
+
+extern "C" tb_status tb_strsm_ex(char side, char uplo, char transa, char diag, long m, long n, const float* A,
+                                 long lda, float* B, long ldb, long nb, int precision) {
+  auto flag = [](char c, char a, char b, bool* v) {
+    if (c == a || c == a + ('a' - 'A')) {
+      *v = false;
+      return true;
+    }
+    if (c == b || c == b + ('a' - 'A')) {
+      *v = true;
+      return true;
+    }
+    return false;
+  };
+  bool right, upper, trans, unit;
+  if (!flag(side, 'L', 'R', &right) || !flag(uplo, 'L', 'U', &upper) || !flag(diag, 'N', 'U', &unit))
+    return TB_ERROR_INVALID_VALUE;
+  if (!flag(transa, 'N', 'T', &trans) && !flag(transa, 'N', 'C', &trans)) return TB_ERROR_INVALID_VALUE;
+  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT) return TB_ERROR_INVALID_VALUE;
+  return tb::trsm_ex_impl(right, upper, trans, unit, m, n, A, lda, B, ldb, nb,
+                          precision == TB_PREC_SPLIT ? tb::Split::kHiLo : tb::Split::kPlain, tb::current_stream());
 }
 
 // ------------------------------------------------------------------ reference C++ API

@@ -23,6 +23,8 @@ lib = ctypes.CDLL(LIB_PATH)
 
 PLAIN = 0  # FP16 operands, FP32 accumulation (reference tc_*)
 SPLIT = 1  # FP16 hi + scaled-lo, 3 products, FP32-level accuracy
+FP8 = 2    # e4m3 scaled per 128x128 block (SYRK/SYR2K/TRMM/SYMM/GEMM), ~1e-2 accuracy
+REFINE = 3  # TRSM: plain solve + one refinement sweep, FP32-level accuracy
 
 _c_long = ctypes.c_long
 _fp = ctypes.c_void_p

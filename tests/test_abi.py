@@ -70,7 +70,7 @@ def test_argument_validation_without_gpu(lib):
     assert lib.tb_ssyrk(b"L", b"N", 8, 4, 1.0, None, 4, 0.0, None, 8, 256, 0) == INVALID  # lda < n
     assert lib.tb_ssyrk(b"L", b"N", 4, 4, 1.0, None, 4, 0.0, None, 4, 0, 0) == INVALID   # nb <= 0
     assert lib.tb_ssyrk(b"L", b"N", 4, 4, 1.0, None, 4, 0.0, None, 4, 256, 7) == INVALID  # precision
-    assert lib.tb_ssyrk(b"U", b"N", 4, 4, 1.0, None, 4, 0.0, None, 4, 256, 0) == NOT_SUPPORTED
+    assert lib.tb_ssyrk(b"X", b"N", 4, 4, 1.0, None, 4, 0.0, None, 4, 256, 0) == INVALID
     assert lib.tb_ssyrk(b"L", b"N", 0, 4, 1.0, None, 1, 0.0, None, 1, 256, 0) == 0       # empty: no-op
     assert lib.tb_strsm(b"X", 4, 4, None, 4, None, 4, 64, 0) == INVALID
     assert lib.tb_strsm(b"L", 4, 4, None, 2, None, 4, 64, 0) == INVALID                # lda < m

@@ -83,3 +83,24 @@ def test_tc_trsm_python_api(tblas):
     err = (torch.linalg.norm(X.double() - ref) / torch.linalg.norm(ref)).item()
     print(f"tc_trsm python api normwise {err:.3e}")
     assert err <= 2e-3
+
+
+@pytest.mark.parametrize("side", ["R", "L"])
+@pytest.mark.parametrize("m,n,nb", [(4096, 512, 512), (512, 4096, 512), (2500, 2100, 256)])
+def test_strsm_refine(tblas, side, m, n, nb):
+    """Precision 3: plain solve plus one refinement sweep reaches FP32-level
+    accuracy where the plain solve alone does not (orders >= 2048)."""
+    rng = _rng(3 + m + 7 * n)
+    nt = n if side == "R" else m
+    A = make_tri(rng, nt)
+    B = rng.uniform(-1, 1, (m, n)).astype(np.float32)
+    A0 = np.nan_to_num(A, nan=0.0).astype(np.float64)
+    exact = np.linalg.solve(A0, B.astype(np.float64).T).T if side == "R" else np.linalg.solve(A0, B.astype(np.float64))
+    X_plain = _run(tblas, side, A, B, nb, 0)
+    X_ref = _run(tblas, side, A, B, nb, 3)
+    _, e_plain = orc.rel_errors(X_plain, exact)
+    _, e_ref = orc.rel_errors(X_ref, exact)
+    print(f"refine side={side} m={m} n={n}: plain {e_plain:.3e} -> refined {e_ref:.3e}")
+    assert e_ref <= 2e-6
+    if nt >= 2048:
+        assert e_ref < 0.1 * e_plain

@@ -259,3 +259,18 @@ def test_fp64_golden_pins():
     low = np.tril(np.ones((n, n), dtype=bool))
     d = (z["C"] - ex)[low].astype(np.float64)
     assert np.linalg.norm(d) / np.linalg.norm(ex[low].astype(np.float64)) <= 1e-15
+
+
+def test_e4m3_rounding_matches_torch():
+    """The oracle's e4m3 rounding (RNE, saturating, subnormals) agrees with
+    torch's float8_e4m3fn conversion, which follows the OCP FP8 spec."""
+    import torch
+
+    g = gi.rng(8)
+    x = np.concatenate([g.standard_normal(50000) * 30, np.ldexp(g.uniform(-1, 1, 20000), -8),
+                        np.array([448.0, -448.0, 0.0, 2.0 ** -9, 2.0 ** -10, 3 * 2.0 ** -10])]).astype(np.float32)
+    x = np.clip(x, -448, 448)
+    ref = torch.from_numpy(x).to(torch.float8_e4m3fn).to(torch.float64).numpy()
+    assert np.array_equal(orc.e4m3(x), ref)
+    Q, S = orc.fp8_quantize(g.standard_normal((200, 300)))
+    assert Q.shape == (200, 300) and S.shape == (2, 3) and np.abs(Q).max() <= 448
