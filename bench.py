@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the other configurations")
     p.add_argument("--profile-step", action="store_true",
                    help="run one untimed step (plain, then split) and exit: the command profiled with ncu")
+    p.add_argument("--profile-gemm", type=int, default=0, metavar="N",
+                   help="run three plain N x N x N SGEMMs and exit (the GEMM-engine ncu captures)")
     return p.parse_args()
 
 
@@ -648,9 +650,29 @@ def profile_step(args):
     print("profile step done", flush=True)
 
 
+def profile_gemm(args):
+    """Three untimed plain SGEMMs of order args.profile_gemm (NN), nothing
+    timed: the command the GEMM-engine ncu summaries were captured from."""
+    import TensorBLAS as TB
+
+    n = args.profile_gemm
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    X = torch.rand(n, n, device="cuda", generator=g) - 0.5
+    Y = torch.rand(n, n, device="cuda", generator=g) - 0.5
+    Z = torch.zeros(n, n, device="cuda")
+    for _ in range(3):
+        TB.sgemm("N", "N", n, n, n, 1.0, X, n, Y, n, 0.0, Z, n, TB.PLAIN)
+    TB.synchronize()
+    print("profile gemm done", flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.profile_gemm:
+        profile_gemm(args)
+        return
     if args.profile_step:
         profile_step(args)
         return

@@ -268,13 +268,13 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   }
 }
 
-// TB_GEMM_PAIR=1 in the environment runs large plain launches on CTA pairs
-// (read once).
+// Large plain launches run on CTA pairs; TB_GEMM_PAIR=0 in the environment
+// keeps them on single CTAs (read once; for comparing the two engines).
 bool pair_engine_enabled() {
   static int on = -1;
   if (on < 0) {
     const char* e = getenv("TB_GEMM_PAIR");
-    on = (e && e[0] == '1') ? 1 : 0;
+    on = (e && e[0] == '0') ? 0 : 1;
   }
   return on == 1;
 }
