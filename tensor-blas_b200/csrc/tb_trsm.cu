@@ -195,24 +195,128 @@ __device__ __forceinline__ void trtri_chain_body(const T* __restrict__ A, long l
   }
 }
 
+// Same recurrence with the growing 32-wide column panel of W kept in global
+// memory (FP64, column-major, ldg) instead of shared memory: each W block is
+// staged through a 32 x 32 shared tile when it is used, so a CTA needs ~27 KB
+// of shared memory and several CTAs share an SM (the shared-memory panel
+// allows one), letting all panels of all leaves run concurrently.
+template <class T>
+__device__ __forceinline__ void trtri_panel_body(const T* __restrict__ A, long long lda, int s, int size,
+                                                 const double* __restrict__ D, __half* __restrict__ hi,
+                                                 __half* __restrict__ lo, double* __restrict__ Wg, long long ldg,
+                                                 long long ldw, int j) {
+  __shared__ __align__(16) double LsT[32][34];  // LsT[k][r] = L(r, k) of the staged sub-block (or Dinv_i)
+  __shared__ __align__(16) double Ts[32][36];   // Ts[k][c]
+  __shared__ __align__(16) double Wb[32][36];   // Wb[k][c] = W(32p + k, 32j + c)
+  const int nsub = (size + 31) / 32;
+  if (j >= nsub) return;
+  const int tid = threadIdx.x;
+  const int r0 = 2 * (tid & 15), c0 = 4 * (tid >> 4);  // 2 x 4 output block
+  const int lr = tid & 31, lc = tid >> 5;              // load role: row lr, columns lc + 4q
+  const long long sub0 = (long long)s / 32;
+  double* Wp = Wg + (long long)(32 * j) * ldg;  // panel column 0 = leaf column 32j
+  for (int q = 0; q < 8; ++q) {
+    const int c = lc + 4 * q;
+    Wp[32 * j + lr + c * ldg] = D[(sub0 + j) * 1024 + lr + 32 * c];
+  }
+  __syncthreads();
+  for (int i = j + 1; i < nsub; ++i) {
+    double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    for (int p = j; p < i; ++p) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int cc = lc + 4 * q;
+        const int gr = 32 * i + lr, gc = 32 * p + cc;
+        LsT[cc][lr] = (gr < size && gc < size) ? (double)A[(long long)s + gr + ((long long)s + gc) * lda] : 0.0;
+        Wb[lr][cc] = __ldcg(Wp + 32 * p + lr + (long long)cc * ldg);
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int kk = 0; kk < 32; ++kk) {
+        const double2 l = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
+        const double2 w01 = *reinterpret_cast<const double2*>(&Wb[kk][c0]);
+        const double2 w23 = *reinterpret_cast<const double2*>(&Wb[kk][c0 + 2]);
+        acc[0][0] = fma(l.x, w01.x, acc[0][0]);
+        acc[0][1] = fma(l.x, w01.y, acc[0][1]);
+        acc[0][2] = fma(l.x, w23.x, acc[0][2]);
+        acc[0][3] = fma(l.x, w23.y, acc[0][3]);
+        acc[1][0] = fma(l.y, w01.x, acc[1][0]);
+        acc[1][1] = fma(l.y, w01.y, acc[1][1]);
+        acc[1][2] = fma(l.y, w23.x, acc[1][2]);
+        acc[1][3] = fma(l.y, w23.y, acc[1][3]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Ts[r0 + a][c0 + b] = acc[a][b];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int cc = lc + 4 * q;
+      LsT[cc][lr] = D[(sub0 + i) * 1024 + lr + 32 * cc];
+    }
+    __syncthreads();
+    double o[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll 4
+    for (int kk = 0; kk < 32; ++kk) {
+      const double2 d = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
+      const double2 t01 = *reinterpret_cast<const double2*>(&Ts[kk][c0]);
+      const double2 t23 = *reinterpret_cast<const double2*>(&Ts[kk][c0 + 2]);
+      o[0][0] = fma(-d.x, t01.x, o[0][0]);
+      o[0][1] = fma(-d.x, t01.y, o[0][1]);
+      o[0][2] = fma(-d.x, t23.x, o[0][2]);
+      o[0][3] = fma(-d.x, t23.y, o[0][3]);
+      o[1][0] = fma(-d.y, t01.x, o[1][0]);
+      o[1][1] = fma(-d.y, t01.y, o[1][1]);
+      o[1][2] = fma(-d.y, t23.x, o[1][2]);
+      o[1][3] = fma(-d.y, t23.y, o[1][3]);
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Wp[32 * i + r0 + a + (long long)(c0 + b) * ldg] = o[a][b];
+    __syncthreads();  // the new W block is visible to the CTA before it is staged
+  }
+  // columns [32j, 32j+32) of W for all rows of the leaf (zeros above the diagonal)
+  for (int q = 0; q < 8; ++q) {
+    const int c = lc + 4 * q;
+    const int gc = 32 * j + c;
+    if (gc >= size) continue;
+    for (int row = lr; row < size; row += 32) {
+      if (!hi) {
+        if (row < 32 * j) Wp[row + (long long)c * ldg] = 0.0;  // FP64 output: the panel is W itself
+        continue;
+      }
+      const double v = row >= 32 * j ? __ldcg(Wp + row + (long long)c * ldg) : 0.0;
+      const __half h = __float2half_rn((float)v);
+      hi[row + (long long)gc * ldw] = h;
+      lo[row + (long long)gc * ldw] = __float2half_rn((float)((v - (double)__half2float(h)) * 2048.0));
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kChainThreads) trtri_chain_kernel(const float* __restrict__ A, long long lda,
                                                                     const int2* __restrict__ leaves,
                                                                     const double* __restrict__ D,
                                                                     __half* __restrict__ Whi, __half* __restrict__ Wlo,
-                                                                    long long ldw, long long wstride) {
+                                                                    long long ldw, long long wstride,
+                                                                    double* __restrict__ Wg) {
   const int2 leaf = leaves[blockIdx.y];  // {s, size}
-  trtri_chain_body<float>(A, lda, leaf.x, leaf.y, D, Whi + (long long)blockIdx.y * wstride,
-                          Wlo + (long long)blockIdx.y * wstride, nullptr, ldw, blockIdx.x);
+  trtri_panel_body<float>(A, lda, leaf.x, leaf.y, D, Whi + (long long)blockIdx.y * wstride,
+                          Wlo + (long long)blockIdx.y * wstride, Wg + (long long)blockIdx.y * wstride, ldw, ldw,
+                          blockIdx.x);
 }
 
-// FP64 operand, FP64 inverse (the Ozaki-scheme FP64 TRSM's leaves).
+// FP64 operand, FP64 inverse (the Ozaki-scheme FP64 TRSM's leaves); the
+// output W itself holds the panels.
 __global__ void __launch_bounds__(kChainThreads) trtri_chain_f64_kernel(const double* __restrict__ A, long long lda,
                                                                         const int2* __restrict__ leaves,
                                                                         const double* __restrict__ D,
                                                                         double* __restrict__ W, long long ldw,
                                                                         long long wstride) {
   const int2 leaf = leaves[blockIdx.y];
-  trtri_chain_body<double>(A, lda, leaf.x, leaf.y, D, nullptr, nullptr, W + (long long)blockIdx.y * wstride, ldw,
+  trtri_panel_body<double>(A, lda, leaf.x, leaf.y, D, nullptr, nullptr, W + (long long)blockIdx.y * wstride, ldw, ldw,
                            blockIdx.x);
 }
 
@@ -386,17 +490,8 @@ tb_status trsm_leaf_inverses_f64(long nt, const double* A, long lda, const int2*
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   const int max_chain = (max_size + 31) / 32;
-  const size_t smem = (size_t)max_chain * 1024 * sizeof(double);
-  static bool attr_done[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !attr_done[dev]) {
-    TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kLeafMax / 32 * 1024 * sizeof(double))));
-    attr_done[dev] = true;
-  }
-  trtri_chain_f64_kernel<<<dim3((unsigned)max_chain, (unsigned)nleaf), kChainThreads, smem, st>>>(A, lda, d_leaves, D,
-                                                                                                 W, ldw, wstride);
+  trtri_chain_f64_kernel<<<dim3((unsigned)max_chain, (unsigned)nleaf), kChainThreads, 0, st>>>(A, lda, d_leaves, D, W,
+                                                                                              ldw, wstride);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   return TB_SUCCESS;
@@ -409,7 +504,7 @@ tb_status trsm_leaf_inverses_f64(long nt, const double* A, long lda, const int2*
 // take it from the pool.
 namespace {
 struct TrsmLayout {
-  size_t o_ah, o_al, o_xh, o_xl, o_wh, o_wl, o_rh, o_rl, o_d, o_lv, total;
+  size_t o_ah, o_al, o_xh, o_xl, o_wh, o_wl, o_rh, o_rl, o_d, o_lv, o_wg, total;
 };
 
 TrsmLayout trsm_layout(TrsmCtx& c, long nleaf) {
@@ -444,6 +539,7 @@ TrsmLayout trsm_layout(TrsmCtx& c, long nleaf) {
   L.o_rl = take(r_bytes);
   L.o_d = take(d_bytes);
   L.o_lv = take(l_bytes);
+  L.o_wg = take((size_t)c.wstride * nleaf * sizeof(double));  // FP64 panels of the leaf inverses
   L.total = off;
   return L;
 }
@@ -494,6 +590,7 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
   c.rl = reinterpret_cast<__half*>(ws + L.o_rl);
   double* D = reinterpret_cast<double*>(ws + L.o_d);
   int2* dleaves = reinterpret_cast<int2*>(ws + L.o_lv);
+  double* W64 = reinterpret_cast<double*>(ws + L.o_wg);
   TB_CUDA_TRY(cudaMemcpyAsync(dleaves, leaves.data(), nleaf * sizeof(int2), cudaMemcpyHostToDevice, st));
 
   // 1. FP16 copy of A's lower part (only off-diagonal leaf blocks are read)
@@ -504,17 +601,8 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   const int max_chain = (int)(leaf / 32);
-  const size_t smem = (size_t)max_chain * 1024 * sizeof(double);
-  static bool attr_done[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !attr_done[dev]) {
-    TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kLeafMax / 32 * 1024 * sizeof(double))));
-    attr_done[dev] = true;
-  }
   dim3 grid((unsigned)max_chain, (unsigned)nleaf);
-  trtri_chain_kernel<<<grid, kChainThreads, smem, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride);
+  trtri_chain_kernel<<<grid, kChainThreads, 0, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride, W64);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   return TB_SUCCESS;
