@@ -44,6 +44,9 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the other configurations")
     p.add_argument("--profile-step", action="store_true",
                    help="run one untimed step (plain, then split) and exit: the command profiled with ncu")
+    p.add_argument("--profile-aux", action="store_true",
+                   help="run the non-GEMM kernels once each (conversions, TRSM leaf inverses, Ozaki slicing, FP8 "
+                        "quantisation) at bench sizes and exit: the command their ncu summaries come from")
     p.add_argument("--profile-gemm", type=int, default=0, metavar="N",
                    help="run three plain N x N x N SGEMMs and exit (the GEMM-engine ncu captures)")
     return p.parse_args()
@@ -280,22 +283,24 @@ def run_mine(args, world, rank, local):
     hB = torch.empty_like(hB0).pin_memory()
     hC = torch.zeros(n, n, dtype=torch.float32).pin_memory()
 
-    def e2e_step():
+    def e2e_step(em):
         TB.ssyrk_host(hA, hC, n, n, n, n, 1.0, 0.0, args.nb_syrk, TB.PLAIN)
+        em.record(stream)
         TB.strsm_host("L", hT, hB, n, n, n, n, args.nb_trsm, TB.PLAIN)
 
-    ms_e2e = 0.0
+    ms_e2e, ms_e2e_syrk = 0.0, 0.0
     for i in range(max(1, args.warmup) + args.e2e_steps):
         hB.copy_(hB0)                        # TRSM overwrites B in host memory; restored outside the timing
         torch.cuda.synchronize()
         barrier(world)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         e0.record(stream)
-        e2e_step()
+        e2e_step(em)
         e1.record(stream)
         torch.cuda.synchronize()
         if i >= max(1, args.warmup):
             ms_e2e += e0.elapsed_time(e1)
+            ms_e2e_syrk += e0.elapsed_time(em)
     ms_e2e = max_over_ranks(ms_e2e, world)
     barrier(world)
     e2e_value = world * args.e2e_steps * flops_step / (ms_e2e * 1e-3) / 1e12
@@ -337,6 +342,7 @@ def run_mine(args, world, rank, local):
                    "errors_vs_fp64": err_split},
         "trsm_16384_by_precision": trsm_only,
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "steps": args.e2e_steps, "ms_per_step": ms_e2e / args.e2e_steps,
+                "ms_syrk_host": ms_e2e_syrk / args.e2e_steps,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "api": "TensorBLAS.ssyrk_host / TensorBLAS.strsm_host (tb_ssyrk_host / tb_strsm_host) on page-locked "
                        "host buffers", "matches_device_results": bool(ok)},
@@ -353,6 +359,9 @@ def run_mine(args, world, rank, local):
         line["cpu_baseline"] = {"value": fl / 1e12, "unit": "TFLOP/s", "cores": tb_cpu.threads(), "kind": "port",
                                 "sample": f"{reps} x (SYRK n=k={nc} + TRSM m=n={nc}, FP16-rounded operands, "
                                           f"FP32 OpenBLAS) in {el:.1f} s"}
+        line["host_blas"] = {"unit": "TFLOP/s", "n": 4096, "cores": tb_cpu.threads(),
+                             "library": "OpenBLAS (SciPy BLAS wrappers)",
+                             "rates": tb_cpu.host_blas_rates(4096, 2.0)}
     if world == 1 and not args.no_extra:
         line["other_configs"] = other_configs(TB)
     return line
@@ -667,9 +676,46 @@ def profile_gemm(args):
     print("profile gemm done", flush=True)
 
 
+def profile_aux(args):
+    """One plain SYRK and TRSM at n (FP32->FP16 conversions, 32x32 and leaf
+    inverses), one Ozaki DSYRK n=k=8192 with 10 slices (exponent and slicing
+    passes) and one FP8 SYR2K n=8192, k=4096 (block quantisation); nothing
+    timed."""
+    import ctypes
+
+    import TensorBLAS as TB
+
+    n = args.n
+    A, T, B0 = make_inputs(n)
+    C = torch.zeros(n, n, device="cuda")
+    TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN)
+    TB.strsm("L", T, B0, n, n, n, n, args.nb_trsm, TB.PLAIN)
+    TB.synchronize()
+    del A, T, B0, C
+    torch.cuda.empty_cache()
+    m = 8192
+    D = torch.randn(m, m, dtype=torch.float64, device="cuda")
+    E = torch.zeros(m, m, dtype=torch.float64, device="cuda")
+    L, P = ctypes.c_long, ctypes.c_void_p
+    TB.lib.tb_dsyrk_ozaki.argtypes = [ctypes.c_char, ctypes.c_char, L, L, ctypes.c_double, P, L, ctypes.c_double, P, L,
+                                      ctypes.c_int]
+    TB._check(TB.lib.tb_dsyrk_ozaki(b"L", b"N", m, m, 1.0, D.data_ptr(), m, 0.0, E.data_ptr(), m, 10))
+    del D, E
+    X = torch.randn(4096, m, device="cuda")
+    Y = torch.randn(4096, m, device="cuda")
+    Z = torch.zeros(m, m, device="cuda")
+    TB._check(TB.lib.tb_ssyr2k(b"L", b"N", m, 4096, 1.0, X.data_ptr(), m, Y.data_ptr(), m, 0.0, Z.data_ptr(), m, 256,
+                               TB.FP8))
+    TB.synchronize()
+    print("profile aux done", flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.profile_aux:
+        profile_aux(args)
+        return
     if args.profile_gemm:
         profile_gemm(args)
         return

@@ -71,3 +71,40 @@ def time_step(n: int, min_seconds: float = 10.0, seed: int = 0):
             if el >= min_seconds:
                 break
     return reps * 2.0 * float(n) ** 3 / el, reps, el
+
+
+def host_blas_rates(n: int = 4096, min_seconds: float = 2.0, seed: int = 1) -> dict:
+    """Host BLAS (OpenBLAS via SciPy, all cores) on the level-3 routines this
+    library replaces: SSYRK/DSYRK (lower, n = k), STRSM (left, lower,
+    non-unit), STRMM (left, upper) and SSYMM (left, lower), all n x n.
+    Returns {routine: TFLOP/s} at the nominal BLAS3 flop counts (SYRK, TRSM
+    and TRMM n^3, SYMM 2 n^3), each repeated for min_seconds."""
+    from threadpoolctl import threadpool_limits
+
+    g = np.random.Generator(np.random.PCG64(seed))
+    A = np.asfortranarray(g.uniform(-1, 1, (n, n)).astype(np.float32))
+    B = np.asfortranarray(g.uniform(-1, 1, (n, n)).astype(np.float32))
+    T = np.asfortranarray((np.tril(g.uniform(-1, 1, (n, n)) / np.sqrt(n), -1)
+                           + np.diag(g.uniform(1, 2, n))).astype(np.float32))
+    A64 = np.asfortranarray(A.astype(np.float64))
+    nf = float(n) ** 3
+    cases = {
+        "ssyrk": (lambda: blas.ssyrk(1.0, A, lower=1), nf),
+        "dsyrk": (lambda: blas.dsyrk(1.0, A64, lower=1), nf),
+        "strsm": (lambda: blas.strsm(1.0, T, B, lower=1), nf),
+        "strmm": (lambda: blas.strmm(1.0, T.T, B, lower=0), nf),
+        "ssymm": (lambda: blas.ssymm(1.0, A, B, lower=1), 2.0 * nf),
+    }
+    out = {}
+    with threadpool_limits(threads()):
+        for name, (fn, fl) in cases.items():
+            fn()  # warm-up
+            reps, t0 = 0, time.perf_counter()
+            while True:
+                fn()
+                reps += 1
+                el = time.perf_counter() - t0
+                if el >= min_seconds:
+                    break
+            out[name] = reps * fl / el / 1e12
+    return out

@@ -11,6 +11,8 @@
 //   warp 0      TMA producer: 64-wide K slabs of A and B into a smem ring.
 //   warp 1      TMEM allocator + single-thread UMMA issuer.
 //   warps 2..5  epilogue: TMEM -> registers -> alpha/beta -> C.
+//   warp 6      (prefetch variants only, 224 threads) C loader: streams
+//               128 x 32 chunks of C into a ring of shared-memory slots.
 // The fp32 accumulator is double-buffered in TMEM (2 x 256 columns) so the
 // epilogue of tile t overlaps the MMAs of tile t+1.
 //
@@ -96,10 +98,12 @@ __device__ __forceinline__ const GemmArgs& tile_problem(const GemmArgs& args, in
 
 // PF (prefetch) variants serve launches whose tiles have few K-blocks: there
 // the epilogue, not the MMA, bounds the tile, so they trade pipeline stages
-// for one shared-memory slot per 32-column chunk of the tile. The whole C
-// tile is requested by TMA as soon as the previous tile's stores have left
-// shared memory -- while this tile's MMAs still run -- instead of one chunk
-// at a time inside the epilogue; fp16 side copies get two staging buffers.
+// for a ring of shared-memory slots of 128 x 32 fp32 C chunks. A dedicated
+// loader warp fills the ring in the epilogue's chunk order, each slot as
+// soon as the stores of the chunk that used it last have read it, so the
+// next tile's C is in flight while this tile's epilogue runs (for chunks the
+// epilogue does not read, the loader only arrives on the slot's barrier).
+// fp16 side copies get two staging buffers.
 // FP8 variant: e4m3 K-major operands scaled per 128 x 128 block; the
 // accumulator is folded into fp32 registers after every 128-deep K block
 // with the product of the two blocks' scales.
@@ -117,20 +121,21 @@ struct GemmCfg {
   static constexpr int A_BYTES = BM * BK * ELEM;
   static constexpr int B_BYTES = BN * BK * ELEM;
   static constexpr int STAGE_BYTES = NOPS * (A_BYTES + B_BYTES);
-  static constexpr int STAGES = FP8 ? 6 : PF ? (NSPLIT == 1 ? 4 : 2) : ((STAGE_BYTES <= 48 * 1024) ? 4 : 3);
+  static constexpr int STAGES = FP8 ? 6 : PF ? (NSPLIT == 1 ? 3 : 2) : ((STAGE_BYTES <= 48 * 1024) ? 4 : 3);
   static constexpr int NACC = (NSPLIT == 1) ? 1 : 2;
   static constexpr int ACC_COLS = NACC * BN;  // TMEM columns per accumulation buffer
   static constexpr int TMEM_COLS = 2 * ACC_COLS;
   static_assert(TMEM_COLS <= 512, "TMEM budget");
   static constexpr int EPI_CHUNK_BYTES = 128 * 32 * 4;  // one staged 128 x 32 fp32 chunk
-  static constexpr int C_SLOTS = PF ? BN / 32 : 2;      // C-chunk staging slots (and their load barriers)
+  // C-chunk staging slots (and their load barriers); PF: the loader's ring
+  static constexpr int C_SLOTS = PF ? (NSPLIT == 1 ? 6 : 4) : 2;
   static constexpr int SIDE_BYTES = PF ? 2 * EPI_CHUNK_BYTES : 0;  // PF: two fp16 hi/lo side buffers
   static constexpr int EPI_BYTES = C_SLOTS * EPI_CHUNK_BYTES + SIDE_BYTES;
   static constexpr int BAR_BYTES = 256;
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + BAR_BYTES;
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
   static constexpr uint32_t IDESC = idesc_f16(BM, BN, false, A_MN, B_MN);
-  static constexpr int THREADS = 192;
+  static constexpr int THREADS = PF ? 224 : 192;
 };
 
 template <bool MN, int ROWS>
@@ -154,25 +159,62 @@ __device__ __forceinline__ uint64_t operand_desc(uint32_t base, int kk) {
 
 // Output triangle mask: tri 1 writes only (i - j) >= diag (lower), tri 2
 // only (j - i) >= diag (upper); masked elements keep their old value.
-__device__ __forceinline__ bool out_masked(const GemmArgs& a, long long gi, long long gj) {
-  return a.tri == 1 ? (gi - gj) < a.diag : (a.tri == 2 ? (gj - gi) < a.diag : false);
-}
 // Whether a BM x BN tile at (m0, n0) reaches into the masked region.
 __device__ __forceinline__ bool tile_reaches_mask(const GemmArgs& a, long long m0, long long n0, int bm, int bn) {
   return a.tri == 1 ? (m0 - (n0 + bn - 1)) < a.diag : (a.tri == 2 ? (n0 - (m0 + bm - 1)) < a.diag : false);
 }
 
+// Epilogue scalars, read into registers once per chunk. The epilogue's
+// stores go through generic pointers (shared-memory slots, C, side copies),
+// which the compiler cannot tell apart from the kernel's parameter memory:
+// GemmArgs fields read inside a store loop are re-read from parameter space
+// after every store, which made the masked/beta chunks several times slower
+// than their arithmetic.
+struct EpiK {
+  float alpha, beta, lo_scale;
+  int tri, diag;
+  __device__ __forceinline__ explicit EpiK(const GemmArgs& a)
+      : alpha(a.alpha), beta(a.beta), lo_scale(a.out_lo_scale), tri(a.tri), diag(a.diag) {}
+  __device__ __forceinline__ bool masked(long long gi, long long gj) const {
+    return tri == 1 ? (gi - gj) < diag : (tri == 2 ? (gj - gi) < diag : false);
+  }
+  // some element of the 128 x 32 chunk at (m0, n0) is masked
+  __device__ __forceinline__ bool chunk_masked(long long m0, long long n0) const {
+    return tri == 1 ? (m0 - (n0 + 31)) < diag : (tri == 2 ? (n0 - (m0 + 127)) < diag : false);
+  }
+};
+
+// New values of one row's 32 staged C elements: alpha v + beta old where
+// unmasked (old kept where masked), written back in place.
+__device__ __forceinline__ void combine32(const EpiK& k, float* S, int row, const float* v, long long gi,
+                                          long long gj0, bool any_masked, float* r) {
+  if (any_masked) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float old = S[j * 128 + row];
+      r[j] = k.masked(gi, gj0 + j) ? old : fmaf(k.beta, old, k.alpha * v[j]);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) r[j] = fmaf(k.beta, S[j * 128 + row], k.alpha * v[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < 32; ++j) S[j * 128 + row] = r[j];
+}
+
 // Fused fp16 hi[/lo] copies of 32 result values of one row.
 __device__ __forceinline__ void store_fp16_copies(const GemmArgs& args, const float* r, long long gi, long long gj0) {
-  __half* hrow = args.out_hi + gi + gj0 * args.ld_out;
-  __half* lrow = args.out_lo ? args.out_lo + gi + gj0 * args.ld_out : nullptr;
+  const EpiK k(args);
+  const long long ld = args.ld_out, out_n = args.out_n;
+  __half* hrow = args.out_hi + gi + gj0 * ld;
+  __half* lrow = args.out_lo ? args.out_lo + gi + gj0 * ld : nullptr;
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    if (gj >= args.out_n || out_masked(args, gi, gj)) continue;
+    if (gj >= out_n || k.masked(gi, gj)) continue;
     const __half h = __float2half_rn(r[j]);
-    hrow[(long long)j * args.ld_out] = h;
-    if (lrow) lrow[(long long)j * args.ld_out] = __float2half_rn((r[j] - __half2float(h)) * args.out_lo_scale);
+    hrow[(long long)j * ld] = h;
+    if (lrow) lrow[(long long)j * ld] = __float2half_rn((r[j] - __half2float(h)) * k.lo_scale);
   }
 }
 
@@ -180,27 +222,30 @@ __device__ __forceinline__ void store_fp16_copies(const GemmArgs& args, const fl
 // with the lower-triangle mask and bounds. With beta != 0 the 32 old values
 // are loaded before any store so the loads are in flight together.
 __device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const float* v, long long gi, long long gj0) {
-  float* crow = args.C + gi + gj0 * args.ldc;
+  const EpiK k(args);
+  const long long ldc = args.ldc, N = args.N;
+  const bool copies = args.out_hi && gi < args.out_m;
+  float* crow = args.C + gi + gj0 * ldc;
   bool keep[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    keep[j] = gj < args.N && !out_masked(args, gi, gj);
+    keep[j] = gj < N && !k.masked(gi, gj);
   }
   float r[32];
-  if (args.beta != 0.0f) {
+  if (k.beta != 0.0f) {
 #pragma unroll
-    for (int j = 0; j < 32; ++j) r[j] = keep[j] ? __ldg(crow + (long long)j * args.ldc) : 0.f;
+    for (int j = 0; j < 32; ++j) r[j] = keep[j] ? __ldg(crow + (long long)j * ldc) : 0.f;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) r[j] = fmaf(args.beta, r[j], args.alpha * v[j]);
+    for (int j = 0; j < 32; ++j) r[j] = fmaf(k.beta, r[j], k.alpha * v[j]);
   } else {
 #pragma unroll
-    for (int j = 0; j < 32; ++j) r[j] = args.alpha * v[j];
+    for (int j = 0; j < 32; ++j) r[j] = k.alpha * v[j];
   }
 #pragma unroll
   for (int j = 0; j < 32; ++j)
-    if (keep[j]) crow[(long long)j * args.ldc] = r[j];
-  if (args.out_hi && gi < args.out_m) store_fp16_copies(args, r, gi, gj0);
+    if (keep[j]) crow[(long long)j * ldc] = r[j];
+  if (copies) store_fp16_copies(args, r, gi, gj0);
 }
 
 // Epilogue state shared by the 4 epilogue warps (identical in all of them).
@@ -216,8 +261,10 @@ struct EpiState {
 __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* stage, uint64_t* cload, EpiState& es,
                                                    const float* v, int m0, int gj0, int row, bool need_load,
                                                    bool issuer, volatile int* abort_flag, bool single_buffer) {
+  const EpiK k(args);
   const bool side_mode = single_buffer || args.tma_out != 0;
   const bool side = args.tma_out != 0 && gj0 < args.out_n && m0 < args.out_m;
+  const bool copies = !side_mode && args.out_hi && (long long)m0 + row < args.out_m;
   const int b = side_mode ? 0 : (es.chunk & 1);
   float* S = stage + b * (128 * 32);
   __half* Hs = reinterpret_cast<__half*>(stage + 128 * 32);
@@ -238,17 +285,11 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
   if (need_load) {
     mbar_wait(&cload[b], (es.lphase >> b) & 1u, abort_flag, args.err, kDevErrTimeoutEpilogue);
     es.lphase ^= 1u << b;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const float old = S[j * 128 + row];
-      const bool masked = out_masked(args, gi, (long long)(gj0 + j));
-      r[j] = masked ? old : fmaf(args.beta, old, args.alpha * v[j]);
-      S[j * 128 + row] = r[j];
-    }
+    combine32(k, S, row, v, gi, gj0, k.chunk_masked(m0, gj0), r);
   } else {
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
-      r[j] = args.alpha * v[j];
+      r[j] = k.alpha * v[j];
       S[j * 128 + row] = r[j];
     }
   }
@@ -257,7 +298,7 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
     for (int j = 0; j < 32; ++j) {
       const __half hv = __float2half_rn(r[j]);
       Hs[j * 128 + row] = hv;
-      Ls[j * 128 + row] = __float2half_rn((r[j] - __half2float(hv)) * args.out_lo_scale);
+      Ls[j * 128 + row] = __float2half_rn((r[j] - __half2float(hv)) * k.lo_scale);
     }
   }
   fence_proxy_async_smem();
@@ -270,47 +311,53 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
     }
     bulk_commit();
   }
-  if (!side_mode && args.out_hi && gi < args.out_m) store_fp16_copies(args, r, gi, gj0);
+  if (copies) store_fp16_copies(args, r, gi, gj0);
   ++es.chunk;
 }
 
-// PF epilogue, one 128 x 32 chunk (index c of the tile, columns gj0..gj0+31).
-// Its C values (when needed) were requested into slot c at the start of the
-// tile; the result is combined in place and stored from the same slot. Side
-// copies alternate between two fp16 buffers. All 128 epilogue threads call
-// it together; pf.lphase / pf.side stay identical across them.
+// PF epilogue, one 128 x 32 chunk (columns gj0..gj0+31) staged in the next
+// slot of the loader's ring. The slot holds this chunk of C when need_load
+// (the loader's TMA load completes its barrier) and is only handed over
+// otherwise; the result is combined in place and stored from the slot. Before
+// the issuer stores a chunk it waits until the previous chunk's stores have
+// read their slot and gives that slot back to the loader. Side copies
+// alternate between two fp16 buffers. All 128 epilogue threads call it
+// together and keep identical state. Returns false, in every thread alike,
+// when the slot's wait gave up.
 struct PfState {
-  uint32_t lphase;  // per-slot phase bits of the C-load barriers
-  int side;         // side-copy chunks written so far (selects the buffer)
+  int slot;        // next ring slot
+  uint32_t phase;  // its barrier's phase (flips when the ring wraps)
+  int prev;        // slot of the previous chunk, still to be released (-1: none)
+  int side;        // side-copy chunks written so far (selects the buffer)
 };
 
-__device__ __forceinline__ void epilogue_chunk_pf(const GemmArgs& args, float* slots, __half* side_base,
-                                                  uint64_t* cload, PfState& pf, const float* v, int m0, int gj0,
-                                                  int c, int row, bool need_load, bool issuer,
+template <int RING>
+__device__ __forceinline__ bool epilogue_chunk_pf(const GemmArgs& args, float* slots, __half* side_base,
+                                                  uint64_t* cfull, uint64_t* cfree, PfState& pf, const float* v,
+                                                  int m0, int gj0, int row, bool need_load, bool issuer,
                                                   volatile int* abort_flag) {
+  const EpiK k(args);
   const bool side = args.tma_out != 0 && gj0 < args.out_n && m0 < args.out_m;
-  float* S = slots + c * (128 * 32);
+  const bool copies = !args.tma_out && args.out_hi && (long long)m0 + row < args.out_m;
+  const int slot = pf.slot;
+  float* S = slots + slot * (128 * 32);
   __half* Hs = side_base + (pf.side & 1) * (2 * 128 * 32);
   __half* Ls = Hs + 128 * 32;
-  // the side buffer's previous store (two side chunks ago) has read it
-  if (side && issuer) bulk_wait_read<1>();
-  named_bar_sync(1, 128);
+  const bool got = mbar_wait(&cfull[slot], pf.phase, abort_flag, args.err, kDevErrTimeoutEpilogue);
+  // also orders this chunk's smem writes after the issuer's previous stores
+  if (named_bar_any(1, 128, !got)) return false;
+  if (++pf.slot == RING) {
+    pf.slot = 0;
+    pf.phase ^= 1u;
+  }
   const long long gi = (long long)m0 + row;
   float r[32];
   if (need_load) {
-    mbar_wait(&cload[c], (pf.lphase >> c) & 1u, abort_flag, args.err, kDevErrTimeoutEpilogue);
-    pf.lphase ^= 1u << c;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const float old = S[j * 128 + row];
-      const bool masked = out_masked(args, gi, (long long)(gj0 + j));
-      r[j] = masked ? old : fmaf(args.beta, old, args.alpha * v[j]);
-      S[j * 128 + row] = r[j];
-    }
+    combine32(k, S, row, v, gi, gj0, k.chunk_masked(m0, gj0), r);
   } else {
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
-      r[j] = args.alpha * v[j];
+      r[j] = k.alpha * v[j];
       S[j * 128 + row] = r[j];
     }
   }
@@ -319,12 +366,15 @@ __device__ __forceinline__ void epilogue_chunk_pf(const GemmArgs& args, float* s
     for (int j = 0; j < 32; ++j) {
       const __half hv = __float2half_rn(r[j]);
       Hs[j * 128 + row] = hv;
-      Ls[j * 128 + row] = __float2half_rn((r[j] - __half2float(hv)) * args.out_lo_scale);
+      Ls[j * 128 + row] = __float2half_rn((r[j] - __half2float(hv)) * k.lo_scale);
     }
   }
   fence_proxy_async_smem();
   named_bar_sync(1, 128);
   if (issuer) {
+    // the previous chunk's stores have read their slot (and side buffer)
+    bulk_wait_read<0>();
+    if (pf.prev >= 0) mbar_arrive(&cfree[pf.prev]);
     tma_store_2d(&args.mapC, S, m0, gj0);
     if (side) {
       tma_store_2d(&args.mapOut[0], Hs, m0, gj0);
@@ -332,12 +382,14 @@ __device__ __forceinline__ void epilogue_chunk_pf(const GemmArgs& args, float* s
     }
     bulk_commit();
   }
-  if (!args.tma_out && args.out_hi && gi < args.out_m) store_fp16_copies(args, r, gi, gj0);
+  pf.prev = slot;
+  if (copies) store_fp16_copies(args, r, gi, gj0);
   if (side) ++pf.side;
+  return true;
 }
 
 template <class Cfg, bool GROUPED>
-__global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ GemmArgs args) {
+__global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_constant__ GemmArgs args) {
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -348,7 +400,8 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
   uint64_t* tempty = tfull + 2;      // [2]
   uint64_t* drain = tempty + 2;      // [1] teardown barrier for the MMA issuer
   uint64_t* cload = drain + 1;       // [C_SLOTS] C-chunk loads of the TMA epilogue
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + Cfg::C_SLOTS);
+  uint64_t* cfree = cload + Cfg::C_SLOTS;  // [C_SLOTS] PF: ring slots the epilogue gave back
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cfree + Cfg::C_SLOTS);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5;
@@ -363,7 +416,10 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4);
     }
-    for (int b = 0; b < Cfg::C_SLOTS; ++b) mbar_init(&cload[b], 1);
+    for (int b = 0; b < Cfg::C_SLOTS; ++b) {
+      mbar_init(&cload[b], 1);
+      mbar_init(&cfree[b], 1);
+    }
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -508,6 +564,55 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
       }
     }
     __syncwarp();
+  } else if (Cfg::PF && warp == 6) {
+    // ------------------------------------------------------------ C loader (PF)
+    // Walks the CTA's tiles in the epilogue's chunk order; chunk n goes to
+    // ring slot n % C_SLOTS once the epilogue has given back the slot's
+    // previous chunk (n - C_SLOTS).
+    if (lane == 0) {
+      int slot = 0;
+      uint32_t ph = 0;
+      uint32_t armed = 0, armed_phase = 0;  // per-slot: a load was armed / its phase
+      bool ok = true;
+      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+        const int4 tile = args.tiles[t];
+        const GemmArgs& P = tile_problem<GROUPED>(args, t);
+        if (!P.tma_c) continue;
+        const bool need = P.beta != 0.0f || tile_reaches_mask(P, tile.x, tile.y, BM, BN);
+        for (int c0 = 0; c0 < BN && tile.y + c0 < P.N; c0 += 32) {
+          if (!mbar_wait(&cfree[slot], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
+            ok = false;
+            break;
+          }
+          if (need) {
+            mbar_arrive_expect_tx(&cload[slot], Cfg::EPI_CHUNK_BYTES);
+            tma_load_2d(stage_c + slot * (128 * 32), &P.mapC, &cload[slot], tile.x, tile.y + c0);
+            armed |= 1u << slot;
+            armed_phase = (armed_phase & ~(1u << slot)) | (ph << slot);
+          } else {
+            // the slot's earlier load was consumed before the slot came back
+            armed &= ~(1u << slot);
+            mbar_arrive(&cload[slot]);
+          }
+          if (++slot == Cfg::C_SLOTS) {
+            slot = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+      // every armed load lands before the CTA exits (immediate unless the
+      // epilogue left early)
+      for (int i = 0; i < Cfg::C_SLOTS; ++i) {
+        if (!((armed >> i) & 1u)) continue;
+        const uint64_t t0 = globaltimer_ns();
+        while (!mbar_try_wait(&cload[i], (armed_phase >> i) & 1u))
+          if (globaltimer_ns() - t0 > 1000000000ull) {
+            if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
+            break;
+          }
+      }
+    }
+    __syncwarp();
   } else {
     // ------------------------------------------------------------ epilogue
     const int quarter = warp & 3;  // TMEM lane quarter this warp may access
@@ -518,8 +623,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
     int it = 0;
     bool ok = true;
     if constexpr (Cfg::PF) {
-      PfState pf{0u, 0};
-      uint32_t pending = 0;  // issuer: slots whose C load is in flight and not yet consumed
+      PfState pf{0, 0u, -1, 0};
       __half* side_base = reinterpret_cast<__half*>(stage_c + Cfg::C_SLOTS * (128 * 32));
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
         const int4 tile = args.tiles[t];
@@ -527,25 +631,13 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
         const long long gi = (long long)tile.x + row;
         const bool row_ok = gi < P.M;
         const bool tile_masked = tile_reaches_mask(P, tile.x, tile.y, BM, BN);
-        const bool need_load = P.tma_c && (P.beta != 0.0f || tile_masked);
-        // request this tile's C while its MMAs run; slots are free once the
-        // previous tile's stores have read them
-        if (issuer && P.tma_c) {
-          bulk_wait_read<0>();
-          if (need_load)
-#pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c)
-              if (tile.y + 32 * c < P.N) {
-                mbar_arrive_expect_tx(&cload[c], Cfg::EPI_CHUNK_BYTES);
-                tma_load_2d(stage_c + c * (128 * 32), &P.mapC, &cload[c], tile.x, tile.y + 32 * c);
-                pending |= 1u << c;
-              }
-        }
+        const bool need_load = P.beta != 0.0f || tile_masked;
         if constexpr (!Cfg::FOLD) {
           const int buf = it & 1;
           const uint32_t tph = (uint32_t)(it >> 1) & 1u;
           ++it;
-          if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) {
+          const bool got = mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue);
+          if (named_bar_any(1, 128, !got)) {
             ok = false;
             break;
           }
@@ -562,9 +654,11 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
             }
             if (tile.y + c0 >= P.N) continue;
             if (P.tma_c) {
-              epilogue_chunk_pf(P, stage_c, side_base, cload, pf, v, tile.x, tile.y + c0, c0 / 32, row, need_load,
-                                issuer, abort_flag);
-              pending &= ~(1u << (c0 / 32));
+              if (!epilogue_chunk_pf<Cfg::C_SLOTS>(P, stage_c, side_base, cload, cfree, pf, v, tile.x, tile.y + c0,
+                                                   row, need_load, issuer, abort_flag)) {
+                ok = false;
+                break;
+              }
             } else if (row_ok)
               epilogue_store32(P, v, gi, (long long)tile.y + c0);
           }
@@ -576,7 +670,8 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
             const int buf = it & 1;
             const uint32_t tph = (uint32_t)(it >> 1) & 1u;
             ++it;
-            if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) {
+            const bool got = mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue);
+            if (named_bar_any(1, 128, !got)) {
               ok = false;
               break;
             }
@@ -599,24 +694,14 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
           for (int c0 = 0; c0 < BN; c0 += 32) {
             if (tile.y + c0 >= P.N) continue;
             if (P.tma_c) {
-              epilogue_chunk_pf(P, stage_c, side_base, cload, pf, acc + c0, tile.x, tile.y + c0, c0 / 32, row,
-                                need_load, issuer, abort_flag);
-              pending &= ~(1u << (c0 / 32));
+              if (!epilogue_chunk_pf<Cfg::C_SLOTS>(P, stage_c, side_base, cload, cfree, pf, acc + c0, tile.x,
+                                                   tile.y + c0, row, need_load, issuer, abort_flag)) {
+                ok = false;
+                break;
+              }
             } else if (row_ok)
               epilogue_store32(P, acc + c0, gi, (long long)tile.y + c0);
           }
-        }
-      }
-      if (issuer && pending) {
-        // abort path: C loads still in flight must land before the CTA exits
-        for (int c = 0; c < Cfg::C_SLOTS; ++c) {
-          if (!((pending >> c) & 1u)) continue;
-          const uint64_t t0 = globaltimer_ns();
-          while (!mbar_try_wait(&cload[c], (pf.lphase >> c) & 1u))
-            if (globaltimer_ns() - t0 > 1000000000ull) {
-              if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
-              break;
-            }
         }
       }
     } else
@@ -631,7 +716,9 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
         ++it;
-        if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) break;
+        // one decision for all 128 epilogue threads: the chunks below hold named barriers
+        if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)))
+          break;
         tc_fence_after();
         const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
 #pragma unroll 1
@@ -659,7 +746,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ge
           const int buf = it & 1;
           const uint32_t tph = (uint32_t)(it >> 1) & 1u;
           ++it;
-          if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) {
+          if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) {
             ok = false;
             break;
           }
@@ -923,7 +1010,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       const bool tile_masked = tile_reaches_mask(args, m0, tile.y, 128, BN);
       const int buf = it & 1;
       const uint32_t tph = (uint32_t)(it >> 1) & 1u;
-      if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) break;
+      if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) break;
       tc_fence_after();
       const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
 #pragma unroll 1

@@ -347,21 +347,31 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
     const int quarter = warp & 3;
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    // scalars in registers: the stores below go through generic pointers the
+    // compiler cannot tell apart from the parameter memory, so fields read in
+    // the store loops would be re-read from it after every store
+    double* const Cg = args.C;
+    int* const raw_out = args.raw_out;
+    const long long ldc = args.ldc, ld_raw = args.ld_raw;
+    const int* const eA = args.eA;
+    const int* const eB = args.eB;
+    const double alpha = args.alpha;
+    const int N = args.N, M = args.M, tri = args.tri, raw_level = args.raw_level;
     int it = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
       const int4 tile = args.tiles[t];
       const double beta = (tile.z & kOzAccumulate) ? 1.0 : args.beta;
       const long long gi = (long long)tile.x + row;
-      const bool row_ok = gi < args.M;
-      const int ei = row_ok ? (args.eA[gi] < -1000 ? 0 : args.eA[gi]) : 0;
+      const bool row_ok = gi < M;
+      const int ei = row_ok ? (eA[gi] < -1000 ? 0 : eA[gi]) : 0;
       if (tile.w <= (tile.z & (kOzAccumulate - 1))) {
         // empty product (K range outside the operand's support): C = beta C
-        if (row_ok && beta != 1.0 && args.raw_level < 2)
+        if (row_ok && beta != 1.0 && raw_level < 2)
           for (int j = 0; j < kOzBN; ++j) {
             const long long gj = (long long)tile.y + j;
-            if (gj < args.N && (args.tri == 0 || (args.tri == 1 ? gj <= gi : gj >= gi))) {
-              double* c = args.C + gi + gj * args.ldc;
+            if (gj < N && (tri == 0 || (tri == 1 ? gj <= gi : gj >= gi))) {
+              double* c = Cg + gi + gj * ldc;
               *c = beta == 0.0 ? 0.0 : beta * *c;
             }
           }
@@ -376,38 +386,42 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
         }
         tc_fence_after();
         const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * kOzBN);
-        const bool fold = args.raw_level < 2;
+        const bool fold = raw_level < 2;
 #pragma unroll 1
         for (int c0 = 0; c0 < kOzBN; c0 += 32) {
           int v[32];
           tmem_ld32_s32(tacc + c0, v);
           if (!row_ok) continue;
           if (!fold) {
-            if (L != args.raw_level) continue;
+            if (L != raw_level) continue;
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
               const long long gj = (long long)tile.y + c0 + j;
-              if (gj < args.N && (args.tri == 0 || (args.tri == 1 ? gj <= gi : gj >= gi))) args.raw_out[gi + gj * args.ld_raw] = v[j];
+              if (gj < N && (tri == 0 || (tri == 1 ? gj <= gi : gj >= gi))) raw_out[gi + gj * ld_raw] = v[j];
             }
             continue;
           }
           double old[32];
           bool keep[32];
+          int ejs[32];
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const long long gj = (long long)tile.y + c0 + j;
-            keep[j] = gj < args.N && (args.tri == 0 || (args.tri == 1 ? gj <= gi : gj >= gi));
+            keep[j] = gj < N && (tri == 0 || (tri == 1 ? gj <= gi : gj >= gi));
             old[j] = 0.0;
-            if (keep[j] && (L > 2 || beta != 0.0)) old[j] = args.C[gi + gj * args.ldc];
+            ejs[j] = 0;
+            if (keep[j]) {
+              if (L > 2 || beta != 0.0) old[j] = Cg[gi + gj * ldc];
+              ejs[j] = eB[gj] < -1000 ? 0 : eB[gj];
+            }
           }
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             if (!keep[j]) continue;
             const long long gj = (long long)tile.y + c0 + j;
-            const int ej = args.eB[gj] < -1000 ? 0 : args.eB[gj];
-            const double scale = args.alpha * ldexp(1.0, ei + ej - 7 * L);
+            const double scale = alpha * ldexp(1.0, ei + ejs[j] - 7 * L);
             const double base = (L == 2) ? beta * old[j] : old[j];
-            args.C[gi + gj * args.ldc] = fma(scale, (double)v[j], base);
+            Cg[gi + gj * ldc] = fma(scale, (double)v[j], base);
           }
         }
         tc_fence_before();
