@@ -47,65 +47,162 @@ __device__ __forceinline__ float q8_load(const Q8Src& s, long long i, long long 
   }
 }
 
-// One 128 x 128 block per CTA: stage it in shared memory (reads coalesced
-// along the source's contiguous index), reduce max|x|, write the scale and
-// the e4m3 block K-major (128 bytes per row; K padding to the block edge is
-// written as zeros).
-__global__ void __launch_bounds__(256) q8_kernel(Q8Src src, long long rows, long long K, uint8_t* __restrict__ Q,
-                                                 long long ldq, long long qoff, float* __restrict__ scales,
-                                                 int scale_ld, int kb_off) {
-  extern __shared__ float tile[];  // [128][129]: tile[r * 129 + p]
-  __shared__ float red[8];
-  const long long r0 = (long long)blockIdx.x * kQB, p0 = (long long)blockIdx.y * kQB;
-  const int t = threadIdx.x;
-  const bool along_p = src.kind == 1;  // source contiguous along p
-  float amax = 0.f;
-  for (int idx = t; idx < kQB * kQB; idx += 256) {
-    const int r = along_p ? (idx >> 7) : (idx & 127);
-    const int p = along_p ? (idx & 127) : (idx >> 7);
-    const long long gi = r0 + r, gp = p0 + p;
-    const float v = (gi < rows && gp < K) ? q8_load(src, gi, gp) : 0.f;
-    tile[r * 129 + p] = v;
-    amax = fmaxf(amax, fabsf(v));
+// How a 128 x 128 block at (r0, p0) can be read: 0 / 1 as a plain kind-0 /
+// kind-1 block (every element inside the operand and unmasked, 16-byte
+// aligned rows), 2 when the mask zeroes all of it, -1 otherwise (diagonal,
+// partially masked or edge blocks take the scalar path).
+__device__ __forceinline__ int q8_block_kind(const Q8Src& s, long long r0, long long p0, long long rows,
+                                             long long K, bool vec) {
+  if (!vec || r0 + kQB > rows || p0 + kQB > K) return -1;
+  if (s.mask == 1) {  // keeps p <= i
+    if (p0 > r0 + kQB - 1) return 2;
+    if (p0 + kQB - 1 > r0) return -1;
+  } else if (s.mask == 2) {  // keeps p >= i
+    if (p0 + kQB - 1 < r0) return 2;
+    if (p0 < r0 + kQB - 1) return -1;
   }
+  if (s.unit && r0 < p0 + kQB && p0 < r0 + kQB) return -1;
+  switch (s.kind) {
+    case 0:
+      return 0;
+    case 1:
+      return 1;
+    case 2:  // lower-stored: i >= p reads X[i + p ld]
+      return r0 >= p0 + kQB - 1 ? 0 : (r0 + kQB - 1 < p0 ? 1 : -1);
+    default:  // upper-stored: i <= p reads X[i + p ld]
+      return r0 + kQB - 1 <= p0 ? 0 : (r0 > p0 + kQB - 1 ? 1 : -1);
+  }
+}
+
+__device__ __forceinline__ uint32_t q8_pack4(float a, float b, float c, float d, float scale) {
+  const uint32_t qa = __nv_cvt_float_to_fp8(a / scale, __NV_SATFINITE, __NV_E4M3);
+  const uint32_t qb = __nv_cvt_float_to_fp8(b / scale, __NV_SATFINITE, __NV_E4M3);
+  const uint32_t qc = __nv_cvt_float_to_fp8(c / scale, __NV_SATFINITE, __NV_E4M3);
+  const uint32_t qd = __nv_cvt_float_to_fp8(d / scale, __NV_SATFINITE, __NV_E4M3);
+  return qa | (qb << 8) | (qc << 16) | (qd << 24);
+}
+
+// Block max|x| over the CTA's 256 threads.
+__device__ __forceinline__ float q8_block_max(float amax, float* red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-  if ((t & 31) == 0) red[t >> 5] = amax;
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
   __syncthreads();
   float m = red[0];
 #pragma unroll
   for (int w = 1; w < 8; ++w) m = fmaxf(m, red[w]);
-  const float scale = m > 0.f ? m / 448.f : 1.f;
-  if (t == 0) scales[(long long)blockIdx.x * scale_ld + kb_off + blockIdx.y] = scale;
-  // thread -> (row r, 16 consecutive p)
-  for (int job = t; job < kQB * (kQB / 16); job += 256) {
-    const int r = job >> 3, c = (job & 7) * 16;
-    const long long gi = r0 + r;
-    if (gi >= rows) continue;
-    uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const __nv_fp8_storage_t q = __nv_cvt_float_to_fp8(tile[r * 129 + c + j] / scale, __NV_SATFINITE, __NV_E4M3);
-      w[j >> 2] |= (uint32_t)q << (8 * (j & 3));
+  return m;
+}
+
+// One 128 x 128 block per CTA (256 threads): s = max|x| / 448, then the
+// e4m3 block K-major (128 bytes per row; K padding to the block edge is
+// written as zeros). Interior blocks hold the whole block in registers
+// (sixteen 16-byte loads per thread, all in flight together); a block read
+// along i is transposed through a 16 KB byte tile whose 4-byte words are
+// XOR-swizzled by row so that neither its writes nor its reads conflict.
+// Other blocks read element by element, twice (max, then quantise).
+__global__ void __launch_bounds__(256) q8_kernel(Q8Src src, long long rows, long long K, uint8_t* __restrict__ Q,
+                                                 long long ldq, long long qoff, float* __restrict__ scales,
+                                                 int scale_ld, int kb_off, int vec) {
+  __shared__ __align__(16) uint32_t qs[kQB * 32];  // row r: 32 words, word w at r * 32 + (w ^ ((r >> 2) & 31))
+  __shared__ float red[8];
+  const long long r0 = (long long)blockIdx.x * kQB, p0 = (long long)blockIdx.y * kQB;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  float* const sc = scales + (long long)blockIdx.x * scale_ld + kb_off + blockIdx.y;
+  const int kind = q8_block_kind(src, r0, p0, rows, K, vec != 0);
+  if (kind == 2) {
+    if (t == 0) *sc = 1.f;
+    for (int job = t; job < kQB * (kQB / 16); job += 256) {
+      const int r = job >> 3, c = (job & 7) * 16;
+      *reinterpret_cast<uint4*>(Q + (r0 + r) * ldq + qoff + p0 + c) = make_uint4(0, 0, 0, 0);
     }
-    *reinterpret_cast<uint4*>(Q + gi * ldq + qoff + p0 + c) = make_uint4(w[0], w[1], w[2], w[3]);
+    return;
+  }
+  if (kind < 0) {
+    float amax = 0.f;
+    for (int idx = t; idx < kQB * kQB; idx += 256) {
+      const int r = src.kind == 1 ? (idx >> 7) : (idx & 127);
+      const int p = src.kind == 1 ? (idx & 127) : (idx >> 7);
+      const long long gi = r0 + r, gp = p0 + p;
+      if (gi < rows && gp < K) amax = fmaxf(amax, fabsf(q8_load(src, gi, gp)));
+    }
+    const float m = q8_block_max(amax, red);
+    const float scale = m > 0.f ? m / 448.f : 1.f;
+    if (t == 0) *sc = scale;
+    for (int job = t; job < kQB * (kQB / 16); job += 256) {
+      const int r = job >> 3, c = (job & 7) * 16;
+      const long long gi = r0 + r;
+      if (gi >= rows) continue;
+      float x[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) x[j] = (p0 + c + j < K) ? q8_load(src, gi, p0 + c + j) : 0.f;
+      *reinterpret_cast<uint4*>(Q + gi * ldq + qoff + p0 + c) =
+          make_uint4(q8_pack4(x[0], x[1], x[2], x[3], scale), q8_pack4(x[4], x[5], x[6], x[7], scale),
+                     q8_pack4(x[8], x[9], x[10], x[11], scale), q8_pack4(x[12], x[13], x[14], x[15], scale));
+    }
+    return;
+  }
+  const float* X = src.X;
+  const long long ld = src.ld;
+  float4 v[16];
+  if (kind == 1) {
+    // row r = w + 8 i, p = 4 lane .. 4 lane + 3
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      v[i] = __ldg(reinterpret_cast<const float4*>(X + (p0 + 4 * lane) + (r0 + w + 8 * i) * ld));
+  } else {
+    // p = 4 (w + 8 jj) + u, r = 4 lane .. 4 lane + 3
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        v[jj * 4 + u] =
+            __ldg(reinterpret_cast<const float4*>(X + (r0 + 4 * lane) + (p0 + 4 * (w + 8 * jj) + u) * ld));
+  }
+  float amax = 0.f;
+#pragma unroll
+  for (int i = 0; i < 16; ++i)
+    amax = fmaxf(fmaxf(amax, fmaxf(fabsf(v[i].x), fabsf(v[i].y))), fmaxf(fabsf(v[i].z), fabsf(v[i].w)));
+  const float m = q8_block_max(amax, red);
+  const float scale = m > 0.f ? m / 448.f : 1.f;
+  if (t == 0) *sc = scale;
+  if (kind == 1) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      *reinterpret_cast<uint32_t*>(Q + (r0 + w + 8 * i) * ldq + qoff + p0 + 4 * lane) =
+          q8_pack4(v[i].x, v[i].y, v[i].z, v[i].w, scale);
+    return;
+  }
+  // rows r = 4 lane + j; word s = w + 8 jj holds p = 4 s .. 4 s + 3
+#pragma unroll
+  for (int jj = 0; jj < 4; ++jj) {
+    const int s = w + 8 * jj;
+    const float4 a = v[jj * 4 + 0], b = v[jj * 4 + 1], c = v[jj * 4 + 2], d = v[jj * 4 + 3];
+    qs[(4 * lane + 0) * 32 + (s ^ lane)] = q8_pack4(a.x, b.x, c.x, d.x, scale);
+    qs[(4 * lane + 1) * 32 + (s ^ lane)] = q8_pack4(a.y, b.y, c.y, d.y, scale);
+    qs[(4 * lane + 2) * 32 + (s ^ lane)] = q8_pack4(a.z, b.z, c.z, d.z, scale);
+    qs[(4 * lane + 3) * 32 + (s ^ lane)] = q8_pack4(a.w, b.w, c.w, d.w, scale);
+  }
+  __syncthreads();
+  // 16-byte pieces: lanes (c = lane & 7, g = lane >> 3) of warp-iteration
+  // wi = 8 it + w take row r = 16 (wi >> 2) + 4 g + (wi & 3), bytes 16 c ..
+#pragma unroll
+  for (int it = 0; it < 4; ++it) {
+    const int wi = 8 * it + w, c = lane & 7, g = lane >> 3;
+    const int r = 16 * (wi >> 2) + 4 * g + (wi & 3);
+    const int sw = (r >> 2) & 31;
+    const uint32_t* row = qs + r * 32;
+    *reinterpret_cast<uint4*>(Q + (r0 + r) * ldq + qoff + p0 + 16 * c) =
+        make_uint4(row[(4 * c + 0) ^ sw], row[(4 * c + 1) ^ sw], row[(4 * c + 2) ^ sw], row[(4 * c + 3) ^ sw]);
   }
 }
 
-constexpr size_t kQ8Smem = (size_t)kQB * 129 * sizeof(float);
-
 tb_status quantize(const Q8Src& src, long long rows, long long K, uint8_t* Q, long long ldq, long long qoff,
                    float* scales, int scale_ld, int kb_off, cudaStream_t st) {
-  static bool attr[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !attr[dev]) {
-    TB_CUDA_TRY(cudaFuncSetAttribute(q8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQ8Smem));
-    attr[dev] = true;
-  }
   if (rows == 0 || K == 0) return TB_SUCCESS;
+  const int vec = (reinterpret_cast<uintptr_t>(src.X) % 16 == 0 && src.ld % 4 == 0) ? 1 : 0;
   dim3 g((unsigned)((rows + kQB - 1) / kQB), (unsigned)((K + kQB - 1) / kQB));
-  q8_kernel<<<g, 256, kQ8Smem, st>>>(src, rows, K, Q, ldq, qoff, scales, scale_ld, kb_off);
+  q8_kernel<<<g, 256, 0, st>>>(src, rows, K, Q, ldq, qoff, scales, scale_ld, kb_off, vec);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   return TB_SUCCESS;
