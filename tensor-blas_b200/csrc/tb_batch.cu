@@ -37,29 +37,43 @@ struct ConvJob {
   __half* lo;
   long long ldd;
   int tri;
-  long long first;  // first column index of this job in the grouped launch
+  long long first;  // first block index of this job in the grouped launch
 };
 
-// One column of one job per block (binary search of the job by column index).
-__global__ void __launch_bounds__(256) conv_grouped_kernel(const ConvJob* __restrict__ jobs, int njobs) {
-  int lo = 0, hi = njobs - 1;
+constexpr int kConvPerThread = 8;
+constexpr int kConvPerBlock = 256 * kConvPerThread;  // elements per block of the grouped conversion
+
+// kConvPerBlock consecutive elements (column-major order over rows x cols)
+// of one job per block, so short columns of small instances do not leave
+// most of a block idle. blk_job maps a block to its job (one load, where a
+// search over the job table would be a chain of dependent loads per block);
+// each thread issues all its loads before it converts and stores.
+__global__ void __launch_bounds__(256) conv_grouped_kernel(const ConvJob* __restrict__ jobs,
+                                                           const int* __restrict__ blk_job) {
   const long long b = blockIdx.x;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (jobs[mid].first <= b)
-      lo = mid;
-    else
-      hi = mid - 1;
+  const ConvJob& jb = jobs[blk_job[b]];
+  const long long rows = jb.rows, total = jb.rows * jb.cols, lds = jb.lds, ldd = jb.ldd;
+  const float* const src = jb.src;
+  __half* const dhi = jb.hi;
+  __half* const dlo = jb.lo;
+  const int tri = jb.tri;
+  const long long e0 = (b - jb.first) * kConvPerBlock + threadIdx.x;
+  long long at[kConvPerThread];
+  float f[kConvPerThread];
+#pragma unroll
+  for (int q = 0; q < kConvPerThread; ++q) {
+    const long long e = e0 + q * 256;
+    const long long j = e / rows, i = e - j * rows;
+    const bool ok = e < total && !(tri == 2 && i < ((j >> 3) << 3));
+    at[q] = ok ? i + j * ldd : -1;
+    f[q] = ok ? __ldg(src + i + j * lds) : 0.f;
   }
-  const ConvJob& jb = jobs[lo];
-  const long long j = b - jb.first;
-  long long i0 = threadIdx.x;
-  if (jb.tri == 2) i0 += (j >> 3) << 3;
-  for (long long i = i0; i < jb.rows; i += blockDim.x) {
-    const float f = jb.src[i + j * jb.lds];
-    const __half h = __float2half_rn(f);
-    jb.hi[i + j * jb.ldd] = h;
-    if (jb.lo) jb.lo[i + j * jb.ldd] = __float2half_rn((f - __half2float(h)) * 2048.f);
+#pragma unroll
+  for (int q = 0; q < kConvPerThread; ++q) {
+    if (at[q] < 0) continue;
+    const __half h = __float2half_rn(f[q]);
+    dhi[at[q]] = h;
+    if (dlo) dlo[at[q]] = __float2half_rn((f[q] - __half2float(h)) * 2048.f);
   }
 }
 
@@ -72,6 +86,7 @@ struct Launch {
   double flops = 0;
   int4* d_tiles = nullptr;
   int* d_prob = nullptr;
+  int* d_sched = nullptr;  // this launch's tile counter (device-side scheduler)
 };
 
 // Grows a byte arena with 256-byte aligned slices.
@@ -92,6 +107,7 @@ struct tb_batch_s {
   void* scratch = nullptr;
   void* tables = nullptr;
   tb::ConvJob* d_conv = nullptr;
+  int* d_blk_job = nullptr;  // job index of each block of the grouped conversion
   int nconv = 0;
   long long conv_blocks = 0;
   tb::DiagJob* d_diag = nullptr;
@@ -100,6 +116,7 @@ struct tb_batch_s {
   tb::ChainJob* d_chain = nullptr;
   int nchain = 0;
   tb::GemmArgs* d_problems = nullptr;
+  int* d_sched = nullptr;  // one tile counter per grouped GEMM launch
   std::vector<tb::Launch> launches;
 };
 
@@ -240,7 +257,7 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
   std::vector<SyrkPlan> syrks;
   std::vector<TrsmPlan> trsms;
   struct TrsmOff {
-    size_t ah, al, xh, xl, wh, wl, rh, rl, d;
+    size_t ah, al, xh, xl, wh, wl, rh, rl, d, wg;
   };
   std::vector<TrsmOff> toff;
   for (int i = 0; i < count; ++i) {
@@ -277,6 +294,7 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
       o.rh = ar.take((size_t)ldh * p.leaf * 2);
       o.rl = ar.take((size_t)ldh * p.leaf * 2);
       o.d = ar.take((size_t)((ni + 31) / 32) * 1024 * sizeof(double));
+      o.wg = ar.take((size_t)p.wstride * p.leaf_start.size() * sizeof(double));
       trsms.push_back(p);
       toff.push_back(o);
     }
@@ -297,11 +315,11 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
   std::vector<GemmCall> probs;  // global problem list
   std::vector<int> prob_step, prob_leaf;
   std::vector<long> prob_k;
-  long long conv_cols = 0, diag_blocks = 0;
+  long long conv_nblk = 0, diag_blocks = 0;
   auto add_conv = [&](const float* src, long long rows, long long cols, long long lds, __half* hi, __half* lo,
                       long long ldd, int tri) {
-    conv.push_back(ConvJob{src, rows, cols, lds, hi, lo, ldd, tri, conv_cols});
-    conv_cols += cols;
+    conv.push_back(ConvJob{src, rows, cols, lds, hi, lo, ldd, tri, conv_nblk});
+    conv_nblk += (rows * cols + kConvPerBlock - 1) / kConvPerBlock;
   };
   for (SyrkPlan& s : syrks) {
     add_conv(s.A, s.n, s.n, s.lda, H(s.off_h), hilo ? H(s.off_l) : nullptr, s.ldh, 0);
@@ -341,7 +359,8 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
     for (size_t l = 0; l < p.leaf_start.size(); ++l) {
       const long s = p.leaf_start[l];
       chain.push_back(ChainJob{p.A, (long long)p.lda, (int)s, (int)std::min<long>(p.leaf, p.n - s), D,
-                               p.wh + l * p.wstride, p.wl + l * p.wstride, p.ldw});
+                               p.wh + l * p.wstride, p.wl + l * p.wstride, p.ldw,
+                               reinterpret_cast<double*>(base + o.wg) + l * p.wstride});
     }
     // as tb_strsm: orders below 2048 keep the reference's FP32 accuracy
     trsm_ops(p, (split == Split::kPlain && p.n < 2048) ? Split::kHiLo : split, 0, p.n);
@@ -381,14 +400,37 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
         }
         L.flops += probs[i].flops;
       }
-      if (!L.tiles.empty()) b->launches.push_back(std::move(L));
+      if (L.tiles.empty()) continue;
+      // longest K range first: CTAs claim tiles in this order as they free
+      // up, so the short tiles fill the tail
+      std::vector<int> order(L.tiles.size());
+      for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return L.tiles[x].w - L.tiles[x].z > L.tiles[y].w - L.tiles[y].z;
+      });
+      std::vector<int4> st_tiles(order.size());
+      std::vector<int> st_prob(order.size());
+      for (size_t q = 0; q < order.size(); ++q) {
+        st_tiles[q] = L.tiles[order[q]];
+        st_prob[q] = L.prob[order[q]];
+      }
+      L.tiles.swap(st_tiles);
+      L.prob.swap(st_prob);
+      b->launches.push_back(std::move(L));
     }
   }
   Arena tab;
   const size_t o_probs = tab.take(sizeof(GemmArgs) * std::max(nprob, 1));
   const size_t o_conv = tab.take(sizeof(ConvJob) * std::max<size_t>(conv.size(), 1));
+  std::vector<int> blk_job((size_t)conv_nblk);
+  for (size_t q = 0; q < conv.size(); ++q) {
+    const long long e = q + 1 < conv.size() ? conv[q + 1].first : conv_nblk;
+    for (long long x = conv[q].first; x < e; ++x) blk_job[(size_t)x] = (int)q;
+  }
+  const size_t o_blk = tab.take(sizeof(int) * std::max<size_t>(blk_job.size(), 1));
   const size_t o_diag = tab.take(sizeof(DiagJob) * std::max<size_t>(diag.size(), 1));
   const size_t o_chain = tab.take(sizeof(ChainJob) * std::max<size_t>(chain.size(), 1));
+  const size_t o_sched = tab.take(sizeof(int) * std::max<size_t>(b->launches.size(), 1));
   std::vector<size_t> o_tiles, o_prob;
   for (Launch& L : b->launches) {
     o_tiles.push_back(tab.take(sizeof(int4) * L.tiles.size()));
@@ -403,6 +445,7 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
   std::vector<char> host(tab.used, 0);
   memcpy(host.data() + o_probs, hargs.data(), sizeof(GemmArgs) * nprob);
   memcpy(host.data() + o_conv, conv.data(), sizeof(ConvJob) * conv.size());
+  memcpy(host.data() + o_blk, blk_job.data(), sizeof(int) * blk_job.size());
   memcpy(host.data() + o_diag, diag.data(), sizeof(DiagJob) * diag.size());
   memcpy(host.data() + o_chain, chain.data(), sizeof(ChainJob) * chain.size());
   b->d_problems = reinterpret_cast<GemmArgs*>(tb_ + o_probs);
@@ -412,14 +455,17 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
     memcpy(host.data() + o_prob[l], L.prob.data(), sizeof(int) * L.prob.size());
     L.d_tiles = reinterpret_cast<int4*>(tb_ + o_tiles[l]);
     L.d_prob = reinterpret_cast<int*>(tb_ + o_prob[l]);
+    L.d_sched = reinterpret_cast<int*>(tb_ + o_sched) + l;
   }
+  b->d_sched = reinterpret_cast<int*>(tb_ + o_sched);
   if (cudaMemcpy(b->tables, host.data(), tab.used, cudaMemcpyHostToDevice) != cudaSuccess) {
     tb_batch_destroy(b);
     return TB_ERROR_CUDA;
   }
   b->d_conv = reinterpret_cast<ConvJob*>(tb_ + o_conv);
+  b->d_blk_job = reinterpret_cast<int*>(tb_ + o_blk);
   b->nconv = (int)conv.size();
-  b->conv_blocks = conv_cols;
+  b->conv_blocks = conv_nblk;
   b->d_diag = reinterpret_cast<DiagJob*>(tb_ + o_diag);
   b->ndiag = (int)diag.size();
   b->diag_blocks = diag_blocks;
@@ -438,14 +484,18 @@ extern "C" tb_status tb_batch_run(tb_batch_t b) {
   using namespace tb;
   if (!b) return TB_ERROR_INVALID_VALUE;
   cudaStream_t st = current_stream();
-  if (b->nconv > 0) {
+  if (b->nconv > 0 && b->conv_blocks > 0) {
     if (b->conv_blocks > 0x7fffffffLL) return TB_ERROR_NOT_SUPPORTED;
-    conv_grouped_kernel<<<(unsigned)b->conv_blocks, 256, 0, st>>>(b->d_conv, b->nconv);
+    conv_grouped_kernel<<<(unsigned)b->conv_blocks, 256, 0, st>>>(b->d_conv, b->d_blk_job);
     TB_CUDA_TRY(cudaGetLastError());
     note_launch();
   }
   TB_TRY(trsm_inverses_grouped(b->d_diag, b->ndiag, b->diag_blocks, b->d_chain, b->nchain, st));
+  // the launches' tile counters start at zero on every run (a memset node
+  // when the run is captured in a graph)
+  if (!b->launches.empty()) TB_CUDA_TRY(cudaMemsetAsync(b->d_sched, 0, sizeof(int) * b->launches.size(), st));
   for (Launch& L : b->launches)
-    TB_TRY(gemm_launch_grouped(L.split, b->d_problems, L.d_tiles, L.d_prob, (int)L.tiles.size(), L.flops, st));
+    TB_TRY(gemm_launch_grouped(L.split, b->d_problems, L.d_tiles, L.d_prob, (int)L.tiles.size(), L.flops, st,
+                               L.d_sched));
   return TB_SUCCESS;
 }

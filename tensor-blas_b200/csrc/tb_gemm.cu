@@ -324,10 +324,11 @@ tb_status gemm_prepare_grouped() {
 // Grouped launch over problems whose descriptors (built by gemm_build_args
 // and copied to the device) all use MN-major operands.
 tb_status gemm_launch_grouped(Split split, const GemmArgs* d_problems, const int4* d_tiles, const int* d_tile_prob,
-                              int num_tiles, double flops, cudaStream_t stream) {
+                              int num_tiles, double flops, cudaStream_t stream, int* d_sched) {
   if (num_tiles <= 0) return TB_SUCCESS;
   GemmArgs a;
   memset(&a, 0, sizeof(a));
+  a.sched = d_sched;
   a.tiles = d_tiles;
   a.num_tiles = num_tiles;
   a.problems = d_problems;

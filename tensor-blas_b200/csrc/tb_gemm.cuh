@@ -83,7 +83,44 @@ struct GemmArgs {
   // GemmArgs (64-byte aligned; their tensor maps are read from global memory).
   const struct GemmArgs* problems;
   const int* tile_prob;
+  // Device-side tile scheduler: nullptr = static striding (CTA b takes tiles
+  // b, b + grid, ...); otherwise a zeroed counter from which the CTAs'
+  // producers claim tiles one at a time.
+  int* sched;
 };
+
+// Tile hand-off inside a CTA under the device-side scheduler: the producer
+// claims a tile and queues its index (or -1, the end) in a kTileQ-deep ring;
+// the MMA issuer, the four epilogue warps and (prefetch variants) the C
+// loader each take the indices in order and release the slot.
+constexpr int kTileQ = 4;
+
+// The next tile of a consumer role: static striding, or the producer's
+// queue (q/ph: the role's ring position). EPI: called by all 128 epilogue
+// threads together, which then agree on the result.
+template <bool EPI>
+__device__ __forceinline__ int next_tile(const GemmArgs& args, int t, const volatile int* tq_idx, uint64_t* tq_full,
+                                         uint64_t* tq_empty, int& q, uint32_t& ph, volatile int* abort_flag,
+                                         int code) {
+  if (!args.sched) {
+    const int n = t < 0 ? (int)blockIdx.x : t + (int)gridDim.x;
+    return n < args.num_tiles ? n : -1;
+  }
+  const bool got = mbar_wait(&tq_full[q], ph, abort_flag, args.err, code);
+  int v = got ? tq_idx[q] : -1;
+  if constexpr (EPI) {
+    if (named_bar_any(1, 128, !got)) v = -1;
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(&tq_empty[q]);
+  } else {
+    mbar_arrive(&tq_empty[q]);
+  }
+  if (++q == kTileQ) {
+    q = 0;
+    ph ^= 1u;
+  }
+  return v;
+}
 
 // The problem a tile belongs to: the launch's own arguments, or (grouped
 // launches) one of the descriptors in global memory.
@@ -131,7 +168,7 @@ struct GemmCfg {
   static constexpr int C_SLOTS = PF ? (NSPLIT == 1 ? 6 : 4) : 2;
   static constexpr int SIDE_BYTES = PF ? 2 * EPI_CHUNK_BYTES : 0;  // PF: two fp16 hi/lo side buffers
   static constexpr int EPI_BYTES = C_SLOTS * EPI_CHUNK_BYTES + SIDE_BYTES;
-  static constexpr int BAR_BYTES = 256;
+  static constexpr int BAR_BYTES = 512;
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + BAR_BYTES;
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
   static constexpr uint32_t IDESC = idesc_f16(BM, BN, false, A_MN, B_MN);
@@ -252,17 +289,21 @@ __device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const flo
 struct EpiState {
   int chunk;        // staged chunks written so far (selects the smem buffer)
   uint32_t lphase;  // per-buffer phase bit of the C-load barriers
+  bool last_side;   // the previous chunk staged side copies (it used both buffers)
 };
 
 // TMA path for one 128 x 32 chunk at (m0, gj0): v[] holds this thread's row
 // (32 consecutive columns). All 128 epilogue threads call it together.
 // With TMA side copies (tma_out) the second staging buffer holds the fp16
-// hi/lo chunk (8 KB each) and the fp32 chunk is single-buffered.
+// hi/lo chunk (8 KB each) and the fp32 chunk is single-buffered; otherwise
+// chunks alternate between the two buffers. Problems of a grouped launch may
+// differ in this, so the wait before reusing a buffer looks at the previous
+// chunk's mode.
 __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* stage, uint64_t* cload, EpiState& es,
                                                    const float* v, int m0, int gj0, int row, bool need_load,
-                                                   bool issuer, volatile int* abort_flag, bool single_buffer) {
+                                                   bool issuer, volatile int* abort_flag) {
   const EpiK k(args);
-  const bool side_mode = single_buffer || args.tma_out != 0;
+  const bool side_mode = args.tma_out != 0;
   const bool side = args.tma_out != 0 && gj0 < args.out_n && m0 < args.out_m;
   const bool copies = !side_mode && args.out_hi && (long long)m0 + row < args.out_m;
   const int b = side_mode ? 0 : (es.chunk & 1);
@@ -270,8 +311,8 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
   __half* Hs = reinterpret_cast<__half*>(stage + 128 * 32);
   __half* Ls = Hs + 128 * 32;
   if (issuer) {
-    if (side_mode)
-      bulk_wait_read<0>();  // single-buffered: every earlier store has read smem
+    if (side_mode || es.last_side)
+      bulk_wait_read<0>();  // this chunk or the previous one uses both buffers: every earlier store has read smem
     else
       bulk_wait_read<1>();  // the store that last used buffer b has finished reading it
     if (need_load) {
@@ -313,6 +354,7 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
   }
   if (copies) store_fp16_copies(args, r, gi, gj0);
   ++es.chunk;
+  es.last_side = side_mode;
 }
 
 // PF epilogue, one 128 x 32 chunk (columns gj0..gj0+31) staged in the next
@@ -401,7 +443,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
   uint64_t* drain = tempty + 2;      // [1] teardown barrier for the MMA issuer
   uint64_t* cload = drain + 1;       // [C_SLOTS] C-chunk loads of the TMA epilogue
   uint64_t* cfree = cload + Cfg::C_SLOTS;  // [C_SLOTS] PF: ring slots the epilogue gave back
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cfree + Cfg::C_SLOTS);
+  uint64_t* tq_full = cfree + Cfg::C_SLOTS;  // [kTileQ] tile hand-off (device-side scheduler)
+  uint64_t* tq_empty = tq_full + kTileQ;     // [kTileQ]
+  int* tq_idx = reinterpret_cast<int*>(tq_empty + kTileQ);  // [kTileQ]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tq_idx + kTileQ);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5;
@@ -419,6 +464,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
     for (int b = 0; b < Cfg::C_SLOTS; ++b) {
       mbar_init(&cload[b], 1);
       mbar_init(&cfree[b], 1);
+    }
+    for (int b = 0; b < kTileQ; ++b) {
+      mbar_init(&tq_full[b], 1);
+      mbar_init(&tq_empty[b], 1 + 4 + (Cfg::PF ? 1 : 0));  // MMA issuer, epilogue warps, C loader
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -453,7 +502,27 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
       uint32_t ph = 0;
       uint32_t issued_mask = 0, phase_mask = 0;  // per-stage: copy issued / its phase
       bool ok = true;
-      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+      const bool dyn = args.sched != nullptr;
+      int tq = 0;
+      uint32_t tq_ph = 0;
+      int t = dyn ? atomicAdd(args.sched, 1) : (int)blockIdx.x;
+      while (ok) {
+        if (t >= args.num_tiles) t = -1;
+        if (dyn) {
+          // hand the tile (or the end mark) to the other roles
+          if (!mbar_wait(&tq_empty[tq], tq_ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
+            ok = false;
+            break;
+          }
+          tq_idx[tq] = t;
+          mbar_arrive(&tq_full[tq]);
+          if (++tq == kTileQ) {
+            tq = 0;
+            tq_ph ^= 1u;
+          }
+        }
+        if (t < 0) break;
+        const int t_next = dyn ? atomicAdd(args.sched, 1) : t + (int)gridDim.x;  // claimed early: its latency hides
         const int4 tile = args.tiles[t];
         for (int kb = tile.z; kb < tile.w; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
@@ -477,6 +546,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
             ph ^= 1u;
           }
         }
+        t = t_next;
       }
       if (!ok) {
         // Abort path: let every copy in flight land before the CTA exits.
@@ -504,7 +574,11 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
       bool ok = true;
       bool any = false;
       const int kc = Cfg::FOLD ? args.kchunk : (1 << 30);
-      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+      int tq = 0;
+      uint32_t tq_ph = 0;
+      for (int t = next_tile<false>(args, -1, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag, kDevErrTimeoutMma);
+           t >= 0 && ok;
+           t = next_tile<false>(args, t, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag, kDevErrTimeoutMma)) {
         const int4 tile = args.tiles[t];
         for (int c0 = tile.z; c0 < tile.w && ok; c0 += kc, ++it) {
           const int c1 = (tile.w - c0 > kc) ? c0 + kc : tile.w;
@@ -574,7 +648,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
       uint32_t ph = 0;
       uint32_t armed = 0, armed_phase = 0;  // per-slot: a load was armed / its phase
       bool ok = true;
-      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+      int tq = 0;
+      uint32_t tq_ph = 0;
+      for (int t = next_tile<false>(args, -1, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag,
+                                    kDevErrTimeoutProducer);
+           t >= 0 && ok;
+           t = next_tile<false>(args, t, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag, kDevErrTimeoutProducer)) {
         const int4 tile = args.tiles[t];
         const GemmArgs& P = tile_problem<GROUPED>(args, t);
         if (!P.tma_c) continue;
@@ -619,13 +698,17 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const bool issuer = (warp == 2 && lane == 0);
-    EpiState es{0, 0u};
+    EpiState es{0, 0u, false};
     int it = 0;
     bool ok = true;
+    int tq = 0;
+    uint32_t tq_ph = 0;
     if constexpr (Cfg::PF) {
       PfState pf{0, 0u, -1, 0};
       __half* side_base = reinterpret_cast<__half*>(stage_c + Cfg::C_SLOTS * (128 * 32));
-      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+      for (int t = next_tile<true>(args, -1, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag, kDevErrTimeoutEpilogue);
+           t >= 0 && ok;
+           t = next_tile<true>(args, t, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag, kDevErrTimeoutEpilogue)) {
         const int4 tile = args.tiles[t];
         const GemmArgs& P = tile_problem<GROUPED>(args, t);
         const long long gi = (long long)tile.x + row;
@@ -680,8 +763,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
 #pragma unroll
             for (int c0 = 0; c0 < BN; c0 += 32) {
               float v[32], w[32];
-              tmem_ld32(tacc + c0, v);
-              tmem_ld32(tacc + BN + c0, w);
+              tmem_ld32x2(tacc + c0, tacc + BN + c0, v, w);
 #pragma unroll
               for (int j = 0; j < 32; ++j) acc[c0 + j] += fmaf(args.corr_scale, w[j], v[j]);
             }
@@ -705,13 +787,18 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
         }
       }
     } else
-    for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+    for (int t = next_tile<true>(args, -1, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag, kDevErrTimeoutEpilogue);
+         t >= 0 && ok;
+         t = next_tile<true>(args, t, tq_idx, tq_full, tq_empty, tq, tq_ph, abort_flag, kDevErrTimeoutEpilogue)) {
       const int4 tile = args.tiles[t];
       const GemmArgs& P = tile_problem<GROUPED>(args, t);
       const long long gi = (long long)tile.x + row;
       const bool row_ok = gi < P.M;
       // the tile crosses the masked (upper) region: min(i - j) < diag
       const bool tile_masked = tile_reaches_mask(P, tile.x, tile.y, BM, BN);
+      // masked tiles with beta == 0 store their unmasked elements directly:
+      // the TMA path would first have to load C to keep the masked ones
+      const bool direct = tile_masked && P.beta == 0.0f;
       if constexpr (!Cfg::FOLD) {
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -730,10 +817,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[buf]);
           }
-          if (P.tma_c) {
+          if (P.tma_c && !direct) {
             if (tile.y + c0 < P.N)
               epilogue_chunk_tma(P, stage_c, cload, es, v, tile.x, tile.y + c0, row, P.beta != 0.0f || tile_masked,
-                                 issuer, abort_flag, GROUPED);
+                                 issuer, abort_flag);
           } else if (row_ok) {
             epilogue_store32(P, v, gi, (long long)tile.y + c0);
           }
@@ -768,8 +855,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
 #pragma unroll
             for (int c0 = 0; c0 < BN; c0 += 32) {
               float v[32], w[32];
-              tmem_ld32(tacc + c0, v);
-              tmem_ld32(tacc + BN + c0, w);
+              tmem_ld32x2(tacc + c0, tacc + BN + c0, v, w);
 #pragma unroll
               for (int j = 0; j < 32; ++j) acc[c0 + j] += fmaf(args.corr_scale, w[j], v[j]);
             }
@@ -781,10 +867,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
         if (!ok) break;
 #pragma unroll
         for (int c0 = 0; c0 < BN; c0 += 32) {
-          if (P.tma_c) {
+          if (P.tma_c && !direct) {
             if (tile.y + c0 < P.N)
               epilogue_chunk_tma(P, stage_c, cload, es, acc + c0, tile.x, tile.y + c0, row,
-                                 P.beta != 0.0f || tile_masked, issuer, abort_flag, GROUPED);
+                                 P.beta != 0.0f || tile_masked, issuer, abort_flag);
           } else if (row_ok) {
             epilogue_store32(P, acc + c0, gi, (long long)tile.y + c0);
           }
@@ -1000,7 +1086,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const bool issuer = (warp == 2 && lane == 0);
-    EpiState es{0, 0u};
+    EpiState es{0, 0u, false};
     int it = 0;
     for (int t = pair; t < args.num_tiles; t += npairs, ++it) {
       const int4 tile = args.tiles[t];
@@ -1008,6 +1094,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       const long long gi = (long long)m0 + row;
       const bool row_ok = gi < args.M;
       const bool tile_masked = tile_reaches_mask(args, m0, tile.y, 128, BN);
+      const bool direct = tile_masked && args.beta == 0.0f;  // as in the single-CTA kernel
       const int buf = it & 1;
       const uint32_t tph = (uint32_t)(it >> 1) & 1u;
       if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) break;
@@ -1022,10 +1109,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
         }
-        if (args.tma_c) {
+        if (args.tma_c && !direct) {
           if (tile.y + c0 < args.N && m0 < args.M)
             epilogue_chunk_tma(args, stage_c, cload, es, v, m0, tile.y + c0, row, args.beta != 0.0f || tile_masked,
-                               issuer, abort_flag, false);
+                               issuer, abort_flag);
         } else if (row_ok) {
           epilogue_store32(args, v, gi, (long long)tile.y + c0);
         }

@@ -110,11 +110,13 @@ tb_status gemm_launch_plan(GemmCall& call, const std::vector<int4>& plan, cudaSt
 
 // Grouped launches: each problem's descriptor is built on the host by
 // gemm_build_args (tensor maps included), copied to a 64-byte aligned device
-// array, and every tile carries the index of its problem.
+// array, and every tile carries the index of its problem. d_sched: a zeroed
+// device counter selects the device-side tile scheduler (CTAs claim tiles
+// in list order as they free up); nullptr keeps static striding.
 struct GemmArgs;
 tb_status gemm_build_args(const GemmCall& c, GemmArgs* out);
 tb_status gemm_launch_grouped(Split split, const GemmArgs* d_problems, const int4* d_tiles, const int* d_tile_prob,
-                              int num_tiles, double flops, cudaStream_t stream);
+                              int num_tiles, double flops, cudaStream_t stream, int* d_sched = nullptr);
 
 // Tile plans (host vectors of {m0, n0, kb_begin, kb_end}); uploaded and
 // cached on the device by `upload_tiles`.
@@ -152,6 +154,7 @@ struct ChainJob {
   __half* Whi;
   __half* Wlo;
   long long ldw;
+  double* Wg;  // FP64 working panels of the inverse (ldw x size)
 };
 tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblocks, const ChainJob* d_chain,
                                 int nchain, cudaStream_t st);

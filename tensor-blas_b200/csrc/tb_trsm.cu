@@ -88,118 +88,17 @@ __global__ void __launch_bounds__(32) diag_inv32_grouped_kernel(const DiagJob* _
 
 // Column chain j of the inverse of leaf block b (rows/cols [s, s+size)):
 //   W[i][j] = -Dinv_i * sum_{p=j}^{i-1} L[i][p] W[p][j]   (32x32 sub-blocks)
-// The 32-wide column panel of W lives in shared memory (FP64). Each 32x32
-// sub-block of L and each Dinv_i is staged (transposed) through shared memory
-// with coalesced loads; each of the 128 threads owns a 2 x 4 block of the
-// 32x32 result so every shared-memory load feeds several FMAs. The result is
-// written as the FP16 hi/lo pair (lo scaled by 2^11) of W, or as FP64 W when
-// w64 is given, column-major with leading dimension ldw, zeros above the
-// diagonal.
+// The growing 32-wide column panel of W is kept in global memory (FP64,
+// column-major, leading dimension ldg); each 32x32 sub-block of L, each W
+// block and each Dinv_i is staged (transposed) through a 32 x 32 shared tile
+// with coalesced loads, and each of the 128 threads owns a 2 x 4 block of
+// the 32x32 result so every shared-memory load feeds several FMAs. A CTA
+// needs ~27 KB of shared memory, so several share an SM and all panels of
+// all leaves run concurrently. The result is written as the FP16 hi/lo pair
+// (lo scaled by 2^11) of W with leading dimension ldw, or, without hi, the
+// FP64 panel is W itself; zeros above the diagonal.
 constexpr int kChainThreads = 128;
 
-template <class T>
-__device__ __forceinline__ void trtri_chain_body(const T* __restrict__ A, long long lda, int s, int size,
-                                                 const double* __restrict__ D, __half* __restrict__ hi,
-                                                 __half* __restrict__ lo, double* __restrict__ w64, long long ldw,
-                                                 int j) {
-  extern __shared__ __align__(16) double sm[];
-  __shared__ __align__(16) double LsT[32][34];  // LsT[k][r] = L(r, k) of the staged sub-block (or Dinv_i)
-  __shared__ __align__(16) double Ts[32][36];   // Ts[k][c]
-  const int nsub = (size + 31) / 32;
-  if (j >= nsub) return;
-  double* Wp = sm;  // [(nsub - j) * 32][32]: Wp[row * 32 + col], row relative to 32j
-  const int tid = threadIdx.x;
-  const int r0 = 2 * (tid & 15), c0 = 4 * (tid >> 4);  // 2 x 4 output block
-  const int lr = tid & 31, lc = tid >> 5;              // load role: row lr, columns lc + 4q
-  const long long sub0 = (long long)s / 32;
-  for (int q = 0; q < 8; ++q) {
-    const int c = lc + 4 * q;
-    Wp[lr * 32 + c] = D[(sub0 + j) * 1024 + lr + 32 * c];
-  }
-  __syncthreads();
-  for (int i = j + 1; i < nsub; ++i) {
-    double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-    for (int p = j; p < i; ++p) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int cc = lc + 4 * q;
-        const int gr = 32 * i + lr, gc = 32 * p + cc;
-        LsT[cc][lr] = (gr < size && gc < size) ? (double)A[(long long)s + gr + ((long long)s + gc) * lda] : 0.0;
-      }
-      __syncthreads();
-      const double* wrow = Wp + (32 * (p - j)) * 32;
-#pragma unroll 4
-      for (int kk = 0; kk < 32; ++kk) {
-        const double2 l = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
-        const double2 w01 = *reinterpret_cast<const double2*>(wrow + kk * 32 + c0);
-        const double2 w23 = *reinterpret_cast<const double2*>(wrow + kk * 32 + c0 + 2);
-        acc[0][0] = fma(l.x, w01.x, acc[0][0]);
-        acc[0][1] = fma(l.x, w01.y, acc[0][1]);
-        acc[0][2] = fma(l.x, w23.x, acc[0][2]);
-        acc[0][3] = fma(l.x, w23.y, acc[0][3]);
-        acc[1][0] = fma(l.y, w01.x, acc[1][0]);
-        acc[1][1] = fma(l.y, w01.y, acc[1][1]);
-        acc[1][2] = fma(l.y, w23.x, acc[1][2]);
-        acc[1][3] = fma(l.y, w23.y, acc[1][3]);
-      }
-      __syncthreads();
-    }
-    // T -> shared; Dinv_i -> LsT (transposed: LsT[k][r] = Dinv_i(r, k))
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) Ts[r0 + a][c0 + b] = acc[a][b];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int cc = lc + 4 * q;
-      LsT[cc][lr] = D[(sub0 + i) * 1024 + lr + 32 * cc];
-    }
-    __syncthreads();
-    double o[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-#pragma unroll 4
-    for (int kk = 0; kk < 32; ++kk) {
-      const double2 d = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
-      const double2 t01 = *reinterpret_cast<const double2*>(&Ts[kk][c0]);
-      const double2 t23 = *reinterpret_cast<const double2*>(&Ts[kk][c0 + 2]);
-      o[0][0] = fma(-d.x, t01.x, o[0][0]);
-      o[0][1] = fma(-d.x, t01.y, o[0][1]);
-      o[0][2] = fma(-d.x, t23.x, o[0][2]);
-      o[0][3] = fma(-d.x, t23.y, o[0][3]);
-      o[1][0] = fma(-d.y, t01.x, o[1][0]);
-      o[1][1] = fma(-d.y, t01.y, o[1][1]);
-      o[1][2] = fma(-d.y, t23.x, o[1][2]);
-      o[1][3] = fma(-d.y, t23.y, o[1][3]);
-    }
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) Wp[(32 * (i - j) + r0 + a) * 32 + c0 + b] = o[a][b];
-    __syncthreads();
-  }
-  // write the 32 columns [32j, 32j+32) of W for all rows of the leaf
-  for (int q = 0; q < 8; ++q) {
-    const int c = lc + 4 * q;
-    const int gc = 32 * j + c;
-    if (gc >= size) continue;
-    for (int row = lr; row < size; row += 32) {
-      double v = 0.0;
-      if (row >= 32 * j) v = Wp[(row - 32 * j) * 32 + c];
-      if (w64) {
-        w64[row + (long long)gc * ldw] = v;
-        continue;
-      }
-      const __half h = __float2half_rn((float)v);
-      hi[row + (long long)gc * ldw] = h;
-      lo[row + (long long)gc * ldw] = __float2half_rn((float)((v - (double)__half2float(h)) * 2048.0));
-    }
-  }
-}
-
-// Same recurrence with the growing 32-wide column panel of W kept in global
-// memory (FP64, column-major, ldg) instead of shared memory: each W block is
-// staged through a 32 x 32 shared tile when it is used, so a CTA needs ~27 KB
-// of shared memory and several CTAs share an SM (the shared-memory panel
-// allows one), letting all panels of all leaves run concurrently.
 template <class T>
 __device__ __forceinline__ void trtri_panel_body(const T* __restrict__ A, long long lda, int s, int size,
                                                  const double* __restrict__ D, __half* __restrict__ hi,
@@ -323,7 +222,7 @@ __global__ void __launch_bounds__(kChainThreads) trtri_chain_f64_kernel(const do
 // Grouped form: one job per (instance, leaf) along blockIdx.y.
 __global__ void __launch_bounds__(kChainThreads) trtri_chain_grouped_kernel(const ChainJob* __restrict__ jobs) {
   const ChainJob& jb = jobs[blockIdx.y];
-  trtri_chain_body<float>(jb.A, jb.lda, jb.s, jb.size, jb.D, jb.Whi, jb.Wlo, nullptr, jb.ldw, blockIdx.x);
+  trtri_panel_body<float>(jb.A, jb.lda, jb.s, jb.size, jb.D, jb.Whi, jb.Wlo, jb.Wg, jb.ldw, jb.ldw, blockIdx.x);
 }
 
 
@@ -447,11 +346,7 @@ tb_status recurse(TrsmCtx& c, long s, long e, const std::vector<long>& leaf_star
 
 }  // namespace
 
-tb_status trsm_prepare_grouped() {
-  TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(kLeafMax / 32 * 1024 * sizeof(double))));
-  return TB_SUCCESS;
-}
+tb_status trsm_prepare_grouped() { return TB_SUCCESS; }
 
 // Diagonal-block inverses of many triangular matrices in two launches.
 tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblocks, const ChainJob* d_chain,
@@ -462,16 +357,7 @@ tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblo
     note_launch();
   }
   if (nchain > 0) {
-    static bool attr_done[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 64 && !attr_done[dev]) {
-      TB_CUDA_TRY(cudaFuncSetAttribute(trtri_chain_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(kLeafMax / 32 * 1024 * sizeof(double))));
-      attr_done[dev] = true;
-    }
-    const size_t smem = (size_t)(kLeafMax / 32) * 1024 * sizeof(double);
-    trtri_chain_grouped_kernel<<<dim3(kLeafMax / 32, (unsigned)nchain), kChainThreads, smem, st>>>(d_chain);
+    trtri_chain_grouped_kernel<<<dim3(kLeafMax / 32, (unsigned)nchain), kChainThreads, 0, st>>>(d_chain);
     TB_CUDA_TRY(cudaGetLastError());
     note_launch();
   }
