@@ -87,7 +87,10 @@ tb_status trmm_ex_impl(bool right, bool upper, bool trans, bool unit, long m, lo
   __half* bh = reinterpret_cast<__half*>(buf + abytes);
   __half* al = hilo ? reinterpret_cast<__half*>(buf + abytes + bbytes) : nullptr;
   __half* bl = hilo ? reinterpret_cast<__half*>(buf + 2 * abytes + bbytes) : nullptr;
-  TB_TRY(convert_f32_f16(na, na, A, lda, ah, al, lda_h, 2048.f, upper ? 3 : 1, st));
+  // left, op(A) = A: the tiles read A's triangle plus a band next to the
+  // diagonal only, so only that is converted
+  const int tri = (!right && !trans) ? (upper ? 4 : 5) : (upper ? 3 : 1);
+  TB_TRY(convert_f32_f16(na, na, A, lda, ah, al, lda_h, 2048.f, tri, st));
   if (unit) TB_TRY(set_unit_diag(na, ah, al, lda_h, st));
   TB_TRY(convert_f32_f16(m, n, B, ldb, bh, bl, ldb_h, 2048.f, 0, st));
   const bool op_lower = upper == trans;  // op(A) lower triangular

@@ -24,24 +24,31 @@ __device__ __forceinline__ uint32_t pack2(__half a, __half b) {
   return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
 }
 
+// Band of the triangle modes 4 / 5: a GEMM tile of at most 256 rows whose K
+// range starts (upper) or ends (lower) at its own diagonal block reads the
+// other triangle only within 256 of the diagonal.
+constexpr long long kTriBand = 256;
+
 // Vector path: rows % 8 == 0, lds % 4 == 0, ldd % 8 == 0, 16-byte aligned bases.
 __global__ void __launch_bounds__(256) convert8_kernel(long long rows, long long cols, const float* __restrict__ src,
                                                        long long lds, __half* __restrict__ hi, __half* __restrict__ lo,
                                                        long long ldd, float lo_scale, int tri) {
   const long long rows8 = rows >> 3;
   for (long long j = blockIdx.y; j < cols; j += gridDim.y) {
-    long long v0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long v0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, vend = rows8;
     if (tri == 2) v0 += (j >> 3);  // rows i >= j (rounded down to 8)
-    for (long long v = v0; v < rows8; v += (long long)gridDim.x * blockDim.x) {
+    if (tri == 4) vend = min(rows8, (j / kTriBand + 1) * (kTriBand / 8));  // rows i < band end
+    if (tri == 5) v0 += (j / kTriBand) * (kTriBand / 8);                   // rows i >= band start
+    for (long long v = v0; v < vend; v += (long long)gridDim.x * blockDim.x) {
       const long long i = v << 3;
       const float* s = src + i + j * lds;
       const float4 a = ld_stream(s), b = ld_stream(s + 4);
       float f[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-      if (tri == 1) {
+      if (tri == 1 || tri == 5) {
 #pragma unroll
         for (int e = 0; e < 8; ++e)
           if (i + e < j) f[e] = 0.f;
-      } else if (tri == 3) {
+      } else if (tri == 3 || tri == 4) {
 #pragma unroll
         for (int e = 0; e < 8; ++e)
           if (i + e > j) f[e] = 0.f;
@@ -75,11 +82,13 @@ __global__ void __launch_bounds__(256) convert1_kernel(long long rows, long long
                                                        long long lds, __half* __restrict__ hi, __half* __restrict__ lo,
                                                        long long ldd, float lo_scale, int tri) {
   for (long long j = blockIdx.y; j < cols; j += gridDim.y) {
-    long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, iend = rows;
     if (tri == 2) i0 += (j >> 3) << 3;
-    for (long long i = i0; i < rows; i += (long long)gridDim.x * blockDim.x) {
+    if (tri == 4) iend = min(rows, (j / kTriBand + 1) * kTriBand);
+    if (tri == 5) i0 += (j / kTriBand) * kTriBand;
+    for (long long i = i0; i < iend; i += (long long)gridDim.x * blockDim.x) {
       float f = src[i + j * lds];
-      if ((tri == 1 && i < j) || (tri == 3 && i > j)) f = 0.f;
+      if (((tri == 1 || tri == 5) && i < j) || ((tri == 3 || tri == 4) && i > j)) f = 0.f;
       const __half h = __float2half_rn(f);
       hi[i + j * ldd] = h;
       if (lo) lo[i + j * ldd] = __float2half_rn((f - __half2float(h)) * lo_scale);

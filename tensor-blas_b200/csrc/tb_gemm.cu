@@ -3,6 +3,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <queue>
+#include <vector>
 #include <map>
 #include <mutex>
 #include <string>
@@ -196,6 +199,7 @@ tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
   }
   a.tiles = c.tiles;
   a.num_tiles = c.num_tiles;
+  a.ranges = c.ranges;
   a.a_off = c.a_off;
   a.b_off = c.b_off;
   a.k_off = c.k_off;
@@ -279,36 +283,87 @@ bool pair_engine_enabled() {
   return on == 1;
 }
 
+// Static assignment for a tile list whose K ranges differ (TRMM, TRSM leaf
+// products): the host simulates `workers` CTAs (or CTA pairs) claiming the
+// tiles in list order as they free up, with a tile's cost its K-blocks plus
+// a fixed epilogue share, and regroups the list by worker; the returned
+// list is the tiles followed by the workers + 1 range bounds (packed into
+// int4s). Lists with uniform K ranges are returned unchanged (striding is
+// balanced for them). Claiming in list order keeps the tiles in flight at
+// any moment close together in the list, as the plans' L2-friendly order
+// intends, while no worker ends more than about one tile after the others.
+static std::vector<int4> balance_tiles(const std::vector<int4>& tiles, int workers, bool* balanced) {
+  *balanced = false;
+  if (tiles.size() <= (size_t)workers || workers <= 1) return tiles;
+  int kmin = 1 << 30, kmax = 0;
+  for (const int4& t : tiles) {
+    kmin = std::min(kmin, t.w - t.z);
+    kmax = std::max(kmax, t.w - t.z);
+  }
+  if (kmin == kmax) return tiles;
+  constexpr long long kEpilogueKb = 4;
+  std::vector<std::vector<int>> own(workers);
+  std::priority_queue<std::pair<long long, int>, std::vector<std::pair<long long, int>>, std::greater<>> q;
+  for (int w = 0; w < workers; ++w) q.push({0, w});
+  for (size_t i = 0; i < tiles.size(); ++i) {
+    auto [tw, w] = q.top();
+    q.pop();
+    own[w].push_back((int)i);
+    q.push({tw + (tiles[i].w - tiles[i].z) + kEpilogueKb, w});
+  }
+  std::vector<int4> out;
+  out.reserve(tiles.size() + (workers + 4) / 4);
+  std::vector<int> bounds(1, 0);
+  for (int w = 0; w < workers; ++w) {
+    for (int i : own[w]) out.push_back(tiles[i]);
+    bounds.push_back((int)out.size());
+  }
+  while (bounds.size() % 4) bounds.push_back((int)out.size());
+  for (size_t i = 0; i < bounds.size(); i += 4) out.push_back(make_int4(bounds[i], bounds[i + 1], bounds[i + 2], bounds[i + 3]));
+  *balanced = true;
+  return out;
+}
+
+// Uploads a (possibly balanced) list and points the call at it.
+static tb_status set_tiles(GemmCall& c, const std::vector<int4>& tiles, int workers, cudaStream_t stream) {
+  bool balanced = false;
+  const std::vector<int4> list = balance_tiles(tiles, workers, &balanced);
+  const int4* d = upload_tiles(list, stream);
+  if (!d) return TB_ERROR_ALLOC;
+  c.tiles = d;
+  c.num_tiles = (int)tiles.size();
+  c.ranges = balanced ? reinterpret_cast<const int*>(d + tiles.size()) : nullptr;
+  return TB_SUCCESS;
+}
+
 tb_status gemm_launch_plan(GemmCall& c, const std::vector<int4>& plan, cudaStream_t stream) {
   const bool pf = c.kblocks > 0 && c.kblocks <= kGemmPfMaxKb;
   c.pair = !c.fp8 && c.split == Split::kPlain && !pf && c.M >= 512 && c.N >= 512 && pair_engine_enabled();
   if (!c.pair) {
-    c.tiles = upload_tiles(plan, stream);
-    if (!c.tiles) return TB_ERROR_ALLOC;
-    c.num_tiles = (int)plan.size();
+    TB_TRY(set_tiles(c, plan, std::min<int>((int)plan.size(), sm_count()), stream));
     return gemm_launch(c, stream);
   }
   // merge vertically adjacent 128-row tiles into 256-row pair tiles (the K
   // range of a pair tile spans both halves; products outside an operand's
   // support multiply stored zeros, and masked outputs are never written)
+  // (a flat index over (256-row block, 128-column block): plans have
+  // thousands of tiles and this runs on every call)
   std::vector<int4> merged;
-  std::map<std::pair<int, int>, size_t> where;
   merged.reserve(plan.size());
+  const long long rb = ((long long)c.M + 255) / 256, cb = ((long long)c.N + 127) / 128;
+  std::vector<int> where((size_t)(rb * cb), -1);
   for (const int4& t : plan) {
-    const std::pair<int, int> key((t.x >> 8) << 8, t.y);
-    auto it = where.find(key);
-    if (it == where.end()) {
-      where.emplace(key, merged.size());
-      merged.push_back(make_int4(key.first, key.second, t.z, t.w));
+    int& w = where[(size_t)((long long)(t.x >> 8) * cb + (t.y >> 7))];
+    if (w < 0) {
+      w = (int)merged.size();
+      merged.push_back(make_int4((t.x >> 8) << 8, t.y, t.z, t.w));
     } else {
-      int4& m = merged[it->second];
+      int4& m = merged[w];
       m.z = t.z < m.z ? t.z : m.z;
       m.w = t.w > m.w ? t.w : m.w;
     }
   }
-  c.tiles = upload_tiles(merged, stream);
-  if (!c.tiles) return TB_ERROR_ALLOC;
-  c.num_tiles = (int)merged.size();
+  TB_TRY(set_tiles(c, merged, std::min<int>((int)merged.size(), sm_count() / 2), stream));
   return gemm_launch(c, stream);
 }
 
@@ -390,22 +445,32 @@ std::vector<int4> plan_upper(int n, int bn, int kb0, int kb1) {
 // Device copies of tile plans, cached by content (per device). Plans are
 // small (16 B per tile) and reused across calls of the same shape.
 const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream) {
+  // Cached by content: a 64-bit FNV-1a hash selects the candidates, a full
+  // comparison confirms.
+  struct Entry {
+    std::vector<int4> tiles;
+    int4* d;
+  };
   static std::mutex mu;
-  static std::map<std::pair<int, std::string>, int4*> cache;
+  static std::map<std::pair<int, uint64_t>, std::vector<Entry>> cache;
   int dev = 0;
   cudaGetDevice(&dev);
-  std::string key(reinterpret_cast<const char*>(tiles.data()), tiles.size() * sizeof(int4));
+  const size_t bytes = tiles.size() * sizeof(int4);
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)bytes;
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(tiles.data());
+  for (size_t i = 0; i < bytes / 4; ++i) h = (h ^ w[i]) * 1099511628211ull;
   std::lock_guard<std::mutex> lk(mu);
-  auto it = cache.find({dev, key});
-  if (it != cache.end()) return it->second;
+  std::vector<Entry>& bucket = cache[{dev, h}];
+  for (const Entry& e : bucket)
+    if (e.tiles.size() == tiles.size() && memcmp(e.tiles.data(), tiles.data(), bytes) == 0) return e.d;
   int4* d = nullptr;
-  if (cudaMalloc(&d, tiles.size() * sizeof(int4)) != cudaSuccess) return nullptr;
-  if (cudaMemcpy(d, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, tiles.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaFree(d);
     return nullptr;
   }
   (void)stream;
-  cache[{dev, key}] = d;
+  bucket.push_back(Entry{tiles, d});
   return d;
 }
 

@@ -83,11 +83,25 @@ struct GemmArgs {
   // GemmArgs (64-byte aligned; their tensor maps are read from global memory).
   const struct GemmArgs* problems;
   const int* tile_prob;
-  // Device-side tile scheduler: nullptr = static striding (CTA b takes tiles
-  // b, b + grid, ...); otherwise a zeroed counter from which the CTAs'
-  // producers claim tiles one at a time.
+  // Device-side tile scheduler: nullptr = static assignment; otherwise a
+  // zeroed counter from which the CTAs' producers claim tiles one at a time.
   int* sched;
+  // Static assignment: nullptr = striding (CTA b takes tiles b, b + grid,
+  // ...); otherwise CTA (or CTA pair) b takes tiles [ranges[b], ranges[b+1])
+  // of a list the host balanced by simulating greedy claiming.
+  const int* ranges;
 };
+
+// First / next tile of CTA (or CTA pair) `b` of `nb` under the static
+// assignment; -1 when there is none.
+__device__ __forceinline__ int static_first(const GemmArgs& a, int b) {
+  if (a.ranges) return a.ranges[b] < a.ranges[b + 1] ? a.ranges[b] : -1;
+  return b < a.num_tiles ? b : -1;
+}
+__device__ __forceinline__ int static_next(const GemmArgs& a, int b, int nb, int t) {
+  if (a.ranges) return t + 1 < a.ranges[b + 1] ? t + 1 : -1;
+  return t + nb < a.num_tiles ? t + nb : -1;
+}
 
 // Tile hand-off inside a CTA under the device-side scheduler: the producer
 // claims a tile and queues its index (or -1, the end) in a kTileQ-deep ring;
@@ -102,10 +116,7 @@ template <bool EPI>
 __device__ __forceinline__ int next_tile(const GemmArgs& args, int t, const volatile int* tq_idx, uint64_t* tq_full,
                                          uint64_t* tq_empty, int& q, uint32_t& ph, volatile int* abort_flag,
                                          int code) {
-  if (!args.sched) {
-    const int n = t < 0 ? (int)blockIdx.x : t + (int)gridDim.x;
-    return n < args.num_tiles ? n : -1;
-  }
+  if (!args.sched) return t < 0 ? static_first(args, blockIdx.x) : static_next(args, blockIdx.x, gridDim.x, t);
   const bool got = mbar_wait(&tq_full[q], ph, abort_flag, args.err, code);
   int v = got ? tq_idx[q] : -1;
   if constexpr (EPI) {
@@ -505,7 +516,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
       const bool dyn = args.sched != nullptr;
       int tq = 0;
       uint32_t tq_ph = 0;
-      int t = dyn ? atomicAdd(args.sched, 1) : (int)blockIdx.x;
+      int t = dyn ? atomicAdd(args.sched, 1) : static_first(args, blockIdx.x);
       while (ok) {
         if (t >= args.num_tiles) t = -1;
         if (dyn) {
@@ -522,7 +533,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
           }
         }
         if (t < 0) break;
-        const int t_next = dyn ? atomicAdd(args.sched, 1) : t + (int)gridDim.x;  // claimed early: its latency hides
+        // the next claim is issued early so its latency hides
+        const int t_next = dyn ? atomicAdd(args.sched, 1) : static_next(args, blockIdx.x, gridDim.x, t);
         const int4 tile = args.tiles[t];
         for (int kb = tile.z; kb < tile.w; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
@@ -990,7 +1002,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       uint32_t ph = 0;
       uint32_t issued_mask = 0, phase_mask = 0;
       bool ok = true;
-      for (int t = pair; t < args.num_tiles && ok; t += npairs) {
+      for (int t = static_first(args, pair); t >= 0 && ok; t = static_next(args, pair, npairs, t)) {
         const int4 tile = args.tiles[t];
         for (int kb = tile.z; kb < tile.w; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
@@ -1037,7 +1049,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       uint32_t ph = 0;
       int it = 0;
       bool ok = true, any = false;
-      for (int t = pair; t < args.num_tiles && ok; t += npairs, ++it) {
+      for (int t = static_first(args, pair); t >= 0 && ok; t = static_next(args, pair, npairs, t), ++it) {
         const int4 tile = args.tiles[t];
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -1088,7 +1100,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     const bool issuer = (warp == 2 && lane == 0);
     EpiState es{0, 0u, false};
     int it = 0;
-    for (int t = pair; t < args.num_tiles; t += npairs, ++it) {
+    for (int t = static_first(args, pair); t >= 0; t = static_next(args, pair, npairs, t), ++it) {
       const int4 tile = args.tiles[t];
       const int m0 = tile.x + 128 * (int)rank;
       const long long gi = (long long)m0 + row;

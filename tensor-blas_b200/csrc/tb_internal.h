@@ -81,6 +81,7 @@ struct GemmCall {
   float out_lo_scale = 2048.0f;
   int out_m = -1, out_n = -1;  // side-copy region (default: all of C)
   int kblocks = 0;   // most K-blocks (64) of any tile; 0 < kblocks <= kGemmPfMaxKb selects the prefetch variants
+  const int* ranges = nullptr;  // per-CTA tile ranges of a balanced list (set by gemm_launch_plan)
   // FP8 (e4m3) operands: K-major byte matrices (Operand.ld in bytes), K
   // blocks of 128, per-(128-row block, K block) scales (row-block-major,
   // scale_ld K blocks per row block); tiles 128 x 128.
@@ -130,7 +131,13 @@ const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
 // orientation (ldd). lo = fp16((x - hi) * lo_scale).
 //   tri == 0: whole matrix; tri == 1: zero the strict upper triangle;
 //   tri == 2: only rows i >= j (rounded down to 8) are written;
-//   tri == 3: zero the strict lower triangle.
+//   tri == 3: zero the strict lower triangle;
+//   tri == 4: upper triangle, and zeros below the diagonal only in the rows
+//             [j, (j / 256 + 1) * 256) of column j (nothing else is written);
+//   tri == 5: lower triangle, and zeros above the diagonal only in the rows
+//             [(j / 256) * 256, j) of column j (nothing else is written).
+// Modes 4 / 5 serve products whose tiles (at most 256 rows, row-aligned to
+// their height) take the K range from / up to their own diagonal block.
 tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
                           long long ldd, float lo_scale, int tri, cudaStream_t stream);
 // Unit diagonal in an FP16 copy (hi = 1, lo = 0) for diag = 'U' operands.

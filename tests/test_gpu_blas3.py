@@ -49,7 +49,8 @@ def test_ssyr2k(tblas, n, k, beta, wide, precision):
 
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("uplo", ["L", "U"])
-@pytest.mark.parametrize("m,n,wide", [(512, 384, False), (333, 200, False), (768, 256, True)])
+# (1100, 600): CTA-pair tiles with host-balanced ranges and a ragged last 256-band
+@pytest.mark.parametrize("m,n,wide", [(512, 384, False), (333, 200, False), (768, 256, True), (1100, 600, False)])
 def test_strmm(tblas, uplo, m, n, wide, precision):
     g = _rng(3 * m + n)
     A = _wide(g, (m, m)) if wide else g.uniform(-1, 1, (m, m)).astype(np.float32)
