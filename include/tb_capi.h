@@ -83,6 +83,30 @@ TB_API tb_status tb_ssyrk(char uplo, char trans, long n, long k, float alpha, co
                           float* C, long ldc, long nb, int precision);
 
 /*
+ * nb = TB_NB_AUTO in tb_ssyrk, tb_strsm, tb_ssyr2k and tb_strmm: the
+ * library's autotuner picks nb (the TRSM leaf size: 128, 256 or 512) and the
+ * GEMM engine (256 x 256 tiles on CTA pairs, or single-CTA tiles) for this
+ * (routine, flags, sizes, precision). The first call with a new key times
+ * each candidate once on zero-filled scratch outputs of the same shape, on
+ * the library's current stream, and caches the fastest per device; the call
+ * then runs with it. The cache lives in memory and, when a file is set
+ * (tb_autotune_set_file, or TB_AUTOTUNE_CACHE in the environment), is loaded
+ * from that file and rewritten to it (temporary file + rename) on every new
+ * entry. Keys carry the device name, compute capability and driver version.
+ */
+#define TB_NB_AUTO (-1L)
+TB_API tb_status tb_autotune_set_file(const char* path); /* NULL: memory only */
+TB_API tb_status tb_autotune_clear(void);                /* forget every entry (the file is kept) */
+TB_API int tb_autotune_entries(void);
+/* routine: "ssyrk" (flags uplo+trans, a = n, b = k), "strsm" (flags side,
+ * a = m, b = n), "ssyr2k" (uplo+trans, n, k), "strmm" (uplo, m, n).
+ * tb_autotune_get returns TB_ERROR_NOT_SUPPORTED when there is no entry. */
+TB_API tb_status tb_autotune_put(const char* routine, const char* flags, long a, long b, int precision, long nb,
+                                 int engine, double ms);
+TB_API tb_status tb_autotune_get(const char* routine, const char* flags, long a, long b, int precision, long* nb,
+                                 int* engine);
+
+/*
  * TRSM with a lower-triangular, non-unit A, B overwritten by X:
  *   side 'R': X * A^T = B,  A n x n, B m x n  (the reference's tc_trsm:
  *             BLAS/tc_trsm.cu:139-174, right/lower/transpose/non-unit)

@@ -45,9 +45,10 @@ tb_status syr2k_impl(long n, long k, float alpha, const float* A, long lda, cons
   __half* hi = reinterpret_cast<__half*>(buf);
   __half* lo = hilo ? reinterpret_cast<__half*>(buf + one) : nullptr;
   const long long blk = ldh * k;  // elements per column block
-  TB_TRY(convert_f32_f16(n, k, A, lda, hi, lo, ldh, 2048.f, 0, st));
+  // column blocks [A | B | A]: the A-operand is [A | B], the B-operand [B | A];
+  // A is read once for both of its copies
+  TB_TRY(convert_f32_f16(n, k, A, lda, hi, lo, ldh, 2048.f, 0, st, 2 * blk));
   TB_TRY(convert_f32_f16(n, k, B, ldb, hi + blk, lo ? lo + blk : nullptr, ldh, 2048.f, 0, st));
-  TB_TRY(convert_f32_f16(n, k, A, lda, hi + 2 * blk, lo ? lo + 2 * blk : nullptr, ldh, 2048.f, 0, st));
   GemmCall c;
   c.split = split;
   c.a_hi = {hi, n, 2 * k, ldh, true};
@@ -190,6 +191,7 @@ static tb::Split to_split(int p) { return p == TB_PREC_SPLIT ? tb::Split::kHiLo 
 
 extern "C" tb_status tb_ssyr2k(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
                                const float* B, long ldb, float beta, float* C, long ldc, long nb, int precision) {
+  if (nb == TB_NB_AUTO) return tb::auto_ssyr2k(uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C, ldc, precision);
   if (uplo != 'L' && uplo != 'l') {
     tb::set_last_error("tb_ssyr2k: only uplo='L' is supported");
     return TB_ERROR_NOT_SUPPORTED;
@@ -212,6 +214,7 @@ extern "C" tb_status tb_ssyr2k(char uplo, char trans, long n, long k, float alph
 
 extern "C" tb_status tb_strmm(char uplo, long m, long n, float alpha, const float* A, long lda, const float* B,
                               long ldb, float* C, long ldc, long nb, int precision) {
+  if (nb == TB_NB_AUTO) return tb::auto_strmm(uplo, m, n, alpha, A, lda, B, ldb, C, ldc, precision);
   bool upper;
   if (uplo == 'L' || uplo == 'l')
     upper = false;

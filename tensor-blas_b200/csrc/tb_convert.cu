@@ -32,7 +32,7 @@ constexpr long long kTriBand = 256;
 // Vector path: rows % 8 == 0, lds % 4 == 0, ldd % 8 == 0, 16-byte aligned bases.
 __global__ void __launch_bounds__(256) convert8_kernel(long long rows, long long cols, const float* __restrict__ src,
                                                        long long lds, __half* __restrict__ hi, __half* __restrict__ lo,
-                                                       long long ldd, float lo_scale, int tri) {
+                                                       long long ldd, float lo_scale, int tri, long long dup) {
   const long long rows8 = rows >> 3;
   for (long long j = blockIdx.y; j < cols; j += gridDim.y) {
     long long v0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, vend = rows8;
@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(256) convert8_kernel(long long rows, long long
       o.z = pack2(h[4], h[5]);
       o.w = pack2(h[6], h[7]);
       *reinterpret_cast<uint4*>(hi + i + j * ldd) = o;
+      if (dup) *reinterpret_cast<uint4*>(hi + dup + i + j * ldd) = o;
       if (lo) {
         __half l[8];
 #pragma unroll
@@ -72,6 +73,7 @@ __global__ void __launch_bounds__(256) convert8_kernel(long long rows, long long
         q.z = pack2(l[4], l[5]);
         q.w = pack2(l[6], l[7]);
         *reinterpret_cast<uint4*>(lo + i + j * ldd) = q;
+        if (dup) *reinterpret_cast<uint4*>(lo + dup + i + j * ldd) = q;
       }
     }
   }
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(256) convert8_kernel(long long rows, long long
 // Scalar fallback for ragged or unaligned shapes.
 __global__ void __launch_bounds__(256) convert1_kernel(long long rows, long long cols, const float* __restrict__ src,
                                                        long long lds, __half* __restrict__ hi, __half* __restrict__ lo,
-                                                       long long ldd, float lo_scale, int tri) {
+                                                       long long ldd, float lo_scale, int tri, long long dup) {
   for (long long j = blockIdx.y; j < cols; j += gridDim.y) {
     long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, iend = rows;
     if (tri == 2) i0 += (j >> 3) << 3;
@@ -91,7 +93,12 @@ __global__ void __launch_bounds__(256) convert1_kernel(long long rows, long long
       if (((tri == 1 || tri == 5) && i < j) || ((tri == 3 || tri == 4) && i > j)) f = 0.f;
       const __half h = __float2half_rn(f);
       hi[i + j * ldd] = h;
-      if (lo) lo[i + j * ldd] = __float2half_rn((f - __half2float(h)) * lo_scale);
+      if (dup) hi[dup + i + j * ldd] = h;
+      if (lo) {
+        const __half l = __float2half_rn((f - __half2float(h)) * lo_scale);
+        lo[i + j * ldd] = l;
+        if (dup) lo[dup + i + j * ldd] = l;
+      }
     }
   }
 }
@@ -140,7 +147,7 @@ tb_status convert_sym_f32_f16(long long n, const float* A, long long lda, bool l
 }
 
 tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
-                          long long ldd, float lo_scale, int tri, cudaStream_t stream) {
+                          long long ldd, float lo_scale, int tri, cudaStream_t stream, long long dup) {
   if (rows <= 0 || cols <= 0) return TB_SUCCESS;
   const bool vec = (rows % 8 == 0) && (lds % 4 == 0) && (ldd % 8 == 0) &&
                    (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(hi) % 16 == 0) &&
@@ -152,9 +159,9 @@ tb_status convert_f32_f16(long long rows, long long cols, const float* src, long
   long long gy = cols < 65535 ? cols : 65535;
   dim3 grid((unsigned)gx, (unsigned)gy);
   if (vec)
-    convert8_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri);
+    convert8_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri, dup);
   else
-    convert1_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri);
+    convert1_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri, dup);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   return TB_SUCCESS;

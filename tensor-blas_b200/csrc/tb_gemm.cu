@@ -273,8 +273,14 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
 }
 
 // Large plain launches run on CTA pairs; TB_GEMM_PAIR=0 in the environment
-// keeps them on single CTAs (read once; for comparing the two engines).
+// keeps them on single CTAs (read once; for comparing the two engines). The
+// autotuner overrides the choice per thread.
+static thread_local int t_engine_override = -1;
+void set_engine_override(int engine) { t_engine_override = engine; }
+int engine_override() { return t_engine_override; }
+
 bool pair_engine_enabled() {
+  if (t_engine_override >= 0) return t_engine_override == 1;
   static int on = -1;
   if (on < 0) {
     const char* e = getenv("TB_GEMM_PAIR");

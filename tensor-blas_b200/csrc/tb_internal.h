@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
+#include <string>
 #include <vector>
 
 #include "../../include/tb_capi.h"
@@ -105,6 +107,15 @@ int gemm_bn(Split s);
 int gemm_bn(Split s, int kblocks);
 
 tb_status gemm_launch(const GemmCall& call, cudaStream_t stream);
+// GEMM engine for the large plain launches of this thread: -1 the default
+// (CTA pairs unless TB_GEMM_PAIR=0), 0 single-CTA tiles, 1 CTA pairs.
+void set_engine_override(int engine);
+int engine_override();
+struct EngineScope {
+  int saved;
+  explicit EngineScope(int engine) : saved(engine_override()) { set_engine_override(engine); }
+  ~EngineScope() { set_engine_override(saved); }
+};
 // Uploads `plan` (128-row tiles) and launches; plain launches that are large
 // enough run on CTA pairs, with the plan merged into 256-row tiles.
 tb_status gemm_launch_plan(GemmCall& call, const std::vector<int4>& plan, cudaStream_t stream);
@@ -138,8 +149,10 @@ const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
 //             [(j / 256) * 256, j) of column j (nothing else is written).
 // Modes 4 / 5 serve products whose tiles (at most 256 rows, row-aligned to
 // their height) take the K range from / up to their own diagonal block.
+// dup != 0: the same values are also written `dup` elements further on (hi
+// and lo alike), from one read of src.
 tb_status convert_f32_f16(long long rows, long long cols, const float* src, long long lds, __half* hi, __half* lo,
-                          long long ldd, float lo_scale, int tri, cudaStream_t stream);
+                          long long ldd, float lo_scale, int tri, cudaStream_t stream, long long dup = 0);
 // Unit diagonal in an FP16 copy (hi = 1, lo = 0) for diag = 'U' operands.
 tb_status set_unit_diag(long long n, __half* hi, __half* lo, long long ld, cudaStream_t stream);
 // ------------------------------------------------------------------ grouped TRSM pieces
@@ -218,6 +231,27 @@ tb_status symm_fp8(bool lower, long m, long n, float alpha, const float* A, long
                    float beta, float* C, long ldc, cudaStream_t st);
 tb_status gemm_fp8(bool ta, bool tb_, long m, long n, long k, float alpha, const float* A, long lda, const float* B,
                    long ldb, float beta, float* C, long ldc, cudaStream_t st);
+
+// ------------------------------------------------------------------ autotuner (tb_tune.cu)
+struct TuneChoice {
+  long nb;
+  int engine;  // 0 single-CTA tiles, 1 CTA pairs
+  double ms;
+};
+std::string tune_key(const char* routine, const char* flags, long a, long b, int precision);
+// The cached choice for `key`, or the fastest of `candidates` under `trial`
+// (run once to warm up, then timed twice with CUDA events on `st`).
+tb_status autotune(const std::string& key, const std::vector<TuneChoice>& candidates,
+                   const std::function<tb_status(const TuneChoice&)>& trial, cudaStream_t st, TuneChoice* out);
+
+// nb = TB_NB_AUTO forms of the public entry points (tuned, then run).
+tb_status auto_ssyrk(char uplo, char trans, long n, long k, float alpha, const float* A, long lda, float beta,
+                     float* C, long ldc, int precision);
+tb_status auto_strsm(char side, long m, long n, const float* A, long lda, float* B, long ldb, int precision);
+tb_status auto_ssyr2k(char uplo, char trans, long n, long k, float alpha, const float* A, long lda, const float* B,
+                      long ldb, float beta, float* C, long ldc, int precision);
+tb_status auto_strmm(char uplo, long m, long n, float alpha, const float* A, long lda, const float* B, long ldb,
+                     float* C, long ldc, int precision);
 
 // C(lower) (or C(upper)) *= beta (C = 0 when beta == 0).
 tb_status scale_lower(long long n, float beta, float* C, long long ldc, cudaStream_t st, bool upper = false);

@@ -90,6 +90,7 @@ tb_status syrk_impl(bool trans, long n, long k, float alpha, const float* A, lon
 
 extern "C" tb_status tb_ssyrk(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
                               float beta, float* C, long ldc, long nb, int precision) {
+  if (nb == TB_NB_AUTO) return tb::auto_ssyrk(uplo, trans, n, k, alpha, A, lda, beta, C, ldc, precision);
   const bool upper = (uplo == 'U' || uplo == 'u');
   if (!upper && uplo != 'L' && uplo != 'l') return TB_ERROR_INVALID_VALUE;
   const bool t = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');

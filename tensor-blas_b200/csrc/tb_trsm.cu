@@ -668,6 +668,7 @@ tb_status trsm_ex_impl(bool right, bool upper, bool trans, bool unit, long m, lo
 
 extern "C" tb_status tb_strsm(char side, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
                               int precision) {
+  if (nb == TB_NB_AUTO) return tb::auto_strsm(side, m, n, A, lda, B, ldb, precision);
   bool right;
   if (side == 'R' || side == 'r')
     right = true;

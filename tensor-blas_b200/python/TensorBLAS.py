@@ -25,6 +25,7 @@ PLAIN = 0  # FP16 operands, FP32 accumulation (reference tc_*)
 SPLIT = 1  # FP16 hi + scaled-lo, 3 products, FP32-level accuracy
 FP8 = 2    # e4m3 scaled per 128x128 block (SYRK/SYR2K/TRMM/SYMM/GEMM), ~1e-2 accuracy
 REFINE = 3  # TRSM: plain solve + one refinement sweep, FP32-level accuracy
+NB_AUTO = -1  # nb for ssyrk / strsm / ssyr2k / strmm: the library's autotuner picks nb and the GEMM engine
 
 _c_long = ctypes.c_long
 _fp = ctypes.c_void_p
@@ -68,6 +69,18 @@ lib.tb_strsm.restype = ctypes.c_int
 lib.tb_ssyrk_host.argtypes = lib.tb_ssyrk.argtypes
 lib.tb_ssyrk_host.restype = ctypes.c_int
 lib.tb_strsm_host.argtypes = lib.tb_strsm.argtypes
+lib.tb_autotune_set_file.argtypes = [ctypes.c_char_p]
+lib.tb_autotune_set_file.restype = ctypes.c_int
+lib.tb_autotune_clear.argtypes = []
+lib.tb_autotune_clear.restype = ctypes.c_int
+lib.tb_autotune_entries.argtypes = []
+lib.tb_autotune_entries.restype = ctypes.c_int
+lib.tb_autotune_put.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _c_long, _c_long, ctypes.c_int, _c_long, ctypes.c_int,
+                                ctypes.c_double]
+lib.tb_autotune_put.restype = ctypes.c_int
+lib.tb_autotune_get.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _c_long, _c_long, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]
+lib.tb_autotune_get.restype = ctypes.c_int
 lib.tb_strsm_host.restype = ctypes.c_int
 
 
@@ -139,6 +152,23 @@ def ssyrk(A_cm, C_cm, n, k, lda, ldc, alpha=1.0, beta=0.0, trans="N", nb=256, pr
 def strsm(side, A_cm, B_cm, m, n, lda, ldb, nb=512, precision=PLAIN):
     """Raw column-major STRSM (lower, non-unit); side 'R': X A^T = B, 'L': A X = B."""
     _check(lib.tb_strsm(side.encode(), m, n, A_cm.data_ptr(), lda, B_cm.data_ptr(), ldb, nb, precision))
+
+
+def autotune_set_file(path):
+    """Keep the autotuner's cache in a JSON file (loaded now, rewritten on
+    every new entry); None keeps it in memory only."""
+    _check(lib.tb_autotune_set_file(path.encode() if path else None))
+
+
+def autotune_entries():
+    return lib.tb_autotune_entries()
+
+
+def autotune_get(routine, flags, a, b, precision=PLAIN):
+    """The cached (nb, engine) of a key, or None (see tb_autotune_get)."""
+    nb, eng = ctypes.c_long(), ctypes.c_int()
+    st = lib.tb_autotune_get(routine.encode(), flags.encode(), a, b, precision, ctypes.byref(nb), ctypes.byref(eng))
+    return (nb.value, eng.value) if st == 0 else None
 
 
 def _host_f32(t, name):

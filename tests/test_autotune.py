@@ -1,0 +1,46 @@
+"""Autotuner cache on the CPU: entries put through the C ABI land in a JSON
+file (a valid JSON document, rewritten through a temporary file), survive a
+clear + reload, and are looked up by (routine, flags, sizes, precision)."""
+import json
+import os
+
+import pytest
+
+import TensorBLAS as TB
+
+
+@pytest.fixture()
+def cache(tmp_path):
+    path = str(tmp_path / "tune.json")
+    TB.autotune_set_file(path)
+    TB.lib.tb_autotune_clear()
+    yield path
+    TB.lib.tb_autotune_clear()
+    TB.autotune_set_file(None)
+
+
+def test_put_get_file_roundtrip(cache):
+    assert TB.autotune_entries() == 0
+    TB._check(TB.lib.tb_autotune_put(b"strsm", b"L", 16384, 16384, TB.PLAIN, 256, 1, 6.1))
+    TB._check(TB.lib.tb_autotune_put(b"ssyrk", b"LN", 4096, 4096, TB.SPLIT, 256, 0, 0.4))
+    assert TB.autotune_entries() == 2
+    assert TB.autotune_get("strsm", "L", 16384, 16384, TB.PLAIN) == (256, 1)
+    assert TB.autotune_get("ssyrk", "LN", 4096, 4096, TB.SPLIT) == (256, 0)
+    assert TB.autotune_get("ssyrk", "LN", 4096, 4096, TB.PLAIN) is None  # precision is part of the key
+    doc = json.load(open(cache))
+    assert doc["format"] == "tensorblas-autotune-1"
+    assert len(doc["entries"]) == 2
+    keys = sorted(e["key"] for e in doc["entries"])
+    assert keys[0].split("|")[1:] == ["ssyrk", "LN", "4096", "4096", "1"]
+    assert not [f for f in os.listdir(os.path.dirname(cache)) if ".tmp." in f]
+    TB.lib.tb_autotune_clear()
+    assert TB.autotune_entries() == 0
+    TB.autotune_set_file(cache)  # reload
+    assert TB.autotune_entries() == 2
+    assert TB.autotune_get("strsm", "L", 16384, 16384, TB.PLAIN) == (256, 1)
+
+
+def test_put_rejects_bad_entries(cache):
+    assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 0, 1, 1.0) == 1   # nb <= 0
+    assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 128, 2, 1.0) == 1  # engine not 0 / 1
+    assert TB.autotune_entries() == 0
