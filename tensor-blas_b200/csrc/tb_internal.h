@@ -30,6 +30,9 @@ void set_last_error(const char* fmt, ...);
 
 // ------------------------------------------------------------------ streams / pool
 cudaStream_t current_stream();
+// A second (non-blocking) stream per device for work the library splits in
+// two; joined back into the caller's stream before a routine returns.
+cudaStream_t aux_stream();
 // Device scratch owned by the library (grow-only, per device and slot).
 // Slot 0 serves the routines' own scratch; slot 1 the host-memory entry
 // points' staging buffers, which live across routine calls. Returns nullptr
@@ -211,6 +214,12 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
                      void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit = false);
 size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split);
 tb_status trsm_solve(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
+// The same solve with B's independent dimension (columns for the left side,
+// rows for the right side) split in two halves solved on the context's
+// stream and the auxiliary stream, so the tail of each launch of one half
+// overlaps the other half's work; small problems and the split precision
+// solve in one piece (TB_TRSM_STREAMS=1 in the environment: always).
+tb_status trsm_solve_2s(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
 // One-time kernel attribute set-up for the grouped launches (not capturable).
 tb_status gemm_prepare_grouped();
 tb_status trsm_prepare_grouped();

@@ -22,6 +22,7 @@ struct DeviceState {
   size_t pool_bytes[kPoolSlots] = {0, 0};
   int* err = nullptr;
   int sms = 0;
+  cudaStream_t aux = nullptr;
 };
 DeviceState g_dev[kMaxDevices];
 std::mutex g_mu;
@@ -91,6 +92,17 @@ tb_status cuda_status(cudaError_t e) {
 }
 
 cudaStream_t current_stream() { return g_stream; }
+
+cudaStream_t aux_stream() {
+  DeviceState* s = state();
+  if (!s) return nullptr;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!s->aux && cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    s->aux = nullptr;
+  }
+  return s->aux;
+}
 
 int sm_count() {
   DeviceState* s = state();
