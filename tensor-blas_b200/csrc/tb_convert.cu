@@ -105,20 +105,24 @@ __global__ void __launch_bounds__(256) convert1_kernel(long long rows, long long
 
 // Full symmetric FP16 copy of an n x n matrix of which only one triangle is
 // stored: out(i, j) = A(i, j) on the stored side, A(j, i) on the other. Each
-// 32 x 32 output tile reads its own tile and the mirrored one through shared
-// memory, so every global read and write is coalesced (the reference instead
-// mirrors the caller's A in place with strided reads, BLAS/tc_symm.cu:7).
+// 32 x 32 output tile reads its own tile (stored side) or the mirrored one
+// (other side; both for diagonal tiles) through shared memory, so every
+// global read and write is coalesced and A is read about once (the
+// reference instead mirrors the caller's A in place with strided reads,
+// BLAS/tc_symm.cu:7).
 __global__ void __launch_bounds__(256) convert_sym_kernel(long long n, const float* __restrict__ A, long long lda,
                                                           int lower, __half* __restrict__ hi, __half* __restrict__ lo,
                                                           long long ldd, float lo_scale) {
   __shared__ float own[32][33], mir[32][33];
   const long long bi = blockIdx.x, bj = blockIdx.y;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  const bool need_own = lower ? bi >= bj : bi <= bj;  // the tile has elements on the stored side
+  const bool need_mir = lower ? bi <= bj : bi >= bj;  // ... and on the other side
   for (int r = ty; r < 32; r += 8) {
     const long long i = bi * 32 + tx, j = bj * 32 + r;  // own tile element (i, j)
-    own[r][tx] = (i < n && j < n) ? A[i + j * lda] : 0.f;
+    if (need_own) own[r][tx] = (i < n && j < n) ? A[i + j * lda] : 0.f;
     const long long mi = bj * 32 + tx, mj = bi * 32 + r;  // mirrored tile element (mi, mj)
-    mir[r][tx] = (mi < n && mj < n) ? A[mi + mj * lda] : 0.f;
+    if (need_mir) mir[r][tx] = (mi < n && mj < n) ? A[mi + mj * lda] : 0.f;
   }
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
