@@ -322,8 +322,10 @@ def run_mine(args, world, rank, local):
     gemm_ms, gemm_flops, gemm_launches = prof
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
     tr = traffic_summary()
-    roof = {"bound": "tensor", "kernel": "tb::gemm_kernel (all GEMM-engine launches of the step)",
-            "achieved": achieved, "peak": sustained, "unit": "TFLOP/s",
+    roof = {"bound": "tensor", "kernel": "tb::gemm_kernel / gemm_pair_kernel (all GEMM-engine launches of the step)",
+            "achieved": achieved, "achieved_note": "algorithmic flops of the launches / the union of their "
+            "event-timed intervals (the TRSM halves' launches on two streams overlap)",
+            "peak": sustained, "unit": "TFLOP/s",
             "frac": (achieved / sustained) if achieved and sustained else None,
             "peak_source": f"{peak_src} bf16_tflops_sustained (burst {burst})",
             "launches_per_step": gemm_launches / args.steps,

@@ -55,8 +55,10 @@ TB_API tb_status tb_synchronize(void);
 TB_API int tb_version(void);
 /* Number of kernels this library has launched in this process. */
 TB_API unsigned long long tb_launch_count(void);
-/* Event timing of every GEMM-engine launch between begin and end (on the
- * launching stream): total device ms, total algorithmic flops, launches. */
+/* Event timing of every GEMM-engine launch between begin and end (events on
+ * the launching stream): device ms during which at least one of them ran (the
+ * union of their intervals: launches on two streams may overlap), total
+ * algorithmic flops, launches. */
 TB_API tb_status tb_profile_begin(void);
 TB_API tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launches);
 

@@ -250,50 +250,63 @@ __device__ __forceinline__ void combine32(const EpiK& k, float* S, int row, cons
   for (int j = 0; j < 32; ++j) S[j * 128 + row] = r[j];
 }
 
+// Scalars of the per-element store path for one tile, read into registers
+// once per tile (EpiK's fields plus C, bounds and the side-copy fields): in
+// grouped launches the problem descriptor lives in global memory, and
+// reading its fields inside every chunk put a chain of global loads in front
+// of each chunk's stores.
+struct StoreK : EpiK {
+  float* C;
+  long long ldc, ld_out;
+  int N, out_m, out_n;
+  __half* out_hi;
+  __half* out_lo;
+  __device__ __forceinline__ explicit StoreK(const GemmArgs& a)
+      : EpiK(a), C(a.C), ldc(a.ldc), ld_out(a.ld_out), N(a.N), out_m(a.out_m), out_n(a.out_n), out_hi(a.out_hi),
+        out_lo(a.out_lo) {}
+};
+
 // Fused fp16 hi[/lo] copies of 32 result values of one row.
-__device__ __forceinline__ void store_fp16_copies(const GemmArgs& args, const float* r, long long gi, long long gj0) {
-  const EpiK k(args);
-  const long long ld = args.ld_out, out_n = args.out_n;
-  __half* hrow = args.out_hi + gi + gj0 * ld;
-  __half* lrow = args.out_lo ? args.out_lo + gi + gj0 * ld : nullptr;
+__device__ __forceinline__ void store_fp16_copies(const StoreK& s, const float* r, long long gi, long long gj0) {
+  const long long ld = s.ld_out, out_n = s.out_n;
+  __half* hrow = s.out_hi + gi + gj0 * ld;
+  __half* lrow = s.out_lo ? s.out_lo + gi + gj0 * ld : nullptr;
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    if (gj >= out_n || k.masked(gi, gj)) continue;
+    if (gj >= out_n || s.masked(gi, gj)) continue;
     const __half h = __float2half_rn(r[j]);
     hrow[(long long)j * ld] = h;
-    if (lrow) lrow[(long long)j * ld] = __float2half_rn((r[j] - __half2float(h)) * k.lo_scale);
+    if (lrow) lrow[(long long)j * ld] = __float2half_rn((r[j] - __half2float(h)) * s.lo_scale);
   }
 }
 
 // Per-element path: alpha/beta update of 32 consecutive columns of one row,
 // with the lower-triangle mask and bounds. With beta != 0 the 32 old values
 // are loaded before any store so the loads are in flight together.
-__device__ __forceinline__ void epilogue_store32(const GemmArgs& args, const float* v, long long gi, long long gj0) {
-  const EpiK k(args);
-  const long long ldc = args.ldc, N = args.N;
-  const bool copies = args.out_hi && gi < args.out_m;
-  float* crow = args.C + gi + gj0 * ldc;
+__device__ __forceinline__ void epilogue_store32(const StoreK& s, const float* v, long long gi, long long gj0) {
+  const long long ldc = s.ldc;
+  float* crow = s.C + gi + gj0 * ldc;
   bool keep[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const long long gj = gj0 + j;
-    keep[j] = gj < N && !k.masked(gi, gj);
+    keep[j] = gj < s.N && !s.masked(gi, gj);
   }
   float r[32];
-  if (k.beta != 0.0f) {
+  if (s.beta != 0.0f) {
 #pragma unroll
     for (int j = 0; j < 32; ++j) r[j] = keep[j] ? __ldg(crow + (long long)j * ldc) : 0.f;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) r[j] = fmaf(k.beta, r[j], k.alpha * v[j]);
+    for (int j = 0; j < 32; ++j) r[j] = fmaf(s.beta, r[j], s.alpha * v[j]);
   } else {
 #pragma unroll
-    for (int j = 0; j < 32; ++j) r[j] = k.alpha * v[j];
+    for (int j = 0; j < 32; ++j) r[j] = s.alpha * v[j];
   }
 #pragma unroll
   for (int j = 0; j < 32; ++j)
     if (keep[j]) crow[(long long)j * ldc] = r[j];
-  if (copies) store_fp16_copies(args, r, gi, gj0);
+  if (s.out_hi && gi < s.out_m) store_fp16_copies(s, r, gi, gj0);
 }
 
 // Epilogue state shared by the 4 epilogue warps (identical in all of them).
@@ -363,7 +376,7 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
     }
     bulk_commit();
   }
-  if (copies) store_fp16_copies(args, r, gi, gj0);
+  if (copies) store_fp16_copies(StoreK(args), r, gi, gj0);
   ++es.chunk;
   es.last_side = side_mode;
 }
@@ -436,7 +449,7 @@ __device__ __forceinline__ bool epilogue_chunk_pf(const GemmArgs& args, float* s
     bulk_commit();
   }
   pf.prev = slot;
-  if (copies) store_fp16_copies(args, r, gi, gj0);
+  if (copies) store_fp16_copies(StoreK(args), r, gi, gj0);
   if (side) ++pf.side;
   return true;
 }
@@ -727,6 +740,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
         const bool row_ok = gi < P.M;
         const bool tile_masked = tile_reaches_mask(P, tile.x, tile.y, BM, BN);
         const bool need_load = P.beta != 0.0f || tile_masked;
+        const StoreK sk(P);
         if constexpr (!Cfg::FOLD) {
           const int buf = it & 1;
           const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -755,7 +769,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
                 break;
               }
             } else if (row_ok)
-              epilogue_store32(P, v, gi, (long long)tile.y + c0);
+              epilogue_store32(sk, v, gi, (long long)tile.y + c0);
           }
         } else {
           float acc[BN];
@@ -794,7 +808,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
                 break;
               }
             } else if (row_ok)
-              epilogue_store32(P, acc + c0, gi, (long long)tile.y + c0);
+              epilogue_store32(sk, acc + c0, gi, (long long)tile.y + c0);
           }
         }
       }
@@ -811,6 +825,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
       // masked tiles with beta == 0 store their unmasked elements directly:
       // the TMA path would first have to load C to keep the masked ones
       const bool direct = tile_masked && P.beta == 0.0f;
+      const StoreK sk(P);
       if constexpr (!Cfg::FOLD) {
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
@@ -834,7 +849,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
               epilogue_chunk_tma(P, stage_c, cload, es, v, tile.x, tile.y + c0, row, P.beta != 0.0f || tile_masked,
                                  issuer, abort_flag);
           } else if (row_ok) {
-            epilogue_store32(P, v, gi, (long long)tile.y + c0);
+            epilogue_store32(sk, v, gi, (long long)tile.y + c0);
           }
         }
       } else {
@@ -884,7 +899,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
               epilogue_chunk_tma(P, stage_c, cload, es, acc + c0, tile.x, tile.y + c0, row,
                                  P.beta != 0.0f || tile_masked, issuer, abort_flag);
           } else if (row_ok) {
-            epilogue_store32(P, acc + c0, gi, (long long)tile.y + c0);
+            epilogue_store32(sk, acc + c0, gi, (long long)tile.y + c0);
           }
         }
       }
@@ -1107,6 +1122,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       const bool row_ok = gi < args.M;
       const bool tile_masked = tile_reaches_mask(args, m0, tile.y, 128, BN);
       const bool direct = tile_masked && args.beta == 0.0f;  // as in the single-CTA kernel
+      const StoreK sk(args);
       const int buf = it & 1;
       const uint32_t tph = (uint32_t)(it >> 1) & 1u;
       if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) break;
@@ -1126,7 +1142,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
             epilogue_chunk_tma(args, stage_c, cload, es, v, m0, tile.y + c0, row, args.beta != 0.0f || tile_masked,
                                issuer, abort_flag);
         } else if (row_ok) {
-          epilogue_store32(args, v, gi, (long long)tile.y + c0);
+          epilogue_store32(sk, v, gi, (long long)tile.y + c0);
         }
       }
     }

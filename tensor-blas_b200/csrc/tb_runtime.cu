@@ -1,6 +1,7 @@
 // Library runtime: status strings, per-thread error text, the current stream,
 // the per-device scratch pool and the device error word used by the bounded
 // waits of the persistent kernels.
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -205,21 +206,40 @@ tb_status tb_profile_begin(void) {
 
 tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launches) {
   tb::g_prof_on = false;
-  double ms = 0, fl = 0;
+  double fl = 0;
   long cnt = 0;
   tb_status st = TB_SUCCESS;
-  for (auto& r : tb::g_prof_live) {
+  // launch intervals relative to the first launch's start event; launches on
+  // different streams may overlap, so the device time is their union
+  std::vector<std::pair<double, double>> iv;
+  const cudaEvent_t ref = tb::g_prof_live.empty() ? nullptr : tb::g_prof_live.front().a;
+  for (auto& r : tb::g_prof_live)
     if (cudaEventSynchronize(r.b) != cudaSuccess) st = TB_ERROR_CUDA;
-    float t = 0;
-    if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
-      ms += t;
+  for (auto& r : tb::g_prof_live) {
+    float t0 = 0, t1 = 0;
+    if (cudaEventElapsedTime(&t0, ref, r.a) == cudaSuccess && cudaEventElapsedTime(&t1, ref, r.b) == cudaSuccess) {
+      iv.push_back({t0, t1});
       fl += r.flops;
       ++cnt;
     }
+  }
+  for (auto& r : tb::g_prof_live) {
     tb::g_ev_free.push_back(r.a);
     tb::g_ev_free.push_back(r.b);
   }
   tb::g_prof_live.clear();
+  std::sort(iv.begin(), iv.end());
+  double ms = 0, cur0 = 0, cur1 = -1e300;
+  for (const auto& x : iv) {
+    if (x.first > cur1) {
+      if (cur1 > cur0) ms += cur1 - cur0;
+      cur0 = x.first;
+      cur1 = x.second;
+    } else if (x.second > cur1) {
+      cur1 = x.second;
+    }
+  }
+  if (cur1 > cur0) ms += cur1 - cur0;
   if (gemm_ms) *gemm_ms = ms;
   if (gemm_flops) *gemm_flops = fl;
   if (gemm_launches) *gemm_launches = cnt;
