@@ -29,7 +29,8 @@ namespace tb {
 namespace {
 
 constexpr int kMaxDev = 64;
-constexpr int kEvents = 24;
+constexpr int kEvents = 32;
+constexpr int kSyrkSlots = 3;  // SYRK staging slots for A and C panels
 
 struct HostPipes {
   cudaStream_t h2d = nullptr, d2h = nullptr;
@@ -65,14 +66,14 @@ enum : int {
   kEvStart = 0,
   kEvEndH2d,
   kEvEndD2h,
-  kEvA,        // [2] A panel staged
-  kEvC = 5,    // [2] C panel staged
-  kEvConv = 7, // [2] A staging slot consumed
-  kEvGemm = 9, // [2] C panel computed
-  kEvOut = 11, // [3] panel copied back
-  kEvIn = 14,  // [3] B panel staged
-  kEvDone = 17,// [3] B panel solved
-  kEvTri = 20, // A triangle staged
+  kEvA,         // [3] A panel staged
+  kEvC = 6,     // [3] C panel staged
+  kEvConv = 9,  // [3] A staging slot consumed
+  kEvGemm = 12, // [3] C panel computed
+  kEvOut = 15,  // [3] panel copied back
+  kEvIn = 18,   // [3] B panel staged
+  kEvDone = 21, // [3] B panel solved
+  kEvTri = 24,  // A triangle staged
 };
 
 tb_status finish(cudaStream_t cs, HostPipes& p) {
@@ -104,7 +105,7 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   const size_t half_bytes = (size_t)round_up(ldh * k * 2, 256);
   const size_t stA_bytes = (size_t)round_up((long long)P * k * 4, 256);
   const size_t cb_bytes = (size_t)round_up((long long)P * n * 4, 256);
-  const size_t total = half_bytes * (hilo ? 2 : 1) + 2 * stA_bytes + 2 * cb_bytes;
+  const size_t total = half_bytes * (hilo ? 2 : 1) + kSyrkSlots * (stA_bytes + cb_bytes);
   char* ws = static_cast<char*>(pool_get(total, 1));
   if (!ws) {
     set_last_error("tb_ssyrk_host: cannot allocate %zu bytes of staging", total);
@@ -113,8 +114,14 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   __half* hi = reinterpret_cast<__half*>(ws);
   __half* lo = hilo ? reinterpret_cast<__half*>(ws + half_bytes) : nullptr;
   char* w2 = ws + half_bytes * (hilo ? 2 : 1);
-  float* stA[2] = {reinterpret_cast<float*>(w2), reinterpret_cast<float*>(w2 + stA_bytes)};
-  float* cb[2] = {reinterpret_cast<float*>(w2 + 2 * stA_bytes), reinterpret_cast<float*>(w2 + 2 * stA_bytes + cb_bytes)};
+  // three slots: the upload of panel i's C block waits for panel i-3's C to
+  // have come back, so a long download does not hold up the uploads behind it
+  float* stA[kSyrkSlots];
+  float* cb[kSyrkSlots];
+  for (int q = 0; q < kSyrkSlots; ++q) {
+    stA[q] = reinterpret_cast<float*>(w2 + q * stA_bytes);
+    cb[q] = reinterpret_cast<float*>(w2 + kSyrkSlots * stA_bytes + q * cb_bytes);
+  }
 
   // everything starts after the work already queued on the caller's stream
   TB_TRY(join(p.h2d, cs, p.ev[kEvStart]));
@@ -133,15 +140,15 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   const long npan = (n + P - 1) / P;
   for (long i = 0; i < npan; ++i) {
     const long r0 = i * P, r1 = std::min(n, r0 + P), pr = r1 - r0;
-    const int s = (int)(i & 1);
-    // A rows [r0, r1) -> staging slot s (reused once panel i-2 was converted)
-    if (i >= 2) TB_CUDA_TRY(cudaStreamWaitEvent(p.h2d, p.ev[kEvConv + s], 0));
+    const int s = (int)(i % kSyrkSlots);
+    // A rows [r0, r1) -> staging slot s (reused once panel i-3 was converted)
+    if (i >= kSyrkSlots) TB_CUDA_TRY(cudaStreamWaitEvent(p.h2d, p.ev[kEvConv + s], 0));
     TB_CUDA_TRY(cudaMemcpy2DAsync(stA[s], P * 4, hA + r0, (size_t)lda * 4, (size_t)pr * 4, (size_t)k,
                                   cudaMemcpyHostToDevice, p.h2d));
     TB_CUDA_TRY(cudaEventRecord(p.ev[kEvA + s], p.h2d));
     // C rows [r0, r1): the diagonal block (its strict upper part must come
     // back unchanged), or all columns [0, r1) when beta != 0
-    if (i >= 2) TB_CUDA_TRY(cudaStreamWaitEvent(p.h2d, p.ev[kEvOut + s], 0));
+    if (i >= kSyrkSlots) TB_CUDA_TRY(cudaStreamWaitEvent(p.h2d, p.ev[kEvOut + s], 0));
     const long c0 = beta != 0.f ? 0 : r0;
     TB_CUDA_TRY(cudaMemcpy2DAsync(cb[s] + c0 * P, P * 4, hC + r0 + (size_t)c0 * ldc, (size_t)ldc * 4, (size_t)pr * 4,
                                   (size_t)(r1 - c0), cudaMemcpyHostToDevice, p.h2d));
