@@ -223,12 +223,20 @@ struct EpiK {
   int tri, diag;
   __device__ __forceinline__ explicit EpiK(const GemmArgs& a)
       : alpha(a.alpha), beta(a.beta), lo_scale(a.out_lo_scale), tri(a.tri), diag(a.diag) {}
-  __device__ __forceinline__ bool masked(long long gi, long long gj) const {
-    return tri == 1 ? (gi - gj) < diag : (tri == 2 ? (gj - gi) < diag : false);
-  }
   // some element of the 128 x 32 chunk at (m0, n0) is masked
   __device__ __forceinline__ bool chunk_masked(long long m0, long long n0) const {
     return tri == 1 ? (m0 - (n0 + 31)) < diag : (tri == 2 ? (n0 - (m0 + 127)) < diag : false);
+  }
+  // The columns gj0 + [lo, hi) of row gi, out of the 32 from gj0 and below
+  // `ncols` (a bound on gj), that the mask keeps: one range per row, so the
+  // element loops compare small ints instead of testing every element's
+  // 64-bit (i, j) against the triangle (which cost more than the stores).
+  __device__ __forceinline__ void keep_range(long long gi, long long gj0, long long ncols, int& lo, int& hi) const {
+    long long h = ncols - gj0, l = 0;
+    if (tri == 1) h = min(h, gi - diag + 1 - gj0);  // keep gj <= gi - diag
+    if (tri == 2) l = gi + diag - gj0;              // keep gj >= gi + diag
+    hi = (int)max(0LL, min(32LL, h));
+    lo = (int)max(0LL, min(32LL, l));
   }
 };
 
@@ -237,10 +245,12 @@ struct EpiK {
 __device__ __forceinline__ void combine32(const EpiK& k, float* S, int row, const float* v, long long gi,
                                           long long gj0, bool any_masked, float* r) {
   if (any_masked) {
+    int lo, hi;
+    k.keep_range(gi, gj0, gj0 + 32, lo, hi);
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       const float old = S[j * 128 + row];
-      r[j] = k.masked(gi, gj0 + j) ? old : fmaf(k.beta, old, k.alpha * v[j]);
+      r[j] = (j >= lo && j < hi) ? fmaf(k.beta, old, k.alpha * v[j]) : old;
     }
   } else {
 #pragma unroll
@@ -268,13 +278,14 @@ struct StoreK : EpiK {
 
 // Fused fp16 hi[/lo] copies of 32 result values of one row.
 __device__ __forceinline__ void store_fp16_copies(const StoreK& s, const float* r, long long gi, long long gj0) {
-  const long long ld = s.ld_out, out_n = s.out_n;
+  const long long ld = s.ld_out;
   __half* hrow = s.out_hi + gi + gj0 * ld;
   __half* lrow = s.out_lo ? s.out_lo + gi + gj0 * ld : nullptr;
+  int lo, hi;
+  s.keep_range(gi, gj0, s.out_n, lo, hi);
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
-    const long long gj = gj0 + j;
-    if (gj >= out_n || s.masked(gi, gj)) continue;
+    if (j < lo || j >= hi) continue;
     const __half h = __float2half_rn(r[j]);
     hrow[(long long)j * ld] = h;
     if (lrow) lrow[(long long)j * ld] = __float2half_rn((r[j] - __half2float(h)) * s.lo_scale);
@@ -287,12 +298,11 @@ __device__ __forceinline__ void store_fp16_copies(const StoreK& s, const float* 
 __device__ __forceinline__ void epilogue_store32(const StoreK& s, const float* v, long long gi, long long gj0) {
   const long long ldc = s.ldc;
   float* crow = s.C + gi + gj0 * ldc;
+  int lo, hi;
+  s.keep_range(gi, gj0, s.N, lo, hi);
   bool keep[32];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    const long long gj = gj0 + j;
-    keep[j] = gj < s.N && !s.masked(gi, gj);
-  }
+  for (int j = 0; j < 32; ++j) keep[j] = j >= lo && j < hi;
   float r[32];
   if (s.beta != 0.0f) {
 #pragma unroll
