@@ -211,6 +211,13 @@ struct OzArgs {
 __device__ __forceinline__ int level_pairs_begin(int L, int S) { return L - S > 1 ? L - S : 1; }
 __device__ __forceinline__ int level_pairs_end(int L, int S) { return L - 1 < S ? L - 1 : S; }
 
+// 2^e for an integer e: built from the IEEE-754 exponent field when 2^e is a
+// normal double (the fold's scales always are in practice), else ldexp.
+__device__ __forceinline__ double pow2i(int e) {
+  if (e >= -1022 && e <= 1023) return __longlong_as_double((long long)(e + 1023) << 52);
+  return ldexp(1.0, e);
+}
+
 __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__ OzArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -392,13 +399,18 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
           int v[32];
           tmem_ld32_s32(tacc + c0, v);
           if (!row_ok) continue;
+          // the columns tile.y + c0 + [lo, hi) of this row that are written:
+          // one range per row instead of a 64-bit triangle test per element
+          const long long g0 = (long long)tile.y + c0;
+          long long hl = (long long)N - g0, ll = 0;
+          if (tri == 1) hl = min(hl, gi - g0 + 1);  // gj <= gi
+          if (tri == 2) ll = gi - g0;               // gj >= gi
+          const int hi = (int)max(0LL, min(32LL, hl)), lo = (int)max(0LL, min(32LL, ll));
           if (!fold) {
             if (L != raw_level) continue;
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const long long gj = (long long)tile.y + c0 + j;
-              if (gj < N && (tri == 0 || (tri == 1 ? gj <= gi : gj >= gi))) raw_out[gi + gj * ld_raw] = v[j];
-            }
+            for (int j = 0; j < 32; ++j)
+              if (j >= lo && j < hi) raw_out[gi + (g0 + j) * ld_raw] = v[j];
             continue;
           }
           double old[32];
@@ -406,8 +418,8 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
           int ejs[32];
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
-            const long long gj = (long long)tile.y + c0 + j;
-            keep[j] = gj < N && (tri == 0 || (tri == 1 ? gj <= gi : gj >= gi));
+            const long long gj = g0 + j;
+            keep[j] = j >= lo && j < hi;
             old[j] = 0.0;
             ejs[j] = 0;
             if (keep[j]) {
@@ -419,7 +431,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
           for (int j = 0; j < 32; ++j) {
             if (!keep[j]) continue;
             const long long gj = (long long)tile.y + c0 + j;
-            const double scale = alpha * ldexp(1.0, ei + ejs[j] - 7 * L);
+            const double scale = alpha * pow2i(ei + ejs[j] - 7 * L);
             const double base = (L == 2) ? beta * old[j] : old[j];
             Cg[gi + gj * ldc] = fma(scale, (double)v[j], base);
           }
