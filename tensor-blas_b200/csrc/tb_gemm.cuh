@@ -213,11 +213,9 @@ __device__ __forceinline__ bool tile_reaches_mask(const GemmArgs& a, long long m
 }
 
 // Epilogue scalars, read into registers once per chunk. The epilogue's
-// stores go through generic pointers (shared-memory slots, C, side copies),
-// which the compiler cannot tell apart from the kernel's parameter memory:
-// GemmArgs fields read inside a store loop are re-read from parameter space
-// after every store, which made the masked/beta chunks several times slower
-// than their arithmetic.
+// stores go through generic pointers (shared-memory slots, C, side copies)
+// that the compiler cannot tell apart from the kernel's parameter memory, so
+// GemmArgs fields read inside a store loop may be reloaded after every store.
 struct EpiK {
   float alpha, beta, lo_scale;
   int tri, diag;
@@ -261,10 +259,8 @@ __device__ __forceinline__ void combine32(const EpiK& k, float* S, int row, cons
 }
 
 // Scalars of the per-element store path for one tile, read into registers
-// once per tile (EpiK's fields plus C, bounds and the side-copy fields): in
-// grouped launches the problem descriptor lives in global memory, and
-// reading its fields inside every chunk put a chain of global loads in front
-// of each chunk's stores.
+// once per tile (EpiK's fields plus C, bounds and the side-copy fields; in
+// grouped launches the problem descriptor lives in global memory).
 struct StoreK : EpiK {
   float* C;
   long long ldc, ld_out;
