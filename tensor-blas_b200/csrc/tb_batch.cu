@@ -60,10 +60,19 @@ __global__ void __launch_bounds__(256) conv_grouped_kernel(const ConvJob* __rest
   const long long e0 = (b - jb.first) * kConvPerBlock + threadIdx.x;
   long long at[kConvPerThread];
   float f[kConvPerThread];
+  // (i, j) of element e0 by one division; the thread's later elements step
+  // 256 further each, which moves i on and wraps it into the next column(s)
+  long long j = e0 / rows, i = e0 - j * rows;
 #pragma unroll
   for (int q = 0; q < kConvPerThread; ++q) {
     const long long e = e0 + q * 256;
-    const long long j = e / rows, i = e - j * rows;
+    if (q > 0) {
+      i += 256;
+      while (i >= rows) {
+        i -= rows;
+        ++j;
+      }
+    }
     const bool ok = e < total && !(tri == 2 && i < ((j >> 3) << 3));
     at[q] = ok ? i + j * ldd : -1;
     f[q] = ok ? __ldg(src + i + j * lds) : 0.f;
