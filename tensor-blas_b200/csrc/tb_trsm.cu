@@ -104,9 +104,12 @@ __device__ __forceinline__ void trtri_panel_body(const T* __restrict__ A, long l
                                                  const double* __restrict__ D, __half* __restrict__ hi,
                                                  __half* __restrict__ lo, double* __restrict__ Wg, long long ldg,
                                                  long long ldw, int j) {
-  __shared__ __align__(16) double LsT[32][34];  // LsT[k][r] = L(r, k) of the staged sub-block (or Dinv_i)
-  __shared__ __align__(16) double Ts[32][36];   // Ts[k][c]
-  __shared__ __align__(16) double Wb[32][36];   // Wb[k][c] = W(32p + k, 32j + c)
+  // two staging buffers: sub-block p + 1 is loaded into registers while p's
+  // products run, so each step of the chain waits on one barrier and its
+  // global loads overlap the FMAs
+  __shared__ __align__(16) double LsT[2][32][34];  // LsT[b][k][r] = L(r, k) of a staged sub-block (or Dinv_i)
+  __shared__ __align__(16) double Ts[32][36];      // Ts[k][c]
+  __shared__ __align__(16) double Wb[2][32][36];   // Wb[b][k][c] = W(32p + k, 32j + c)
   const int nsub = (size + 31) / 32;
   if (j >= nsub) return;
   const int tid = threadIdx.x;
@@ -121,20 +124,35 @@ __device__ __forceinline__ void trtri_panel_body(const T* __restrict__ A, long l
   __syncthreads();
   for (int i = j + 1; i < nsub; ++i) {
     double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-    for (int p = j; p < i; ++p) {
+    double ra[8], rw[8];
+    auto fetch = [&](int p) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int cc = lc + 4 * q;
         const int gr = 32 * i + lr, gc = 32 * p + cc;
-        LsT[cc][lr] = (gr < size && gc < size) ? (double)A[(long long)s + gr + ((long long)s + gc) * lda] : 0.0;
-        Wb[lr][cc] = __ldcg(Wp + 32 * p + lr + (long long)cc * ldg);
+        ra[q] = (gr < size && gc < size) ? (double)A[(long long)s + gr + ((long long)s + gc) * lda] : 0.0;
+        rw[q] = __ldcg(Wp + 32 * p + lr + (long long)cc * ldg);
+      }
+    };
+    fetch(j);
+    int bsel = 0;
+    for (int p = j; p < i; ++p) {
+      bsel = (p - j) & 1;
+      // buffer bsel was last read in step p - 2, which every thread finished
+      // before the barrier of step p - 1
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int cc = lc + 4 * q;
+        LsT[bsel][cc][lr] = ra[q];
+        Wb[bsel][lr][cc] = rw[q];
       }
       __syncthreads();
+      if (p + 1 < i) fetch(p + 1);
 #pragma unroll 4
       for (int kk = 0; kk < 32; ++kk) {
-        const double2 l = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
-        const double2 w01 = *reinterpret_cast<const double2*>(&Wb[kk][c0]);
-        const double2 w23 = *reinterpret_cast<const double2*>(&Wb[kk][c0 + 2]);
+        const double2 l = *reinterpret_cast<const double2*>(&LsT[bsel][kk][r0]);
+        const double2 w01 = *reinterpret_cast<const double2*>(&Wb[bsel][kk][c0]);
+        const double2 w23 = *reinterpret_cast<const double2*>(&Wb[bsel][kk][c0 + 2]);
         acc[0][0] = fma(l.x, w01.x, acc[0][0]);
         acc[0][1] = fma(l.x, w01.y, acc[0][1]);
         acc[0][2] = fma(l.x, w23.x, acc[0][2]);
@@ -144,8 +162,10 @@ __device__ __forceinline__ void trtri_panel_body(const T* __restrict__ A, long l
         acc[1][2] = fma(l.y, w23.x, acc[1][2]);
         acc[1][3] = fma(l.y, w23.y, acc[1][3]);
       }
-      __syncthreads();
     }
+    // Ts was last read by the previous step's tail, behind its final barrier;
+    // Dinv_i goes into the staging buffer the last product step did not read
+    const int dsel = bsel ^ 1;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -153,13 +173,13 @@ __device__ __forceinline__ void trtri_panel_body(const T* __restrict__ A, long l
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int cc = lc + 4 * q;
-      LsT[cc][lr] = D[(sub0 + i) * 1024 + lr + 32 * cc];
+      LsT[dsel][cc][lr] = D[(sub0 + i) * 1024 + lr + 32 * cc];
     }
     __syncthreads();
     double o[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
 #pragma unroll 4
     for (int kk = 0; kk < 32; ++kk) {
-      const double2 d = *reinterpret_cast<const double2*>(&LsT[kk][r0]);
+      const double2 d = *reinterpret_cast<const double2*>(&LsT[dsel][kk][r0]);
       const double2 t01 = *reinterpret_cast<const double2*>(&Ts[kk][c0]);
       const double2 t23 = *reinterpret_cast<const double2*>(&Ts[kk][c0 + 2]);
       o[0][0] = fma(-d.x, t01.x, o[0][0]);
