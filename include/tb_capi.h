@@ -115,6 +115,11 @@ TB_API tb_status tb_autotune_get(const char* routine, const char* flags, long a,
  *   side 'L': A * X = B,    A m x m, B m x n  (left/lower/no-trans)
  * Replaces tc_trsm (include/TensorBLAS.h:147) and, with TB_PREC_SPLIT,
  * tc_cumpsgemm_trsm (BLAS/tc_cumpsgemm_trsm.cu:3-126).
+ * In plain precision, when B has at least 4096 independent columns (left)
+ * or rows (right), the two halves are solved on the library's stream and
+ * on an internal second stream of the same device, which is joined back
+ * into the library's stream (event wait) before the call returns: work
+ * queued afterwards on that stream sees the whole result.
  */
 TB_API tb_status tb_strsm(char side, long m, long n, const float* A, long lda, float* B, long ldb, long nb,
                           int precision);
