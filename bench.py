@@ -49,6 +49,8 @@ def parse():
                         "quantisation) at bench sizes and exit: the command their ncu summaries come from")
     p.add_argument("--profile-gemm", type=int, default=0, metavar="N",
                    help="run three plain N x N x N SGEMMs and exit (the GEMM-engine ncu captures)")
+    p.add_argument("--profile-ozaki", type=int, default=0, metavar="N",
+                   help="run two FP64 Ozaki DSYRKs n = k = N with 8 slices and exit (the Ozaki-engine ncu captures)")
     return p.parse_args()
 
 
@@ -678,6 +680,27 @@ def profile_gemm(args):
     print("profile gemm done", flush=True)
 
 
+def profile_ozaki(args):
+    """Two untimed Ozaki DSYRKs n = k = args.profile_ozaki, 8 slices (lower,
+    'N'): the command the Ozaki-engine ncu summaries were captured from."""
+    import ctypes
+
+    import TensorBLAS as TB
+
+    m = args.profile_ozaki
+    g = torch.Generator(device="cuda")
+    g.manual_seed(9)
+    D = torch.randn(m, m, dtype=torch.float64, device="cuda", generator=g)
+    E = torch.zeros(m, m, dtype=torch.float64, device="cuda")
+    L, P = ctypes.c_long, ctypes.c_void_p
+    TB.lib.tb_dsyrk_ozaki.argtypes = [ctypes.c_char, ctypes.c_char, L, L, ctypes.c_double, P, L, ctypes.c_double, P, L,
+                                      ctypes.c_int]
+    for _ in range(2):
+        TB._check(TB.lib.tb_dsyrk_ozaki(b"L", b"N", m, m, 1.0, D.data_ptr(), m, 0.0, E.data_ptr(), m, 8))
+    TB.synchronize()
+    print("profile ozaki done", flush=True)
+
+
 def profile_aux(args):
     """One plain SYRK and TRSM at n (FP32->FP16 conversions, 32x32 and leaf
     inverses), one Ozaki DSYRK n=k=8192 with 10 slices (exponent and slicing
@@ -720,6 +743,9 @@ def main():
         return
     if args.profile_gemm:
         profile_gemm(args)
+        return
+    if args.profile_ozaki:
+        profile_ozaki(args)
         return
     if args.profile_step:
         profile_step(args)

@@ -218,6 +218,81 @@ __device__ __forceinline__ double pow2i(int e) {
   return ldexp(1.0, e);
 }
 
+// The fold epilogue's scalars, copied into registers: the stores go through
+// generic pointers the compiler cannot tell apart from the parameter memory,
+// so fields read in the store loops would be re-read from it after every
+// store.
+struct OzEpi {
+  double* C;
+  int* raw_out;
+  long long ldc, ld_raw;
+  const int* eA;
+  const int* eB;
+  double alpha;
+  int N, M, tri, raw_level;
+};
+
+__device__ __forceinline__ OzEpi oz_epi(const OzArgs& a) {
+  return OzEpi{a.C, a.raw_out, a.ldc, a.ld_raw, a.eA, a.eB, a.alpha, a.N, a.M, a.tri, a.raw_level};
+}
+
+// A row's slicing exponent (all-zero rows keep a very negative one and were
+// sliced with exponent 0).
+__device__ __forceinline__ int oz_row_exp(const int* e, long long i) { return e[i] < -1000 ? 0 : e[i]; }
+
+// Empty product (K range outside the operands' support): C(gi, n0 + j) =
+// beta C(gi, n0 + j) for the tile's written columns.
+__device__ __forceinline__ void oz_scale_row(const OzEpi& ep, long long gi, long long n0, double beta) {
+  if (beta == 1.0 || ep.raw_level >= 2) return;
+  for (int j = 0; j < kOzBN; ++j) {
+    const long long gj = n0 + j;
+    if (gj < ep.N && (ep.tri == 0 || (ep.tri == 1 ? gj <= gi : gj >= gi))) {
+      double* c = ep.C + gi + gj * ep.ldc;
+      *c = beta == 0.0 ? 0.0 : beta * *c;
+    }
+  }
+}
+
+// Level L's INT32 sums v of row gi at columns g0 + [0, 32): each folded into
+// C with one rounding, C = alpha 2^(ei + ej - 7L) v + (L == 2 ? beta C : C),
+// or written as they are when L is the requested raw level.
+__device__ __forceinline__ void oz_fold32(const OzEpi& ep, const int* v, long long gi, long long g0, int ei, int L,
+                                          double beta) {
+  // the columns g0 + [lo, hi) of this row that are written: one range per
+  // row instead of a 64-bit triangle test per element
+  long long hl = (long long)ep.N - g0, ll = 0;
+  if (ep.tri == 1) hl = min(hl, gi - g0 + 1);  // gj <= gi
+  if (ep.tri == 2) ll = gi - g0;               // gj >= gi
+  const int hi = (int)max(0LL, min(32LL, hl)), lo = (int)max(0LL, min(32LL, ll));
+  if (ep.raw_level >= 2) {
+    if (L != ep.raw_level) return;
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (j >= lo && j < hi) ep.raw_out[gi + (g0 + j) * ep.ld_raw] = v[j];
+    return;
+  }
+  double old[32];
+  bool keep[32];
+  int ejs[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    keep[j] = j >= lo && j < hi;
+    old[j] = 0.0;
+    ejs[j] = 0;
+    if (keep[j]) {
+      if (L > 2 || beta != 0.0) old[j] = ep.C[gi + (g0 + j) * ep.ldc];
+      ejs[j] = oz_row_exp(ep.eB, g0 + j);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (!keep[j]) continue;
+    const double scale = ep.alpha * pow2i(ei + ejs[j] - 7 * L);
+    const double base = (L == 2) ? beta * old[j] : old[j];
+    ep.C[gi + (g0 + j) * ep.ldc] = fma(scale, (double)v[j], base);
+  }
+}
+
 __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__ OzArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -354,34 +429,17 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
     const int quarter = warp & 3;
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
-    // scalars in registers: the stores below go through generic pointers the
-    // compiler cannot tell apart from the parameter memory, so fields read in
-    // the store loops would be re-read from it after every store
-    double* const Cg = args.C;
-    int* const raw_out = args.raw_out;
-    const long long ldc = args.ldc, ld_raw = args.ld_raw;
-    const int* const eA = args.eA;
-    const int* const eB = args.eB;
-    const double alpha = args.alpha;
-    const int N = args.N, M = args.M, tri = args.tri, raw_level = args.raw_level;
+    const OzEpi ep = oz_epi(args);
     int it = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
       const int4 tile = args.tiles[t];
       const double beta = (tile.z & kOzAccumulate) ? 1.0 : args.beta;
       const long long gi = (long long)tile.x + row;
-      const bool row_ok = gi < M;
-      const int ei = row_ok ? (eA[gi] < -1000 ? 0 : eA[gi]) : 0;
+      const bool row_ok = gi < ep.M;
+      const int ei = row_ok ? oz_row_exp(ep.eA, gi) : 0;
       if (tile.w <= (tile.z & (kOzAccumulate - 1))) {
-        // empty product (K range outside the operand's support): C = beta C
-        if (row_ok && beta != 1.0 && raw_level < 2)
-          for (int j = 0; j < kOzBN; ++j) {
-            const long long gj = (long long)tile.y + j;
-            if (gj < N && (tri == 0 || (tri == 1 ? gj <= gi : gj >= gi))) {
-              double* c = Cg + gi + gj * ldc;
-              *c = beta == 0.0 ? 0.0 : beta * *c;
-            }
-          }
+        if (row_ok) oz_scale_row(ep, gi, tile.y, beta);
         continue;
       }
       for (int L = 2; L <= S + 1; ++L, ++it) {
@@ -393,48 +451,11 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
         }
         tc_fence_after();
         const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * kOzBN);
-        const bool fold = raw_level < 2;
 #pragma unroll 1
         for (int c0 = 0; c0 < kOzBN; c0 += 32) {
           int v[32];
           tmem_ld32_s32(tacc + c0, v);
-          if (!row_ok) continue;
-          // the columns tile.y + c0 + [lo, hi) of this row that are written:
-          // one range per row instead of a 64-bit triangle test per element
-          const long long g0 = (long long)tile.y + c0;
-          long long hl = (long long)N - g0, ll = 0;
-          if (tri == 1) hl = min(hl, gi - g0 + 1);  // gj <= gi
-          if (tri == 2) ll = gi - g0;               // gj >= gi
-          const int hi = (int)max(0LL, min(32LL, hl)), lo = (int)max(0LL, min(32LL, ll));
-          if (!fold) {
-            if (L != raw_level) continue;
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (j >= lo && j < hi) raw_out[gi + (g0 + j) * ld_raw] = v[j];
-            continue;
-          }
-          double old[32];
-          bool keep[32];
-          int ejs[32];
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const long long gj = g0 + j;
-            keep[j] = j >= lo && j < hi;
-            old[j] = 0.0;
-            ejs[j] = 0;
-            if (keep[j]) {
-              if (L > 2 || beta != 0.0) old[j] = Cg[gi + gj * ldc];
-              ejs[j] = eB[gj] < -1000 ? 0 : eB[gj];
-            }
-          }
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            if (!keep[j]) continue;
-            const long long gj = (long long)tile.y + c0 + j;
-            const double scale = alpha * pow2i(ei + ejs[j] - 7 * L);
-            const double base = (L == 2) ? beta * old[j] : old[j];
-            Cg[gi + gj * ldc] = fma(scale, (double)v[j], base);
-          }
+          if (row_ok) oz_fold32(ep, v, gi, (long long)tile.y + c0, ei, L, beta);
         }
         tc_fence_before();
         __syncwarp();
@@ -447,6 +468,254 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
   __syncthreads();
   tc_fence_after();
   if (warp == 1) tmem_dealloc(tmem_base, 512);
+}
+
+// ---------------------------------------------------------------- CTA pairs
+// The same product on 256 x 256 tiles, each run by a cluster of two CTAs on
+// two SMs (tcgen05 cta_group::2): CTA r loads rows tile.x + 128 r of the A
+// planes and rows tile.y + 128 r of the B planes into its own shared memory;
+// the leader (r = 0) issues the 256-row MMA, which reads both CTAs' halves,
+// and each CTA's TMEM receives its 128 accumulator rows, which its own
+// epilogue folds. Per SM one 128-deep K block moves 32 KB from L2 instead of
+// the single-CTA tile's 48 KB for the same MMA work. The level sums are the
+// same exact integers and the fold the same arithmetic, so the results are
+// bit-identical to the single-CTA kernel's.
+//   full[s]   leader only: both CTAs' loads complete_tx on it, the leader's
+//             producer arms it with both CTAs' bytes;
+//   empty[s]  both CTAs: the leader's commit multicasts to the pair;
+//   tfull[b]  both CTAs: the leader's commit multicasts to the pair;
+//   tempty[b] leader only: the 8 epilogue warps of the pair arrive remotely.
+// Every wait is bounded; a cluster barrier before TMEM is freed keeps either
+// CTA from leaving while the pair's MMAs or remote arrivals may still touch it.
+constexpr int kOzPairStages = 6;
+constexpr int kOzPairStageBytes = 2 * kOzABytes;  // 128 rows of A and 128 rows of B planes
+constexpr int kOzPairSmem = kOzPairStages * kOzPairStageBytes + 1024 + 256;
+static_assert(kOzPairSmem <= 232448, "shared memory budget");
+constexpr uint32_t kOzPairIdesc =
+    (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kOzBN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// 3-D tiled load into this CTA's shared memory whose completion is counted on
+// the pair leader's mbarrier (`leader_bar`, a shared::cluster address). No
+// multicast: every CTA fetches only its own half.
+__device__ __forceinline__ void tma_load_3d_pair(void* smem_dst, const CUtensorMap* map, uint32_t leader_bar, int x,
+                                                 int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+      "%5}], [%2];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(leader_bar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1) oz_pair_kernel(const __grid_constant__ OzArgs args) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOzPairStages * kOzPairStageBytes);
+  uint64_t* empty = full + kOzPairStages;
+  uint64_t* tfull = empty + kOzPairStages;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = args.S;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kOzPairStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 8);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_map(&args.mapA);
+    tma_prefetch_map(&args.mapB);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(tmem_slot, 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // the peer's barriers exist before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const uint32_t full_leader = mapa_shared(smem_u32(full), 0);
+  const uint32_t tempty_leader = mapa_shared(smem_u32(tempty), 0);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producers (both CTAs)
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      uint32_t issued_mask = 0, phase_mask = 0;
+      bool ok = true;
+      for (int t = pair; t < args.num_tiles && ok; t += npairs) {
+        const int4 tile = args.tiles[t];
+        const int kb0 = tile.z & (kOzAccumulate - 1), kb1 = tile.w;
+        for (int L = 2; L <= S + 1 && ok; ++L)
+          for (int s = level_pairs_begin(L, S); s <= level_pairs_end(L, S) && ok; ++s)
+            for (int kb = kb0; kb < kb1; ++kb) {
+              if (!mbar_wait(&empty[st], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
+                ok = false;
+                break;
+              }
+              int kbb = kb + args.kb_shift;
+              if (args.kb_mod > 0 && kbb >= args.kb_mod) kbb -= args.kb_mod;
+              if (leader) mbar_arrive_expect_tx(&full[st], 2 * kOzPairStageBytes);
+              uint8_t* dst = smem + st * kOzPairStageBytes;
+              const uint32_t bar = full_leader + 8u * (uint32_t)st;
+              tma_load_3d_pair(dst, &args.mapA, bar, kb * kOzBK, tile.x + 128 * (int)rank, s - 1);
+              tma_load_3d_pair(dst + kOzABytes, &args.mapB, bar, kbb * kOzBK, tile.y + 128 * (int)rank, L - s - 1);
+              issued_mask |= 1u << st;
+              phase_mask = (phase_mask & ~(1u << st)) | (ph << st);
+              if (++st == kOzPairStages) {
+                st = 0;
+                ph ^= 1u;
+              }
+            }
+      }
+      if (!ok) {
+        // Abort path: the leader sees its loads land on its own barriers; the
+        // peer's loads report to the leader, so the peer waits a bounded time.
+        if (leader) {
+          for (int i = 0; i < kOzPairStages; ++i) {
+            if (!((issued_mask >> i) & 1u)) continue;
+            const uint64_t t0 = globaltimer_ns();
+            while (!mbar_try_wait(&full[i], (phase_mask >> i) & 1u))
+              if (globaltimer_ns() - t0 > 1000000000ull) break;
+          }
+        } else {
+          const uint64_t t0 = globaltimer_ns();
+          while (globaltimer_ns() - t0 < 2000000ull) {
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer (leader)
+    if (leader && lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      int it = 0;
+      bool ok = true, any = false;
+      for (int t = pair; t < args.num_tiles && ok; t += npairs) {
+        const int4 tile = args.tiles[t];
+        const int kb0 = tile.z & (kOzAccumulate - 1), kb1 = tile.w;
+        if (kb1 <= kb0) continue;  // empty product: no accumulator round trip
+        for (int L = 2; L <= S + 1 && ok; ++L, ++it) {
+          const int buf = it & 1;
+          const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+          if (!mbar_wait(&tempty[buf], tph ^ 1u, abort_flag, args.err, kDevErrTimeoutMma)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem_base + (uint32_t)(buf * kOzBN);
+          bool first = true;
+          for (int s = level_pairs_begin(L, S); s <= level_pairs_end(L, S) && ok; ++s)
+            for (int kb = kb0; kb < kb1; ++kb) {
+              if (!mbar_wait(&full[st], ph, abort_flag, args.err, kDevErrTimeoutMma)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              const uint32_t a = smem_u32(smem + st * kOzPairStageBytes), b = a + kOzABytes;
+#pragma unroll
+              for (int kk = 0; kk < kOzBK / 32; ++kk) {
+                umma_i8_pair(d, sdesc_sw128(a + kk * 32, 16, 1024), sdesc_sw128(b + kk * 32, 16, 1024), kOzPairIdesc,
+                             first ? 0u : 1u);
+                first = false;
+              }
+              any = true;
+              tc_commit_pair(&empty[st], 3);
+              if (++st == kOzPairStages) {
+                st = 0;
+                ph ^= 1u;
+              }
+            }
+          if (!ok) break;
+          tc_commit_pair(&tfull[buf], 3);
+        }
+      }
+      if (!ok && any) {
+        tc_commit_pair(drain, 1);
+        const uint64_t t0 = globaltimer_ns();
+        while (!mbar_try_wait(drain, 0)) {
+          if (globaltimer_ns() - t0 > 1000000000ull) {
+            if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
+            break;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue (both CTAs)
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    const OzEpi ep = oz_epi(args);
+    int it = 0;
+    bool ok = true;
+    for (int t = pair; t < args.num_tiles && ok; t += npairs) {
+      const int4 tile = args.tiles[t];
+      const double beta = (tile.z & kOzAccumulate) ? 1.0 : args.beta;
+      const long long gi = (long long)tile.x + 128 * (int)rank + row;
+      const bool row_ok = gi < ep.M;
+      const int ei = row_ok ? oz_row_exp(ep.eA, gi) : 0;
+      if (tile.w <= (tile.z & (kOzAccumulate - 1))) {
+        if (row_ok) oz_scale_row(ep, gi, tile.y, beta);
+        continue;
+      }
+      for (int L = 2; L <= S + 1; ++L, ++it) {
+        const int buf = it & 1;
+        const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+        if (!mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * kOzBN);
+#pragma unroll 1
+        for (int c0 = 0; c0 < kOzBN; c0 += 32) {
+          int v[32];
+          tmem_ld32_s32(tacc + c0, v);
+          if (c0 == kOzBN - 32) {  // this CTA's half of the accumulator is read: tell the leader
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
+          }
+          if (row_ok) oz_fold32(ep, v, gi, (long long)tile.y + c0, ei, L, beta);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // the pair's MMAs, remote arrivals and TMEM reads are over
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc_pair(tmem_base, 512);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -600,17 +869,64 @@ std::vector<int4> oz_plan(int M, int N, int tiles, KRange kr, long long K, long 
   return out;
 }
 
+// Products of at least 256 x 256 run on CTA pairs; TB_OZ_PAIR=0 in the
+// environment keeps them on single CTAs (read once; the two give
+// bit-identical results, so this only compares their speed).
+bool oz_pair_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("TB_OZ_PAIR");
+    on = (e && e[0] == '0') ? 0 : 1;
+  }
+  return on == 1;
+}
+
+// Vertically adjacent 128-row tiles of a plan merged into 256-row pair tiles.
+// A pair tile's K range spans both halves' ranges: a half's product outside
+// its own range multiplies plane values that are zero there (the slicing
+// masks triangular operands; leaf inverses store zeros above the diagonal),
+// and an empty half adds no range (its rows then fold zero products, which
+// leaves beta C).
+std::vector<int4> oz_pair_plan(const std::vector<int4>& plan, int M, int N) {
+  const long long rb = ((long long)M + 255) / 256, cb = ((long long)N + kOzBN - 1) / kOzBN;
+  std::vector<int> where((size_t)(rb * cb), -1);
+  std::vector<int4> out;
+  out.reserve(plan.size());
+  for (const int4& t : plan) {
+    int& w = where[(size_t)((long long)(t.x >> 8) * cb + t.y / kOzBN)];
+    if (w < 0) {
+      w = (int)out.size();
+      out.push_back(make_int4((t.x >> 8) << 8, t.y, t.z, t.w));
+      continue;
+    }
+    int4& m = out[w];
+    const int tz = t.z & (kOzAccumulate - 1), mz = m.z & (kOzAccumulate - 1);
+    if (t.w <= tz) continue;  // empty half
+    if (m.w <= mz) {          // only the other half's range so far: empty
+      m.z = t.z;
+      m.w = t.w;
+      continue;
+    }
+    m.z = (tz < mz ? tz : mz) | (t.z & kOzAccumulate);
+    m.w = t.w > m.w ? t.w : m.w;
+  }
+  return out;
+}
+
 tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_mod, const std::vector<int4>& plan,
                     int M, int N, int tri, double alpha, double* C, long long ldc, double beta, int S, double flops,
                     int raw_level, int* raw_out, long long ld_raw, cudaStream_t st) {
   if (plan.empty()) return TB_SUCCESS;
+  const bool pair = M >= 256 && N >= 256 && oz_pair_enabled();
   OzArgs g;
   memset(&g, 0, sizeof(g));
   TB_TRY(make_q_map(&g.mapA, a.Q, a.ldq, a.rows, S, kOzBM));
-  TB_TRY(make_q_map(&g.mapB, b.Q, b.ldq, b.rows, S, kOzBN));
-  g.tiles = upload_tiles(plan, st);
+  TB_TRY(make_q_map(&g.mapB, b.Q, b.ldq, b.rows, S, pair ? 128 : kOzBN));
+  const std::vector<int4> pair_plan = pair ? oz_pair_plan(plan, M, N) : std::vector<int4>();
+  const std::vector<int4>& tiles = pair ? pair_plan : plan;
+  g.tiles = upload_tiles(tiles, st);
   if (!g.tiles) return TB_ERROR_ALLOC;
-  g.num_tiles = (int)plan.size();
+  g.num_tiles = (int)tiles.size();
   g.S = S;
   g.kb_shift = kb_shift;
   g.kb_mod = kb_mod;
@@ -632,11 +948,18 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
   cudaGetDevice(&dev);
   if (dev < 64 && !attr[dev]) {
     TB_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzSmem));
+    TB_CUDA_TRY(cudaFuncSetAttribute(oz_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzPairSmem));
     attr[dev] = true;
   }
-  const int grid = g.num_tiles < sm_count() ? g.num_tiles : sm_count();
   void* tok = prof_begin(st);
-  oz_gemm_kernel<<<grid, 192, kOzSmem, st>>>(g);
+  if (pair) {
+    const int pairs_max = sm_count() / 2;
+    const int pairs = g.num_tiles < pairs_max ? g.num_tiles : pairs_max;
+    oz_pair_kernel<<<2 * pairs, 192, kOzPairSmem, st>>>(g);
+  } else {
+    const int grid = g.num_tiles < sm_count() ? g.num_tiles : sm_count();
+    oz_gemm_kernel<<<grid, 192, kOzSmem, st>>>(g);
+  }
   TB_CUDA_TRY(cudaGetLastError());
   prof_end(tok, st, flops);
   note_launch();
