@@ -35,9 +35,10 @@ cudaStream_t current_stream();
 cudaStream_t aux_stream();
 // Device scratch owned by the library (grow-only, per device and slot).
 // Slot 0 serves the routines' own scratch; slot 1 the host-memory entry
-// points' staging buffers, which live across routine calls. Returns nullptr
-// on allocation failure. Growing synchronises the device.
-constexpr int kPoolSlots = 2;
+// points' staging buffers, which live across routine calls; slot 2 the Ozaki
+// engine's per-level INT32 sums. Returns nullptr on allocation failure.
+// Growing synchronises the device.
+constexpr int kPoolSlots = 3;
 void* pool_get(size_t bytes, int slot = 0);
 // Device error word used by bounded waits inside kernels (per device).
 int* device_error_word();

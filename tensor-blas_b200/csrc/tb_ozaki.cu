@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(256) oz_slice_cols_kernel(long long rows, long
 // as 1 for this tile (a later K chunk of a product whose first chunk
 // already applied beta).
 constexpr int kOzAccumulate = 1 << 30;
+constexpr int kOzRawAll = 1;
 
 struct OzArgs {
   CUtensorMap mapA;  // QA planes, box {128, 128, 1}
@@ -202,9 +203,12 @@ struct OzArgs {
   double alpha, beta;
   const int* eA;
   const int* eB;
-  int raw_level;  // >= 2: write P_raw_level (int32) to raw_out instead of folding into C
+  // 0: fold every level into C; kOzRawAll: write every level's INT32 sums to
+  // raw_out + (L - 2) raw_plane (oz_fold_kernel folds them afterwards); >= 2:
+  // write only P_raw_level to raw_out (a checking aid)
+  int raw_level;
   int* raw_out;
-  long long ld_raw;
+  long long ld_raw, raw_plane;
   int* err;
 };
 
@@ -225,7 +229,7 @@ __device__ __forceinline__ double pow2i(int e) {
 struct OzEpi {
   double* C;
   int* raw_out;
-  long long ldc, ld_raw;
+  long long ldc, ld_raw, raw_plane;
   const int* eA;
   const int* eB;
   double alpha;
@@ -233,7 +237,7 @@ struct OzEpi {
 };
 
 __device__ __forceinline__ OzEpi oz_epi(const OzArgs& a) {
-  return OzEpi{a.C, a.raw_out, a.ldc, a.ld_raw, a.eA, a.eB, a.alpha, a.N, a.M, a.tri, a.raw_level};
+  return OzEpi{a.C, a.raw_out, a.ldc, a.ld_raw, a.raw_plane, a.eA, a.eB, a.alpha, a.N, a.M, a.tri, a.raw_level};
 }
 
 // A row's slicing exponent (all-zero rows keep a very negative one and were
@@ -241,9 +245,10 @@ __device__ __forceinline__ OzEpi oz_epi(const OzArgs& a) {
 __device__ __forceinline__ int oz_row_exp(const int* e, long long i) { return e[i] < -1000 ? 0 : e[i]; }
 
 // Empty product (K range outside the operands' support): C(gi, n0 + j) =
-// beta C(gi, n0 + j) for the tile's written columns.
+// beta C(gi, n0 + j) for the tile's written columns (oz_fold_kernel does it
+// when the levels are folded there).
 __device__ __forceinline__ void oz_scale_row(const OzEpi& ep, long long gi, long long n0, double beta) {
-  if (beta == 1.0 || ep.raw_level >= 2) return;
+  if (beta == 1.0 || ep.raw_level != 0) return;
   for (int j = 0; j < kOzBN; ++j) {
     const long long gj = n0 + j;
     if (gj < ep.N && (ep.tri == 0 || (ep.tri == 1 ? gj <= gi : gj >= gi))) {
@@ -255,7 +260,7 @@ __device__ __forceinline__ void oz_scale_row(const OzEpi& ep, long long gi, long
 
 // Level L's INT32 sums v of row gi at columns g0 + [0, 32): each folded into
 // C with one rounding, C = alpha 2^(ei + ej - 7L) v + (L == 2 ? beta C : C),
-// or written as they are when L is the requested raw level.
+// or written as they are (every level, or only the requested one).
 __device__ __forceinline__ void oz_fold32(const OzEpi& ep, const int* v, long long gi, long long g0, int ei, int L,
                                           double beta) {
   // the columns g0 + [lo, hi) of this row that are written: one range per
@@ -264,11 +269,12 @@ __device__ __forceinline__ void oz_fold32(const OzEpi& ep, const int* v, long lo
   if (ep.tri == 1) hl = min(hl, gi - g0 + 1);  // gj <= gi
   if (ep.tri == 2) ll = gi - g0;               // gj >= gi
   const int hi = (int)max(0LL, min(32LL, hl)), lo = (int)max(0LL, min(32LL, ll));
-  if (ep.raw_level >= 2) {
-    if (L != ep.raw_level) return;
+  if (ep.raw_level != 0) {
+    if (ep.raw_level != kOzRawAll && L != ep.raw_level) return;
+    int* const out = ep.raw_out + (ep.raw_level == kOzRawAll ? (long long)(L - 2) * ep.raw_plane : 0LL);
 #pragma unroll
     for (int j = 0; j < 32; ++j)
-      if (j >= lo && j < hi) ep.raw_out[gi + (g0 + j) * ep.ld_raw] = v[j];
+      if (j >= lo && j < hi) out[gi + (g0 + j) * ep.ld_raw] = v[j];
     return;
   }
   double old[32];
@@ -718,6 +724,52 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1) oz_pair_kern
   if (warp == 1) tmem_dealloc_pair(tmem_base, 512);
 }
 
+// ---------------------------------------------------------------- level fold
+// FP64 instructions issued while an SM's tensor core runs tcgen05 MMAs wait
+// until the MMAs pause: folded in the GEMM's epilogue, a level's fold ended
+// only when the next level's MMAs did, and the MMA issuer then waited 30-70
+// us per level for its accumulator (measured with %globaltimer stamps). So
+// large products write every level's exact INT32 sums to a workspace and this
+// kernel folds them afterwards with the same arithmetic, in the same order,
+// as the epilogue fold (results are bit-identical):
+//   c = beta (beta != 0 ? C : 0); c = fma(alpha 2^(ei + ej - 7L), P_L, c),
+//   L = 2 .. S + 1.
+// One block per tile of the GEMM's tile list (tile_rows rows x 256 columns);
+// a thread takes one row and every (256 / tile_rows)-th column, so a warp's
+// loads and stores cover 32 consecutive rows of a column.
+__global__ void __launch_bounds__(256) oz_fold_kernel(const int4* __restrict__ tiles, int tile_rows, int M, int N,
+                                                      int tri, int S, double alpha, double beta, double* C,
+                                                      long long ldc, const int* __restrict__ eA,
+                                                      const int* __restrict__ eB, const int* __restrict__ raw,
+                                                      long long ld_raw, long long plane) {
+  const int4 tile = tiles[blockIdx.x];
+  const double b = (tile.z & kOzAccumulate) ? 1.0 : beta;
+  const bool empty = tile.w <= (tile.z & (kOzAccumulate - 1));
+  const long long i = (long long)tile.x + (int)(threadIdx.x % tile_rows);
+  if (i >= M) return;
+  const int ei = oz_row_exp(eA, i);
+  for (int c = (int)(threadIdx.x / tile_rows); c < kOzBN; c += 256 / tile_rows) {
+    const long long j = (long long)tile.y + c;
+    if (j >= N || (tri == 1 && j > i)) break;  // columns only grow
+    if (tri == 2 && j < i) continue;
+    double* const cp = C + i + j * ldc;
+    if (empty) {
+      if (b != 1.0) *cp = b == 0.0 ? 0.0 : b * *cp;
+      continue;
+    }
+    const int ej = oz_row_exp(eB, j);
+    const int* const p = raw + i + j * ld_raw;
+    int v[kOzMaxSlices];
+#pragma unroll
+    for (int l = 0; l < kOzMaxSlices; ++l) v[l] = l < S ? p[l * plane] : 0;
+    double acc = b * (b != 0.0 ? *cp : 0.0);
+#pragma unroll
+    for (int l = 0; l < kOzMaxSlices; ++l)
+      if (l < S) acc = fma(alpha * pow2i(ei + ej - 7 * (l + 2)), (double)v[l], acc);
+    *cp = acc;
+  }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -881,6 +933,20 @@ bool oz_pair_enabled() {
   return on == 1;
 }
 
+// Products fold their levels after the GEMM (oz_fold_kernel) when the INT32
+// level sums fit in kOzLevelBytesMax of workspace; TB_OZ_FOLD=fused in the
+// environment folds them in the GEMM's epilogue instead (read once; the two
+// give bit-identical results).
+constexpr double kOzLevelBytesMax = 32.0 * (1ull << 30);
+bool oz_split_fold_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("TB_OZ_FOLD");
+    on = (e && strcmp(e, "fused") == 0) ? 0 : 1;
+  }
+  return on == 1;
+}
+
 // Vertically adjacent 128-row tiles of a plan merged into 256-row pair tiles.
 // A pair tile's K range spans both halves' ranges: a half's product outside
 // its own range multiplies plane values that are zero there (the slicing
@@ -918,6 +984,11 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
                     int raw_level, int* raw_out, long long ld_raw, cudaStream_t st) {
   if (plan.empty()) return TB_SUCCESS;
   const bool pair = M >= 256 && N >= 256 && oz_pair_enabled();
+  // fold after the GEMM (oz_fold_kernel) when the levels' workspace fits
+  const long long ld_r = round_up((long long)M, 32), plane = ld_r * (long long)N;
+  int* levels = nullptr;
+  if (raw_level == 0 && oz_split_fold_enabled() && (double)S * plane * 4.0 <= kOzLevelBytesMax)
+    levels = static_cast<int*>(pool_get((size_t)S * (size_t)plane * 4, 2));
   OzArgs g;
   memset(&g, 0, sizeof(g));
   TB_TRY(make_q_map(&g.mapA, a.Q, a.ldq, a.rows, S, kOzBM));
@@ -939,9 +1010,10 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
   g.beta = beta;
   g.eA = a.e;
   g.eB = b.e;
-  g.raw_level = raw_level;
-  g.raw_out = raw_out;
-  g.ld_raw = ld_raw;
+  g.raw_level = levels ? kOzRawAll : raw_level;
+  g.raw_out = levels ? levels : raw_out;
+  g.ld_raw = levels ? ld_r : ld_raw;
+  g.raw_plane = plane;
   g.err = device_error_word();
   static bool attr[64] = {false};
   int dev = 0;
@@ -961,6 +1033,12 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
     oz_gemm_kernel<<<grid, 192, kOzSmem, st>>>(g);
   }
   TB_CUDA_TRY(cudaGetLastError());
+  if (levels) {
+    note_launch();
+    oz_fold_kernel<<<g.num_tiles, 256, 0, st>>>(g.tiles, pair ? 256 : kOzBM, M, N, tri, S, alpha, beta, C, ldc, g.eA,
+                                                g.eB, levels, ld_r, plane);
+    TB_CUDA_TRY(cudaGetLastError());
+  }
   prof_end(tok, st, flops);
   note_launch();
   return TB_SUCCESS;

@@ -19,8 +19,8 @@ cudaStream_t g_stream = nullptr;
 
 constexpr int kMaxDevices = 64;
 struct DeviceState {
-  void* pool[kPoolSlots] = {nullptr, nullptr};
-  size_t pool_bytes[kPoolSlots] = {0, 0};
+  void* pool[kPoolSlots] = {};
+  size_t pool_bytes[kPoolSlots] = {};
   int* err = nullptr;
   int sms = 0;
   cudaStream_t aux = nullptr;

@@ -1,12 +1,14 @@
 """Ozaki products of at least 256 x 256 run on CTA pairs (256 x 256 tiles on
-two SMs). Their INT32 level sums are exact and their fold is the same FP64
-arithmetic in the same order as the single-CTA kernel's, so every FP64
-routine must give bit-identical results with the pair engine on and off.
-The choice is read once per process (TB_OZ_PAIR), so each setting runs in
-its own subprocess. The cases cover ragged edges (rows and columns past a
+two SMs), and large products fold their levels in a kernel of their own
+after the GEMM instead of in its epilogue. The INT32 level sums are exact
+and every fold is the same FP64 arithmetic in the same order, so every FP64
+routine must give bit-identical results with the pair engine on and off and
+with either fold. The choices are read once per process (TB_OZ_PAIR,
+TB_OZ_FOLD), so each setting runs in its own subprocess. The cases cover ragged edges (rows and columns past a
 pair tile's halves), both triangles, transposes, K chunks with accumulation,
-SYR2K's shifted K blocks, triangular K ranges (TRMM, TRSM leaves) and the
-raw INT32 level sums."""
+SYR2K's shifted K blocks, triangular K ranges (TRMM, TRSM leaves), rows
+whose fold scales leave the normal double range, and the raw INT32 level
+sums."""
 import os
 import subprocess
 import sys
@@ -50,6 +52,12 @@ for uplo, trans, n, k, S in [(b"L", b"N", 600, 700, 8), (b"U", b"T", 520, 300, 1
     dA, dC = dev(A), dev(g.standard_normal((n, n)))
     ok(lib.tb_dsyrk_ozaki(uplo, trans, n, k, -0.75, dA.data_ptr(), A.shape[0], 0.5, dC.data_ptr(), n, S))
     digest(dC)
+# rows of very different magnitudes: some fold scales leave the normal range
+n, k = 300, 200
+A = wide(n, k, 0.5) * np.exp2(g.integers(-600, 500, n)).reshape(n, 1)
+dA, dC = dev(A), dev(np.zeros((n, n)))
+ok(lib.tb_dsyrk_ozaki(b"L", b"N", n, k, 1.0, dA.data_ptr(), n, 0.0, dC.data_ptr(), n, 8))
+digest(dC)
 for n, k, S in [(384, 257, 10), (700, 129, 7)]:
     A, B = wide(n, k), wide(n, k)
     dA, dB, dC = dev(A), dev(B), dev(g.standard_normal((n, n)))
@@ -77,18 +85,21 @@ print(" ".join(out))
 """
 
 
-def _digests(pair):
-    env = dict(os.environ, TB_OZ_PAIR=str(pair))
+def _digests(pair, fold):
+    env = dict(os.environ, TB_OZ_PAIR=str(pair), TB_OZ_FOLD=fold)
     out = subprocess.run([sys.executable, "-c", SCRIPT, os.path.join(ROOT, "tensor-blas_b200", "python")], env=env,
                          capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     return out.stdout.strip().splitlines()[-1].split()
 
 
-def test_pair_engine_is_bit_identical():
-    single, pair = _digests(0), _digests(1)
-    assert len(single) == len(pair) == 15
-    names = ["syrk L N", "syrk U T", "syrk K chunks", "syr2k", "syr2k k 129", "trmm L", "trmm U", "trsm R", "trsm L"]
+def test_engines_and_folds_are_bit_identical():
+    base = _digests(0, "fused")
+    assert len(base) == 16
+    names = ["syrk L N", "syrk U T", "syrk K chunks", "syrk wide exponents", "syr2k", "syr2k k 129", "trmm L", "trmm U",
+             "trsm R", "trsm L"]
     names += [f"level {L}" for L in range(2, 8)]
-    diff = [nm for nm, a, b in zip(names, single, pair) if a != b]
-    assert not diff, diff
+    for pair, fold in ((1, "fused"), (0, "split"), (1, "split")):
+        other = _digests(pair, fold)
+        diff = [nm for nm, a, b in zip(names, base, other) if a != b]
+        assert not diff, (pair, fold, diff)
