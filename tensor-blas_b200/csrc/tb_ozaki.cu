@@ -734,21 +734,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1) oz_pair_kern
 // as the epilogue fold (results are bit-identical):
 //   c = beta (beta != 0 ? C : 0); c = fma(alpha 2^(ei + ej - 7L), P_L, c),
 //   L = 2 .. S + 1.
-// One block per tile of the GEMM's tile list (tile_rows rows x 256 columns);
-// a thread takes one row and every (256 / tile_rows)-th column, so a warp's
-// loads and stores cover 32 consecutive rows of a column.
+// One block per 32-column slab of a tile of the GEMM's tile list (tile_rows
+// rows; eight slabs per tile, so even a one-wave GEMM gives every SM several
+// blocks); a thread takes one row and every (256 / tile_rows)-th column of
+// the slab, so a warp's loads and stores cover 32 consecutive rows of a
+// column.
+constexpr int kOzFoldSlab = 32;
 __global__ void __launch_bounds__(256) oz_fold_kernel(const int4* __restrict__ tiles, int tile_rows, int M, int N,
                                                       int tri, int S, double alpha, double beta, double* C,
                                                       long long ldc, const int* __restrict__ eA,
                                                       const int* __restrict__ eB, const int* __restrict__ raw,
                                                       long long ld_raw, long long plane) {
-  const int4 tile = tiles[blockIdx.x];
+  const int4 tile = tiles[blockIdx.x / (kOzBN / kOzFoldSlab)];
+  const int c0 = (int)(blockIdx.x % (kOzBN / kOzFoldSlab)) * kOzFoldSlab;
   const double b = (tile.z & kOzAccumulate) ? 1.0 : beta;
   const bool empty = tile.w <= (tile.z & (kOzAccumulate - 1));
   const long long i = (long long)tile.x + (int)(threadIdx.x % tile_rows);
   if (i >= M) return;
   const int ei = oz_row_exp(eA, i);
-  for (int c = (int)(threadIdx.x / tile_rows); c < kOzBN; c += 256 / tile_rows) {
+  for (int c = c0 + (int)(threadIdx.x / tile_rows); c < c0 + kOzFoldSlab; c += 256 / tile_rows) {
     const long long j = (long long)tile.y + c;
     if (j >= N || (tri == 1 && j > i)) break;  // columns only grow
     if (tri == 2 && j < i) continue;
@@ -1035,8 +1039,9 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
   TB_CUDA_TRY(cudaGetLastError());
   if (levels) {
     note_launch();
-    oz_fold_kernel<<<g.num_tiles, 256, 0, st>>>(g.tiles, pair ? 256 : kOzBM, M, N, tri, S, alpha, beta, C, ldc, g.eA,
-                                                g.eB, levels, ld_r, plane);
+    oz_fold_kernel<<<g.num_tiles * (kOzBN / kOzFoldSlab), 256, 0, st>>>(g.tiles, pair ? 256 : kOzBM, M, N, tri, S,
+                                                                       alpha, beta, C, ldc, g.eA, g.eB, levels, ld_r,
+                                                                       plane);
     TB_CUDA_TRY(cudaGetLastError());
   }
   prof_end(tok, st, flops);
