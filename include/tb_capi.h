@@ -216,6 +216,12 @@ TB_API tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, float a
  * 7 * slices exceeds 53 bits plus the in-row exponent spread. The reference's
  * tc_ozimmu_* drivers run native FP64 cuBLAS GEMMs instead.
  *
+ * Scratch: the slice planes, plus each product's INT32 level sums
+ * (4 * slices bytes per element of the output's bounding rectangle) when
+ * they fit in 32 GB; the levels are then folded into C by a second kernel
+ * (TB_OZ_FOLD=fused in the environment folds them inside the GEMM instead,
+ * with the same results).
+ *
  * SYRK: C = alpha op(A) op(A)^T + beta C, the `uplo` triangle ('L' or 'U');
  * A n x k ('N') or k x n ('T'). Replaces tc_ozimmu_syrk
  * (BLAS/tc_ozimmu_syrk.cu:108-143).
