@@ -14,9 +14,11 @@
 // keeping levels L = 2..S+1. Each P_L is computed EXACTLY on tcgen05.mma
 // kind::i8 with INT32 accumulation in TMEM (|P_L| <= (L-1) * k * 127^2 <
 // 2^31 for k <= 8192 and S <= 14 — checked on the host), then folded into
-// FP64 C by the epilogue: C += alpha 2^(e_i+e_j-7L) P_L (one FP64 rounding per
-// level). Slices are stored K-major, one int8 plane per slice, so a single
-// 3-D tensor map (k, row, slice) feeds every pair.
+// FP64 C: C += alpha 2^(e_i+e_j-7L) P_L (one FP64 rounding per level), by a
+// kernel of its own after the GEMM (which stores the level sums) or, when
+// their workspace does not fit, by the GEMM's epilogue. Slices are stored
+// K-major, one int8 plane per slice, so a single 3-D tensor map (k, row,
+// slice) feeds every pair.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -482,7 +484,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(const __grid_constant__
 // planes and rows tile.y + 128 r of the B planes into its own shared memory;
 // the leader (r = 0) issues the 256-row MMA, which reads both CTAs' halves,
 // and each CTA's TMEM receives its 128 accumulator rows, which its own
-// epilogue folds. Per SM one 128-deep K block moves 32 KB from L2 instead of
+// epilogue stores or folds. Per SM one 128-deep K block moves 32 KB from L2 instead of
 // the single-CTA tile's 48 KB for the same MMA work. The level sums are the
 // same exact integers and the fold the same arithmetic, so the results are
 // bit-identical to the single-CTA kernel's.
