@@ -13,6 +13,13 @@ each with its error against an FP64 evaluation on the host.
 
 N > 1 runs independent replicas, one per GPU (the path has no exchange step);
 value = all ranks' flops / max-over-ranks device time.
+
+--impl reference runs the reference library (built from its sources into
+oracle/_ref by oracle/Makefile) on the same seeded inputs and prints its line
+with the same config; it also records sampled entries of its SYRK and TRSM
+outputs in .bench_reference_samples.npz, from which a later run of this arm on
+the same machine reports its agreement with the reference
+(agreement_vs_reference).
 """
 import argparse
 import datetime
@@ -136,6 +143,25 @@ class Clocks:
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+SAMPLES = os.path.join(ROOT, ".bench_reference_samples.npz")
+
+
+def workload(n, nb_syrk, nb_trsm):
+    """The config both arms report: the same matrices, shapes and flops."""
+    return {"workload": f"plain SYRK n=k={n} nb={nb_syrk} + plain TRSM m=n={n} nb={nb_trsm} (lower, non-unit, "
+                        f"{n} right-hand sides) per step", "n": n, "precision": "plain",
+            "l2": "inputs larger than L2 (1 GiB per matrix)", "parallelism": "replicas x1"}
+
+
+def sample_indices(n):
+    """Entries compared with the reference: 4096 lower SYRK entries and 32
+    rows of the right-side TRSM solution X (X A^T = B)."""
+    g = np.random.Generator(np.random.PCG64(7))
+    i, j = g.integers(0, n, 4096), g.integers(0, n, 4096)
+    rows = np.random.Generator(np.random.PCG64(8)).integers(0, n, 32)
+    return np.maximum(i, j), np.minimum(i, j), rows
 
 
 def measured_peaks():
@@ -273,8 +299,26 @@ def run_mine(args, world, rank, local):
         e = fp64_errors(n, A, C, T, B0, Bw)["trsm"] if rank == 0 else None
         trsm_only[name] = {"ms": ms_t, "tflops": float(n) ** 3 / (ms_t * 1e-3) / 1e12, "errors_vs_fp64": e}
 
+    ms_syrk = _median_ms(lambda: TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN), 5)
+    # per-kernel rooflines: the step's two GEMM kernels timed on their own
+    # (event-timed launches between tb_profile_begin / end; 5 calls each)
+    kernels = {}
+    for name, call in (("syrk", lambda: TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN)),
+                       ("trsm", lambda: TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, TB.PLAIN))):
+        call()
+        TB.synchronize()
+        TB.lib.tb_profile_begin()
+        for _ in range(5):
+            Bw.copy_(B0)
+            call()
+        torch.cuda.synchronize()
+        ms, fl, cnt = TB.ctypes.c_double(), TB.ctypes.c_double(), TB.ctypes.c_long()
+        TB.lib.tb_profile_end(TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
+        kernels[name] = (ms.value / 5, fl.value / 5, cnt.value / 5)
+
     value = world * args.steps * flops_step / (ms_plain * 1e-3) / 1e12
     value_split = world * args.steps * flops_step / (ms_split * 1e-3) / 1e12
+    agreement = agreement_vs_reference(TB, args, A, C, T, B0, Bw) if rank == 0 else None
 
     # ---- end to end through the public host-memory API (page-locked buffers):
     # every byte of the step's inputs crosses PCIe inside the timed region
@@ -322,25 +366,36 @@ def run_mine(args, world, rank, local):
         return None
     burst, sustained, peak_src = measured_peaks()
     gemm_ms, gemm_flops, gemm_launches = prof
-    achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
-    tr = traffic_summary()
-    roof = {"bound": "tensor", "kernel": "tb::gemm_kernel / gemm_pair_kernel (all GEMM-engine launches of the step)",
-            "achieved": achieved, "achieved_note": "algorithmic flops of the launches / the union of their "
-            "event-timed intervals (the TRSM halves' launches on two streams overlap)",
-            "peak": sustained, "unit": "TFLOP/s",
-            "frac": (achieved / sustained) if achieved and sustained else None,
-            "peak_source": f"{peak_src} bf16_tflops_sustained (burst {burst})",
-            "launches_per_step": gemm_launches / args.steps,
-            "traffic": tr.get("bytes_per_launch") if tr else None,
-            "traffic_note": tr.get("note") if tr else "no ncu traffic summary committed"}
+    tr = traffic_summary() or {}
+    names = {"syrk": "tb::gemm_pair_kernel (plain SYRK: one launch over the lower-triangle tile list)",
+             "trsm": "tb::trsm_dag_kernel (plain TRSM: one persistent launch for every leaf product and update)"}
+    per_kernel = {}
+    for key, (ms, fl, cnt) in kernels.items():
+        ach = fl / (ms * 1e-3) / 1e12 if ms > 0 else None
+        t = tr.get(key, {})
+        per_kernel[key] = {"bound": "tensor", "kernel": names[key], "achieved": ach, "peak": burst,
+                           "unit": "TFLOP/s", "frac": (ach / burst) if ach and burst else None,
+                           "ms_per_launch": ms / cnt if cnt else None, "launches_per_call": cnt,
+                           "flops_per_launch": fl / cnt if cnt else None,
+                           "traffic": t.get("bytes_per_launch"), "traffic_note": t.get("note")}
+    dominant = max(per_kernel, key=lambda k: kernels[k][0])
+    roof = dict(per_kernel[dominant])
+    roof.update({"peak_source": f"{peak_src} bf16_tflops (burst: each kernel timed alone; sustained {sustained})",
+                 "achieved_note": "algorithmic flops per launch (nominal BLAS3 counts of the tiles' products) / "
+                                  "the launch's CUDA-event duration, 5 calls",
+                 "step_gemm": {"achieved": gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None,
+                               "launches_per_step": gemm_launches / args.steps,
+                               "note": "all GEMM launches of the timed step: flops / union of their intervals"},
+                 "other_kernel": per_kernel[[k for k in per_kernel if k != dominant][0]]})
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_plain / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f16 operands, f32 accumulate", "data": "synthetic (seeded)",
-        "config": {"workload": f"plain SYRK n=k={n} nb={args.nb_syrk} + plain TRSM left/lower/N m=n={n} "
-                               f"nb={args.nb_trsm} per step", "n": n, "precision": "plain",
-                   "l2": "inputs larger than L2 (1 GiB per matrix)", "parallelism": f"replicas x{world}"},
+        "config": dict(workload(n, args.nb_syrk, args.nb_trsm), parallelism=f"replicas x{world}"),
+        "detail": {"syrk_ms": ms_syrk, "trsm_ms": trsm_only["plain"]["ms"],
+                   "timing": "median per call, CUDA events, device-resident", "trsm_side": "left (A X = B)"},
         "errors_vs_fp64": err_plain,
+        "agreement_vs_reference": agreement,
         "chosen": {"precision": "split (FP16 hi + scaled lo, 3 products, RN folds)", "value": value_split,
                    "ms_per_step": ms_split / args.steps, "ratio_vs_plain": value_split / value,
                    "errors_vs_fp64": err_split},
@@ -371,6 +426,35 @@ def run_mine(args, world, rank, local):
     return line
 
 
+def agreement_vs_reference(TB, args, A, C, T, B0, Bw):
+    """Normwise and largest elementwise relative difference between this
+    library's plain outputs and the reference's own tc_syrk / tc_trsm outputs
+    on the same seeded inputs (sampled entries the reference arm recorded in
+    .bench_reference_samples.npz). TRSM is compared in the reference's form,
+    X A^T = B, solved here with tb_strsm('R')."""
+    n = args.n
+    if not os.path.exists(SAMPLES):
+        return {"status": "no reference samples: run bench.py --impl reference first on this machine"}
+    z = np.load(SAMPLES)
+    if int(z["n"]) != n or int(z["nb_syrk"]) != args.nb_syrk or int(z["nb_trsm"]) != args.nb_trsm:
+        return {"status": "reference samples are for another configuration"}
+    lo, hi, rows = sample_indices(n)
+    Bw.copy_(B0)
+    TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN)
+    TB.strsm("R", T, Bw, n, n, n, n, args.nb_trsm, TB.PLAIN)
+    TB.synchronize()
+    mine_s = C.cpu().numpy()[hi, lo].astype(np.float64)
+    mine_t = Bw[:, torch.from_numpy(rows).cuda()].cpu().numpy().T.astype(np.float64)   # rows of X
+    out = {"sample": "4096 lower SYRK entries; 32 rows of X (X A^T = B)",
+           "reference": "tc_syrk / tc_trsm built from the reference's sources (oracle/_ref)"}
+    for name, mine, ref in (("syrk", mine_s, z["syrk"]), ("trsm", mine_t, z["trsm_rows"])):
+        d = np.abs(mine - ref)
+        out[name] = {"norm_rel": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+                     "max_rel": float(np.max(d / np.maximum(np.abs(ref), 1e-30)))}
+    out["reference_errors_vs_fp64"] = {"syrk": float(z["err_syrk"]), "trsm": float(z["err_trsm"])}
+    return out
+
+
 def _median_ms(fn, reps, prep=None):
     fn()
     torch.cuda.synchronize()
@@ -387,16 +471,13 @@ def _median_ms(fn, reps, prep=None):
     return float(np.median(out))
 
 
-def blas3_config(TB, ref_lib):
+def blas3_config(TB):
     """SYR2K n=16384 k=4096, TRMM left/upper m=n=16384 and SYMM left/lower
     m=n=16384 with entries N(0,1) * 2^U(-8,8): plain, split and FP8-e4m3
-    (per-128x128-block scaled), each with a sampled FP64 error, beside the reference's tc_syr2k / tc_trmm / tc_symm
-    on inputs of the same shape (its TRMM is lower-only; the flops are the
-    same). Flop conventions: SYR2K 2 n^2 k, TRMM m^2 n, SYMM 2 m^2 n."""
-    import ctypes
-
+    (per-128x128-block scaled), each with a sampled FP64 error (the
+    reference's tc_syr2k / tc_trmm / tc_symm are timed by the reference arm
+    on inputs of the same shape). Flop conventions: SYR2K 2 n^2 k, TRMM m^2 n, SYMM 2 m^2 n."""
     lib = TB.lib
-    P = ctypes.c_void_p
     gen = torch.Generator(device="cuda")
     gen.manual_seed(99)
     rng = np.random.Generator(np.random.PCG64(99))
@@ -427,11 +508,6 @@ def blas3_config(TB, ref_lib):
         ms = _median_ms(run, 5)
         got = C.cpu().numpy()[hi, lo].astype(np.float64)
         entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "errors_vs_fp64": err(got, ref)}
-    if ref_lib is not None:
-        t = ref_lib.ref_time_syr2k(n, k, 256, A.cpu().numpy().ctypes.data_as(P), B.cpu().numpy().ctypes.data_as(P),
-                                   1, 3)
-        entry["reference_plain_ms"] = t
-        entry["speedup_plain_vs_reference"] = t / entry["plain"]["ms"] if t > 0 else None
     out["syr2k"] = entry
     del A, B, C, Ah, Bh
     torch.cuda.empty_cache()
@@ -451,11 +527,6 @@ def blas3_config(TB, ref_lib):
         ms = _median_ms(run, 5)
         got = C.cpu().numpy()[j, i].astype(np.float64)
         entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "errors_vs_fp64": err(got, ref)}
-    if ref_lib is not None:
-        t = ref_lib.ref_time_trmm(m, n, 256, An.ctypes.data_as(P), Bn.ctypes.data_as(P), 1, 3)
-        entry["reference_plain_ms"] = t
-        entry["reference_note"] = "reference tc_trmm is lower-only: timed on a lower operand of the same size"
-        entry["speedup_plain_vs_reference"] = t / entry["plain"]["ms"] if t > 0 else None
     out["trmm"] = entry
     # SYMM lower: C(i, j) = sum_p A(i, p) B(p, j), A(i, p) = A(max, min) from the lower triangle
     ref = []
@@ -470,10 +541,6 @@ def blas3_config(TB, ref_lib):
         ms = _median_ms(run, 5)
         got = C.cpu().numpy()[j, i].astype(np.float64)
         entry[name] = {"ms": ms, "tflops": entry["flops"] / (ms * 1e-3) / 1e12, "errors_vs_fp64": err(got, ref)}
-    if ref_lib is not None:
-        t = ref_lib.ref_time_symm(m, n, An.ctypes.data_as(P), Bn.ctypes.data_as(P), 1, 3)
-        entry["reference_plain_ms"] = t
-        entry["speedup_plain_vs_reference"] = t / entry["plain"]["ms"] if t > 0 else None
     out["symm"] = entry
     del A, B, C
     torch.cuda.empty_cache()
@@ -481,11 +548,12 @@ def blas3_config(TB, ref_lib):
 
 
 def other_configs(TB):
-    """The other configurations of the hot path, one measurement each:
-    SYRK n=k=4096 (plain, the CPU-runnable case), FP64 DSYRK n=k=8192 by
-    Ozaki-INT8 vs the reference's native-FP64 tc_ozimmu_syrk, SYR2K / TRMM /
-    SYMM at 16384 vs the reference's tc_* forms, and 512 uneven
-    SYRK/TRSM instances as one grouped batch vs a per-instance plain loop."""
+    """The other configurations of the hot path, one measurement each (the
+    reference library's timings of the same configurations are in the
+    reference arm's line): SYRK n=k=4096 (plain, the CPU-runnable case), FP64
+    DSYRK n=k=8192 on the INT8 Ozaki engine with the automatic slice count,
+    SYR2K / TRMM / SYMM at 16384, and 512 uneven SYRK/TRSM instances as one
+    grouped batch vs a per-instance loop, in both precisions."""
     import ctypes
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -499,26 +567,20 @@ def other_configs(TB):
     ms = _median_ms(lambda: TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", 256, TB.PLAIN), 20)
     res["syrk_4096_plain"] = {"ms": ms, "tflops": float(n) ** 3 / (ms * 1e-3) / 1e12}
     del A, C
-    # ---- Ozaki DSYRK n = k = 8192
+    # ---- Ozaki DSYRK n = k = 8192, slices chosen by the library
     lib = TB.lib
     P, L = ctypes.c_void_p, ctypes.c_long
     lib.tb_dsyrk_ozaki.argtypes = [ctypes.c_char, ctypes.c_char, L, L, ctypes.c_double, P, L, ctypes.c_double, P, L,
                                    ctypes.c_int]
     n = k = 8192
     oz = {}
-    ref_lib = None
-    so = os.path.join(ROOT, "oracle", "_ref", "libTensorBLAS_ref.so")
-    if os.path.exists(so):
-        ref_lib = ctypes.CDLL(so)
-        ref_lib.ref_time_ozimmu_syrk.argtypes = [L, L, L, P, ctypes.c_int, ctypes.c_int]
-        ref_lib.ref_time_ozimmu_syrk.restype = ctypes.c_double
-    for phi, slices in ((0.5, 8), (2.0, 9)):
+    for phi in (0.5, 2.0):
         g = np.random.Generator(np.random.PCG64(17))
         Ah = g.standard_normal((n, k)) * np.exp(phi * g.standard_normal((n, k)))
         dA = torch.from_numpy(np.ascontiguousarray(Ah.T)).cuda()
         dC = torch.zeros(n, n, dtype=torch.float64, device="cuda")
         run = lambda: TB._check(lib.tb_dsyrk_ozaki(b"L", b"N", n, k, 1.0, dA.data_ptr(), n, 0.0,  # noqa: E731
-                                                   dC.data_ptr(), n, slices))
+                                                   dC.data_ptr(), n, 0))
         ms = _median_ms(run, 5)
         Ch = dC.cpu().numpy().T
         r = g.integers(0, n, 3000)
@@ -526,24 +588,25 @@ def other_configs(TB):
         lo, hi = np.maximum(r, c), np.minimum(r, c)
         ex = orc.syrk_extended(Ah, lo, hi)
         d = np.abs(Ch[lo, hi] - ex).astype(np.float64)
-        entry = {"slices": slices, "ms": ms, "tflops_eff": float(n) ** 2 * k / (ms * 1e-3) / 1e12,
-                 "normwise_err_vs_long_double": float(np.linalg.norm(d) / np.linalg.norm(ex.astype(np.float64)))}
-        if ref_lib is not None:
-            t_ref = ref_lib.ref_time_ozimmu_syrk(n, k, 256, np.asfortranarray(Ah).ctypes.data_as(P), 1, 3)
-            entry["reference_native_fp64_ms"] = t_ref
-            entry["speedup_vs_native_fp64"] = t_ref / ms if t_ref > 0 else None
-        oz[f"phi={phi}"] = entry
+        oz[f"phi={phi}"] = {"slices": "automatic", "ms": ms, "tflops_eff": float(n) ** 2 * k / (ms * 1e-3) / 1e12,
+                            "normwise_err_vs_long_double": float(np.linalg.norm(d) /
+                                                                 np.linalg.norm(ex.astype(np.float64)))}
         del dA, dC
     res["dsyrk_ozaki_8192"] = oz
     torch.cuda.empty_cache()
-    if ref_lib is not None:
-        for name in ("ref_time_syr2k", "ref_time_trmm"):
-            getattr(ref_lib, name).argtypes = [L, L, L, P, P, ctypes.c_int, ctypes.c_int]
-            getattr(ref_lib, name).restype = ctypes.c_double
-        ref_lib.ref_time_symm.argtypes = [L, L, P, P, ctypes.c_int, ctypes.c_int]
-        ref_lib.ref_time_symm.restype = ctypes.c_double
-    res["syr2k_trmm_symm_16384"] = blas3_config(TB, ref_lib)
-    # ---- 512 uneven instances, grouped batch (split) vs per-instance loop (plain)
+    res["syr2k_trmm_symm_16384"] = blas3_config(TB)
+    res["batched_512_uneven"] = batch_config(TB)
+    return res
+
+
+def batch_config(TB):
+    """512 independent instances, n log-uniform in [64, 2048], half SYRK
+    (k = n) and half TRSM (X A^T = B, square B): the grouped batch (a few
+    launches, replayed as one CUDA graph) against a loop of per-instance
+    calls, each in the plain and the split precision, with the worst normwise
+    error against FP64 over sampled instances."""
+    from scipy.linalg import solve_triangular
+
     g = np.random.Generator(np.random.PCG64(2025))
     ns = np.round(np.exp(g.uniform(np.log(64), np.log(2048), 512))).astype(int)
     kinds, As, BC, B0 = [], [], [], []
@@ -562,37 +625,75 @@ def other_configs(TB):
         B0.append(bc.clone())
         flops += float(m) ** 3
     restore = lambda: [b.copy_(b0) for b, b0 in zip(BC, B0)]  # noqa: E731
-    batch = TB.Batch(kinds, As, BC, precision=TB.SPLIT)
-    s = torch.cuda.Stream()
-    s.wait_stream(torch.cuda.current_stream())
-    with torch.cuda.stream(s):
-        batch.run()
-    torch.cuda.current_stream().wait_stream(s)
-    torch.cuda.synchronize()
-    graph = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(graph):
-        batch.run()
-    ms_graph = _median_ms(graph.replay, 5, restore)
+    check = list(range(0, 512, 16)) + list(range(1, 512, 16))  # 32 SYRK and 32 TRSM instances
 
-    def loop():
-        for kind, a, bc, m in zip(kinds, As, BC, ns):
-            if kind == 0:
-                TB.ssyrk(a, bc, m, m, m, m, 1.0, 0.0, "N", 256, TB.PLAIN)
+    def errors():
+        worst = {"syrk": 0.0, "trsm": 0.0}
+        for i in check:
+            Ai = As[i].cpu().numpy().T.astype(np.float64)
+            got = BC[i].cpu().numpy().T.astype(np.float64)
+            if kinds[i] == 0:
+                ref = Ai @ Ai.T
+                low = np.tril(np.ones_like(ref, dtype=bool))
+                e = float(np.linalg.norm((got - ref)[low]) / np.linalg.norm(ref[low]))
+                worst["syrk"] = max(worst["syrk"], e)
             else:
-                TB.strsm("R", a, bc, m, m, m, m, 512, TB.PLAIN)
+                b0 = B0[i].cpu().numpy().T.astype(np.float64)
+                ref = solve_triangular(Ai, b0.T, lower=True).T
+                worst["trsm"] = max(worst["trsm"], float(np.linalg.norm(got - ref) / np.linalg.norm(ref)))
+        return worst
 
-    ms_loop = _median_ms(loop, 3, restore)
-    res["batched_512_uneven"] = {"instances": 512, "flops_sum_n3": flops, "grouped_split_graph_ms": ms_graph,
-                                 "grouped_split_tflops": flops / (ms_graph * 1e-3) / 1e12,
-                                 "per_instance_plain_loop_ms": ms_loop,
-                                 "per_instance_plain_loop_tflops": flops / (ms_loop * 1e-3) / 1e12}
-    del graph
-    batch.close()
-    return res
+    out = {"instances": 512, "flops_sum_n3": flops,
+           "timing": "median of CUDA-event-timed replays (graph) / loops; B restored outside the timed region",
+           "errors": "worst normwise error vs FP64 over 32 SYRK and 32 TRSM instances"}
+    for prec, name in ((TB.PLAIN, "plain"), (TB.SPLIT, "split")):
+        batch = TB.Batch(kinds, As, BC, precision=prec)
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            batch.run()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            batch.run()
+        ms_graph = _median_ms(graph.replay, 5, restore)
+        restore()
+        graph.replay()
+        torch.cuda.synchronize()
+        e_grouped = errors()
+        l0 = TB.lib.tb_launch_count()
+        batch.run()
+        torch.cuda.synchronize()
+        launches = TB.lib.tb_launch_count() - l0
+        del graph
+        batch.close()
+
+        def loop(prec=prec):
+            for kind, a, bc, m in zip(kinds, As, BC, ns):
+                if kind == 0:
+                    TB.ssyrk(a, bc, m, m, m, m, 1.0, 0.0, "N", 256, prec)
+                else:
+                    TB.strsm("R", a, bc, m, m, m, m, 512, prec)
+
+        ms_loop = _median_ms(loop, 3, restore)
+        restore()
+        loop()
+        torch.cuda.synchronize()
+        e_loop = errors()
+        out[name] = {"grouped_graph_ms": ms_graph, "grouped_tflops": flops / (ms_graph * 1e-3) / 1e12,
+                     "grouped_launches_per_run": int(launches), "grouped_errors_vs_fp64": e_grouped,
+                     "per_instance_loop_ms": ms_loop, "per_instance_loop_tflops": flops / (ms_loop * 1e-3) / 1e12,
+                     "loop_errors_vs_fp64": e_loop, "speedup_grouped_vs_loop": ms_loop / ms_graph}
+    return out
 
 
 def run_reference(args, world, rank, local):
-    """The reference library (built from its sources into oracle/_ref/) on this B200."""
+    """The reference library (built from its sources into oracle/_ref/) on this
+    B200, on the same seeded inputs as the library's arm: tc_syrk + tc_trsm
+    (its right-side form X A^T = B: same shapes and flops), timed per call;
+    its sampled outputs and their FP64 errors, recorded for the other arm's
+    agreement check; and its timings of the other configurations."""
     if rank != 0:
         return None
     import ctypes
@@ -601,11 +702,15 @@ def run_reference(args, world, rank, local):
     if not os.path.exists(so):
         return {"impl": "reference", "unavailable": "oracle/_ref/libTensorBLAS_ref.so not built (make -C oracle)"}
     lib = ctypes.CDLL(so)
-    P = ctypes.c_void_p
-    lib.ref_time_syrk.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, P, ctypes.c_int, ctypes.c_int]
-    lib.ref_time_syrk.restype = ctypes.c_double
-    lib.ref_time_trsm.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, P, P, ctypes.c_int, ctypes.c_int]
-    lib.ref_time_trsm.restype = ctypes.c_double
+    P, L, I = ctypes.c_void_p, ctypes.c_long, ctypes.c_int
+    for name, args_t in (("ref_time_syrk", [L, L, L, P, I, I]), ("ref_time_trsm", [L, L, L, P, P, I, I]),
+                         ("ref_time_e2e", [L, L, L, P, P, P, I, I]), ("ref_time_syr2k", [L, L, L, P, P, I, I]),
+                         ("ref_time_trmm", [L, L, L, P, P, I, I]), ("ref_time_symm", [L, L, P, P, I, I]),
+                         ("ref_time_ozimmu_syrk", [L, L, L, P, I, I]), ("ref_time_cublas_dsyrk", [L, L, P, I, I])):
+        getattr(lib, name).argtypes = args_t
+        getattr(lib, name).restype = ctypes.c_double
+    lib.ref_syrk.argtypes = [L, L, ctypes.c_float, P, ctypes.c_float, P, L]
+    lib.ref_trsm.argtypes = [L, L, P, P, L]
     n = args.n
     A, T, B0 = make_inputs(n)
     hA = A.cpu().numpy()
@@ -621,21 +726,44 @@ def run_reference(args, world, rank, local):
     if t_syrk <= 0 or t_trsm <= 0:
         return {"impl": "reference", "unavailable": "reference routine failed on this device"}
     # end to end through the reference's public API: the same host <-> device
-    # bytes per step as the library's own e2e measurement
-    lib.ref_time_e2e.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, P, P, P, ctypes.c_int, ctypes.c_int]
-    lib.ref_time_e2e.restype = ctypes.c_double
+    # bytes per step as the library's own end-to-end measurement
     t_e2e = lib.ref_time_e2e(n, args.nb_syrk, args.nb_trsm, hA.ctypes.data_as(P), hT.ctypes.data_as(P),
                              hB.ctypes.data_as(P), 1, args.e2e_steps)
+    # sampled outputs (for the library arm's agreement check) and their FP64 errors
+    lo, hi, rows = sample_indices(n)
+    hC = np.zeros((n, n), dtype=np.float32)
+    hX = np.ascontiguousarray(hB.copy())
+    rc = lib.ref_syrk(n, n, 1.0, hA.ctypes.data_as(P), 0.0, hC.ctypes.data_as(P), args.nb_syrk)
+    rc |= lib.ref_trsm(n, n, hT.ctypes.data_as(P), hX.ctypes.data_as(P), args.nb_trsm)
+    errors = None
+    if rc == 0:
+        from scipy.linalg import solve_triangular
+
+        ref_s = hC[hi, lo].astype(np.float64)
+        ref_t = hX[:, rows].T.astype(np.float64)      # rows of X (column-major storage)
+        Ah = hA.astype(np.float64)
+        exact_s = np.einsum("pk,pk->k", Ah[:, lo], Ah[:, hi])
+        del Ah
+        Lh = hT.T.astype(np.float64)
+        exact_t = solve_triangular(Lh, hB[:, rows].astype(np.float64), lower=True).T
+        del Lh
+        e_s = float(np.linalg.norm(ref_s - exact_s) / np.linalg.norm(exact_s))
+        e_t = float(np.linalg.norm(ref_t - exact_t) / np.linalg.norm(exact_t))
+        errors = {"syrk": {"norm_rel": e_s, "sample": "4096 lower entries"},
+                  "trsm": {"norm_rel": e_t, "sample": "32 rows of X (X A^T = B)"}}
+        np.savez(SAMPLES, n=n, nb_syrk=args.nb_syrk, nb_trsm=args.nb_trsm, syrk=ref_s, trsm_rows=ref_t,
+                 err_syrk=e_s, err_trsm=e_t)
+    del hC, hX
     ms = t_syrk + t_trsm
     value = 2.0 * float(n) ** 3 / (ms * 1e-3) / 1e12
-    return {
+    line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f16 operands, f32 accumulate (cuBLAS GemmEx) + f32 cublasStrsm leaves", "data": "synthetic (seeded)",
-        "config": {"workload": f"reference tc_syrk n=k={n} nb={args.nb_syrk} + tc_trsm m=n={n} nb={args.nb_trsm} "
-                               "(its right-side form X A^T = B: same shape and flops) per step", "n": n,
-                   "precision": "plain", "l2": "inputs larger than L2", "parallelism": "replicas x1"},
-        "detail": {"syrk_ms": t_syrk, "trsm_ms": t_trsm, "timing": "median per call, CUDA events, device-resident"},
+        "config": workload(n, args.nb_syrk, args.nb_trsm),
+        "detail": {"syrk_ms": t_syrk, "trsm_ms": t_trsm, "timing": "median per call, CUDA events, device-resident",
+                   "trsm_side": "right (X A^T = B, the reference's tc_trsm form)"},
+        "errors_vs_fp64": errors,
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": 1, "kind": "reference",
                          "sample": "the reference library itself (oracle/_ref, built from its sources for sm_100a; "
                                    "its path is GPU code on cuBLAS) timed on this B200"},
@@ -645,6 +773,63 @@ def run_reference(args, world, rank, local):
                 if t_e2e > 0 else {"value": None, "unit": "TFLOP/s", "note": "end-to-end run failed"}),
         "clocks": clk,
     }
+    if not args.no_extra:
+        line["other_configs"] = reference_other_configs(lib)
+    return line
+
+
+def reference_other_configs(lib):
+    """The reference's timings of the other configurations, on inputs drawn
+    as in the library arm: tc_syrk n=k=4096 (its one-full-GEMM branch,
+    BLAS/tc_syrk.cu:104-110), tc_syr2k n=16384 k=4096, tc_trmm 16384 (lower:
+    its only form; same flops as the library's upper case), tc_symm 16384,
+    and FP64 SYRK n=k=8192 through tc_ozimmu_syrk (native FP64 cuBLAS
+    recursion) and one cuBLAS DSYRK, the native-FP64 baselines of the Ozaki
+    engine."""
+    P = ctypes_P()
+    out = {}
+    n = 4096
+    hA = (np.random.Generator(np.random.PCG64(1)).random((n, n), dtype=np.float32) * 2 - 1)
+    t = lib.ref_time_syrk(n, n, 256, hA.ctypes.data_as(P), 3, 20)
+    out["syrk_4096_plain"] = {"ms": t, "tflops": float(n) ** 3 / (t * 1e-3) / 1e12 if t > 0 else None,
+                              "note": "n < 8192: the reference computes one full n x n x k GEMM"}
+    g = np.random.Generator(np.random.PCG64(99))
+
+    def wide(r, c):
+        return np.ascontiguousarray((g.standard_normal((r, c)) * np.exp2(g.uniform(-8, 8, (r, c)))).astype(np.float32))
+
+    n, k = 16384, 4096
+    A, B = wide(k, n), wide(k, n)
+    t = lib.ref_time_syr2k(n, k, 256, A.ctypes.data_as(P), B.ctypes.data_as(P), 1, 5)
+    out["syr2k_16384x4096_plain"] = {"ms": t, "tflops": 2.0 * n * n * k / (t * 1e-3) / 1e12 if t > 0 else None}
+    del A, B
+    m = 16384
+    A, B = wide(m, m), wide(m, m)
+    At = np.ascontiguousarray(np.triu(A))   # storage (m, m) row-major = column-major A^T: keep A's lower part
+    t = lib.ref_time_trmm(m, m, 256, At.ctypes.data_as(P), B.ctypes.data_as(P), 1, 5)
+    out["trmm_16384_plain"] = {"ms": t, "tflops": float(m) ** 3 / (t * 1e-3) / 1e12 if t > 0 else None,
+                               "note": "tc_trmm is lower-only"}
+    del At
+    t = lib.ref_time_symm(m, m, A.ctypes.data_as(P), B.ctypes.data_as(P), 1, 5)
+    out["symm_16384_plain"] = {"ms": t, "tflops": 2.0 * float(m) ** 3 / (t * 1e-3) / 1e12 if t > 0 else None}
+    del A, B
+    n = k = 8192
+    fp64 = {}
+    for phi in (0.5, 2.0):
+        g2 = np.random.Generator(np.random.PCG64(17))
+        Ah = np.asfortranarray(g2.standard_normal((n, k)) * np.exp(phi * g2.standard_normal((n, k))))
+        t_oz = lib.ref_time_ozimmu_syrk(n, k, 256, Ah.ctypes.data_as(P), 1, 3)
+        t_cb = lib.ref_time_cublas_dsyrk(n, k, Ah.ctypes.data_as(P), 1, 3)
+        fp64[f"phi={phi}"] = {"tc_ozimmu_syrk_ms": t_oz, "cublas_dsyrk_ms": t_cb}
+        del Ah
+    out["dsyrk_8192_native_fp64"] = fp64
+    return out
+
+
+def ctypes_P():
+    import ctypes
+
+    return ctypes.c_void_p
 
 
 def profile_step(args):

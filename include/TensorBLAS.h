@@ -33,8 +33,8 @@ typedef struct cublasContext* cublasHandle_t;
 #endif
 #ifndef TB_HAVE_CUMPSGEMM
 namespace cumpsgemm {
-struct handle;
-typedef handle* handle_t;
+struct handle_struct;
+typedef handle_struct* handle_t;
 }  // namespace cumpsgemm
 #endif
 

@@ -55,6 +55,31 @@ TB_API tb_status tb_synchronize(void);
 TB_API int tb_version(void);
 /* Number of kernels this library has launched in this process. */
 TB_API unsigned long long tb_launch_count(void);
+/* Number of device allocations (cudaMalloc) this library has made in this
+ * process: scratch pool growth, cached tile lists, error blocks, batches and
+ * autotuner trial outputs (no reference counterpart; a diagnostic). */
+TB_API unsigned long long tb_alloc_count(void);
+/* Waits for the device, then frees the library's scratch pool and cached
+ * device tile lists on the current device (no reference counterpart: the
+ * reference's wrappers malloc and free per call). The next routine call
+ * allocates again. Batches keep their own memory until tb_batch_destroy. */
+TB_API tb_status tb_release_scratch(void);
+/* Test hook of the failure path (no reference counterpart). From now on the
+ * GEMM kernels' producers skip the operand loads of tile `tile` of every
+ * launch (-1: none), and every bounded device wait gives up after `wait_ns`
+ * ns (0: the default of 4 s): a launch that reaches that tile stops with its
+ * output partly written and tb_synchronize returns TB_ERROR_TIMEOUT, while
+ * the context stays usable. tb_debug_stall(-1, 0) restores normal
+ * operation. Not for production use. */
+TB_API tb_status tb_debug_stall(long tile, unsigned long long wait_ns);
+/* Host-only check of the task plan the persistent TRSM solve would use for
+ * tb_strsm(side, m, n, ..., nb, precision) (no reference counterpart; no
+ * device memory is touched): every tile and counter index in range and the
+ * claim order topological, so that no task can wait for a later one.
+ * stats[4] receives {tasks, counters, ops, simulated makespan in cost
+ * units}; TB_ERROR_INVALID_VALUE and the reason in tb_last_error if the
+ * plan is not valid. */
+TB_API tb_status tb_debug_trsm_plan(char side, long m, long n, long nb, int precision, long* stats);
 /* Event timing of every GEMM-engine launch between begin and end (events on
  * the launching stream): device ms during which at least one of them ran (the
  * union of their intervals: launches on two streams may overlap), total
@@ -191,30 +216,38 @@ TB_API tb_status tb_strsm_host(char side, long m, long n, const float* A, long l
 
 /*
  * tb_ssyrk_noalloc: tb_ssyrk for callers that cannot allocate device memory
- * (no counterpart in the reference library). Same arguments and results as
+ * (no counterpart in the reference library). Arguments and results as
  * tb_ssyrk, but every byte of scratch comes from one static 64 MiB device
  * array compiled into the library, so the call makes no cudaMalloc/cudaFree.
  * It is meant for callers whose GPU memory is owned by another allocator
  * (e.g. a framework's caching allocator holding nearly all HBM) and for
  * latency-critical code that cannot absorb the device-wide synchronisation
- * cudaMalloc/cudaFree imply. Limit: the tile list plus the FP16 copy of A
+ * cudaMalloc/cudaFree imply. Limits: the tile list plus the FP16 copy of A
  * (round_up(rows, 64) * cols * 2 bytes, twice that for TB_PREC_SPLIT) must
- * fit in 64 MiB, else TB_ERROR_INVALID_VALUE with the size in tb_last_error.
+ * fit in 64 MiB, else TB_ERROR_INVALID_VALUE with the size in tb_last_error;
+ * precision TB_PREC_PLAIN or TB_PREC_SPLIT only (TB_PREC_FP8 is rejected)
+ * and nb > 0 (TB_NB_AUTO is rejected). k == 0 or alpha == 0 only scales C.
  * The first call on a device looks up the array's address; make it before
  * any stream capture. All calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller. k == 0 / alpha == 0 are
- * not supported here (use tb_ssyrk).
+ * GPU race and must be serialised by the caller. A device-side wait that
+ * runs out is reported by tb_synchronize (TB_ERROR_TIMEOUT), which reads
+ * the call's own static error block and allocates nothing.
  */
 TB_API tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
                                   float beta, float* C, long ldc, long nb, int precision);
 
 /*
  * FP64 routines on the INT8 tensor cores (Ozaki scheme). Each operand row is
- * split into `slices` INT8 slices (1..14; <= 0 selects 10) under a per-row
- * power-of-two exponent; every slice-pair product is exact (INT32, K chunked
- * so the level sums cannot overflow), and the result is FP64-accurate once
- * 7 * slices exceeds 53 bits plus the in-row exponent spread. The reference's
- * tc_ozimmu_* drivers run native FP64 cuBLAS GEMMs instead.
+ * split into `slices` INT8 slices (1..14) under a per-row power-of-two
+ * exponent; every slice-pair product is exact (INT32, K chunked so the level
+ * sums cannot overflow), and the result is FP64-accurate once 7 * slices
+ * exceeds 53 bits plus the in-row exponent spread. slices <= 0 selects the
+ * count automatically (SYRK, SYR2K, TRMM): one pass over the operands
+ * measures each row's spread d = e_max - log2(rms) in bits, and the count is
+ * the smallest with 7 * slices >= 50 + max d, within [8, 14] (the call then
+ * waits for that measurement); TRSM takes 10. The reference's tc_ozimmu_*
+ * drivers run native FP64 cuBLAS GEMMs instead; the tc_ozimmu_* entry points
+ * here use the automatic count (TRSM: 10).
  *
  * Scratch: the slice planes, plus each product's INT32 level sums
  * (4 * slices bytes per element of the output's bounding rectangle) when
@@ -271,6 +304,13 @@ TB_API tb_status tb_batch_create(tb_batch_t* batch, int count, const int* kind, 
                                  const long* lda, float* const* BC, const long* ldbc, long nb, int precision);
 TB_API tb_status tb_batch_run(tb_batch_t batch);
 TB_API tb_status tb_batch_destroy(tb_batch_t batch);
+
+/* FP32 -> FP16 conversion of an m x n column-major matrix, round to
+ * nearest even: ah = fp16(as) (ldah), and when al is not NULL also the
+ * scaled low half al = fp16((as - ah) * lo_scale) of the split form.
+ * Replaces the reference's s2h / s2h_swpipe kernels (util/util.cu:127-136,
+ * include/TensorBLAS.h:185-283); ah and al are __half arrays. */
+TB_API tb_status tb_s2h(long m, long n, const float* as, long ldas, void* ah, long ldah, void* al, float lo_scale);
 
 /* Mirror lower -> upper of an n x n matrix (util/util.cu:148-157). */
 TB_API tb_status tb_ssymmetrize(long n, float* A, long lda);

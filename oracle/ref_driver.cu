@@ -411,3 +411,30 @@ double ref_time_e2e(long n, long nb_syrk, long nb_trsm, const float* hA, const f
   return rc ? -1.0 : median(t);
 }
 }  // extern "C"
+
+extern "C" {
+// Median device time (ms) of one cuBLAS DSYRK (lower, 'N', alpha = 1,
+// beta = 0) on device-resident inputs: the plain native-FP64 routine beside
+// the reference's tc_ozimmu_syrk recursion, for the FP64 comparison.
+double ref_time_cublas_dsyrk(long n, long k, const double* hA, int warmup, int iters) {
+  double* A = up(hA, (size_t)n * k);
+  double* C = up<double>(nullptr, (size_t)n * n);
+  if (!A || !C) return -1.0;
+  const double one = 1.0, zero = 0.0;
+  Events ev;
+  std::vector<float> t;
+  for (int i = 0; i < warmup + iters; ++i) {
+    cudaEventRecord(ev.a);
+    cublasDsyrk(handle(), CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)n, (int)k, &one, A, (int)n, &zero, C, (int)n);
+    cudaEventRecord(ev.b);
+    cudaEventSynchronize(ev.b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev.a, ev.b);
+    if (i >= warmup) t.push_back(ms);
+  }
+  int rc = finish();
+  cudaFree(A);
+  cudaFree(C);
+  return rc ? -1.0 : median(t);
+}
+}  // extern "C"

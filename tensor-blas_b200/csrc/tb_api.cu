@@ -53,6 +53,10 @@ tb_status tb_ssymmetrize(long n, float* A, long lda) {
 
 // BLAS/tc_syrk.cu:4-39: C = A A^T for the row-major n x k torch tensor A
 // (column-major k x n in memory), full symmetric C, 0 on success / 1 on error.
+// Like the reference's wrapper (whose cudaFree of its workspace waits for the
+// device), it returns only once the result is complete: it synchronises the
+// library's stream and reports a CUDA error or a device-side wait that ran
+// out as 1.
 int tc_syrk_wrapper(long n, long k, float* A, float* C, long nb) {
   tb_status s = tb_ssyrk('L', 'T', n, k, 1.0f, A, k > 1 ? k : 1, 0.0f, C, n > 1 ? n : 1, nb, TB_PREC_PLAIN);
   if (s == TB_SUCCESS) s = tb_ssymmetrize(n, C, n > 1 ? n : 1);
@@ -60,6 +64,7 @@ int tc_syrk_wrapper(long n, long k, float* A, float* C, long nb) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) s = tb::cuda_status(e);
   }
+  if (s == TB_SUCCESS) s = tb_synchronize();
   if (s != TB_SUCCESS) {
     printf("TensorBLAS error: %s %s\n", tb_status_string(s), tb_last_error());
     return 1;
@@ -68,13 +73,15 @@ int tc_syrk_wrapper(long n, long k, float* A, float* C, long nb) {
 }
 
 // BLAS/tc_trsm.cu:4-28: X A^T = B, A n x n lower (lda = n), B m x n (ldb = m),
-// B overwritten; 0 on success / 1 on error.
+// B overwritten; 0 on success / 1 on error (synchronous, errors as in
+// tc_syrk_wrapper).
 int tc_trsm_wrapper(long m, long n, float* A, float* B, long nb) {
   tb_status s = tb_strsm('R', m, n, A, n > 1 ? n : 1, B, m > 1 ? m : 1, nb, TB_PREC_PLAIN);
   if (s == TB_SUCCESS) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) s = tb::cuda_status(e);
   }
+  if (s == TB_SUCCESS) s = tb_synchronize();
   if (s != TB_SUCCESS) {
     printf("TensorBLAS error: %s %s\n", tb_status_string(s), tb_last_error());
     return 1;

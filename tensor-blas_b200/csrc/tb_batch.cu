@@ -308,7 +308,7 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
       toff.push_back(o);
     }
   }
-  if (ar.used > 0 && cudaMalloc(&b->scratch, ar.used) != cudaSuccess) {
+  if (ar.used > 0 && dev_malloc(&b->scratch, ar.used) != cudaSuccess) {
     cudaGetLastError();
     delete b;
     set_last_error("tb_batch_create: cannot allocate %zu bytes of scratch", ar.used);
@@ -445,7 +445,7 @@ extern "C" tb_status tb_batch_create(tb_batch_t* out, int count, const int* kind
     o_tiles.push_back(tab.take(sizeof(int4) * L.tiles.size()));
     o_prob.push_back(tab.take(sizeof(int) * L.prob.size()));
   }
-  if (cudaMalloc(&b->tables, tab.used) != cudaSuccess) {
+  if (dev_malloc(&b->tables, tab.used) != cudaSuccess) {
     cudaGetLastError();
     tb_batch_destroy(b);
     return TB_ERROR_ALLOC;

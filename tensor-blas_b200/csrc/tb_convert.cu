@@ -190,3 +190,15 @@ tb_status set_unit_diag(long long n, __half* hi, __half* lo, long long ld, cudaS
 }
 
 }  // namespace tb
+
+// The conversion as an entry point of its own: the reference's s2h
+// (util/util.cu:127-136; the FP32 -> FP16 step of every routine), with the
+// optional scaled-lo half of the split form.
+extern "C" tb_status tb_s2h(long m, long n, const float* as, long ldas, void* ah, long ldah, void* al,
+                            float lo_scale) {
+  if (m < 0 || n < 0 || ldas < (m > 1 ? m : 1) || ldah < (m > 1 ? m : 1)) return TB_ERROR_INVALID_VALUE;
+  if (m == 0 || n == 0) return TB_SUCCESS;
+  if (!as || !ah) return TB_ERROR_INVALID_VALUE;
+  return tb::convert_f32_f16(m, n, as, ldas, static_cast<__half*>(ah), static_cast<__half*>(al), ldah, lo_scale, 0,
+                             tb::current_stream());
+}

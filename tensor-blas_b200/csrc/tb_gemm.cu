@@ -167,6 +167,15 @@ tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t strea
 
 }  // namespace
 
+int split_kchunk() {
+  static const int k = [] {
+    const char* e = getenv("TB_SPLIT_KCHUNK");
+    const int v = e ? atoi(e) : 0;
+    return (v >= 1 && v <= 64) ? v : 2;
+  }();
+  return k;
+}
+
 int gemm_bn(Split s) { return s == Split::kPlain ? 256 : 128; }
 int gemm_bn(Split s, int kblocks) {
   const bool pf = kblocks > 0 && kblocks <= kGemmPfMaxKb;
@@ -395,7 +404,7 @@ tb_status gemm_launch_grouped(Split split, const GemmArgs* d_problems, const int
   a.problems = d_problems;
   a.tile_prob = d_tile_prob;
   a.corr_scale = 1.0f / 2048.0f;
-  a.kchunk = 2;
+  a.kchunk = split_kchunk();
   a.err = device_error_word();
   if (split == Split::kHiLo)
     return launch_variant<GemmCfg<128, 3, true, true>, true>(a, num_tiles, stream, flops);
@@ -449,35 +458,102 @@ std::vector<int4> plan_upper(int n, int bn, int kb0, int kb1) {
 }
 
 // Device copies of tile plans, cached by content (per device). Plans are
-// small (16 B per tile) and reused across calls of the same shape.
+// small (16 B per tile) and reused across calls of the same shape. The cache
+// holds at most kTileCacheBytes per device; beyond that the least recently
+// used lists are freed (after a device synchronisation, since launches still
+// queued may read them).
+namespace {
+struct TileEntry {
+  std::vector<int4> tiles;
+  int4* d;
+  uint64_t last_use;
+};
+struct TileCache {
+  std::mutex mu;
+  std::map<std::pair<int, uint64_t>, std::vector<TileEntry>> map;
+  size_t bytes[64] = {};
+  uint64_t clock = 0;
+};
+TileCache& tile_cache() {
+  static TileCache c;
+  return c;
+}
+constexpr size_t kTileCacheBytes = 64ull << 20;
+
+// Frees least recently used lists of device `dev` until `need` more bytes
+// fit under the cap (caller holds the lock).
+void evict_tiles(TileCache& tc, int dev, size_t need) {
+  if (dev >= 64 || tc.bytes[dev] + need <= kTileCacheBytes) return;
+  cudaDeviceSynchronize();
+  while (tc.bytes[dev] + need > kTileCacheBytes) {
+    auto best = tc.map.end();
+    size_t bi = 0;
+    for (auto it = tc.map.begin(); it != tc.map.end(); ++it) {
+      if (it->first.first != dev) continue;
+      for (size_t i = 0; i < it->second.size(); ++i)
+        if (best == tc.map.end() || it->second[i].last_use < best->second[bi].last_use) {
+          best = it;
+          bi = i;
+        }
+    }
+    if (best == tc.map.end()) break;
+    TileEntry& e = best->second[bi];
+    cudaFree(e.d);
+    tc.bytes[dev] -= e.tiles.size() * sizeof(int4);
+    best->second.erase(best->second.begin() + (long)bi);
+    if (best->second.empty()) tc.map.erase(best);
+  }
+}
+}  // namespace
+
 const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream) {
   // Cached by content: a 64-bit FNV-1a hash selects the candidates, a full
   // comparison confirms.
-  struct Entry {
-    std::vector<int4> tiles;
-    int4* d;
-  };
-  static std::mutex mu;
-  static std::map<std::pair<int, uint64_t>, std::vector<Entry>> cache;
+  TileCache& tc = tile_cache();
   int dev = 0;
   cudaGetDevice(&dev);
   const size_t bytes = tiles.size() * sizeof(int4);
   uint64_t h = 1469598103934665603ull ^ (uint64_t)bytes;
   const uint32_t* w = reinterpret_cast<const uint32_t*>(tiles.data());
   for (size_t i = 0; i < bytes / 4; ++i) h = (h ^ w[i]) * 1099511628211ull;
-  std::lock_guard<std::mutex> lk(mu);
-  std::vector<Entry>& bucket = cache[{dev, h}];
-  for (const Entry& e : bucket)
-    if (e.tiles.size() == tiles.size() && memcmp(e.tiles.data(), tiles.data(), bytes) == 0) return e.d;
+  std::lock_guard<std::mutex> lk(tc.mu);
+  ++tc.clock;
+  {
+    auto it = tc.map.find({dev, h});
+    if (it != tc.map.end())
+      for (TileEntry& e : it->second)
+        if (e.tiles.size() == tiles.size() && memcmp(e.tiles.data(), tiles.data(), bytes) == 0) {
+          e.last_use = tc.clock;
+          return e.d;
+        }
+  }
+  evict_tiles(tc, dev, bytes);
   int4* d = nullptr;
-  if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+  if (dev_malloc(reinterpret_cast<void**>(&d), bytes) != cudaSuccess) return nullptr;
   if (cudaMemcpy(d, tiles.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaFree(d);
     return nullptr;
   }
   (void)stream;
-  bucket.push_back(Entry{tiles, d});
+  tc.map[{dev, h}].push_back(TileEntry{tiles, d, tc.clock});
+  if (dev < 64) tc.bytes[dev] += bytes;
   return d;
+}
+
+void release_tile_cache() {
+  TileCache& tc = tile_cache();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(tc.mu);
+  for (auto it = tc.map.begin(); it != tc.map.end();) {
+    if (it->first.first != dev) {
+      ++it;
+      continue;
+    }
+    for (TileEntry& e : it->second) cudaFree(e.d);
+    it = tc.map.erase(it);
+  }
+  if (dev < 64) tc.bytes[dev] = 0;
 }
 
 }  // namespace tb

@@ -552,6 +552,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
           }
         }
         if (t < 0) break;
+        if (debug_stall_tile(args.err, t)) break;  // test hook: this tile's loads never come
         // the next claim is issued early so its latency hides
         const int t_next = dyn ? atomicAdd(args.sched, 1) : static_next(args, blockIdx.x, gridDim.x, t);
         const int4 tile = args.tiles[t];
@@ -1024,6 +1025,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       uint32_t issued_mask = 0, phase_mask = 0;
       bool ok = true;
       for (int t = static_first(args, pair); t >= 0 && ok; t = static_next(args, pair, npairs, t)) {
+        if (debug_stall_tile(args.err, t)) break;  // test hook: this tile's loads never come
         const int4 tile = args.tiles[t];
         for (int kb = tile.z; kb < tile.w; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {

@@ -36,14 +36,32 @@ cudaStream_t aux_stream();
 // Device scratch owned by the library (grow-only, per device and slot).
 // Slot 0 serves the routines' own scratch; slot 1 the host-memory entry
 // points' staging buffers, which live across routine calls; slot 2 the Ozaki
-// engine's per-level INT32 sums. Returns nullptr on allocation failure.
-// Growing synchronises the device.
-constexpr int kPoolSlots = 3;
+// engine's per-level INT32 sums; slot 3 the persistent TRSM solve's per-leaf
+// operand copies, progress counters and op descriptors. Returns nullptr on
+// allocation failure. Growing synchronises the device.
+constexpr int kPoolSlots = 4;
 void* pool_get(size_t bytes, int slot = 0);
-// Device error word used by bounded waits inside kernels (per device).
+// Bytes currently held by a pool slot of the current device.
+size_t pool_capacity(int slot);
+// Device error block used by bounded waits inside kernels (per device):
+// kErrBlockInts ints, word 0 the error code (layout in tb_ptx.cuh).
+constexpr int kErrBlockInts = 4;
 int* device_error_word();
-// Reads and clears the device error word (synchronises `stream`).
+// A second error block of the current device (the allocation-free entry
+// point's static one), read by check_device_error alongside the library's.
+void register_error_block(int* block);
+// Synchronises `stream`, then reads and clears the error code of every error
+// block of the current device that exists; creates none (allocates nothing).
 tb_status check_device_error(cudaStream_t stream);
+// cudaMalloc, counted (tb_alloc_count): every device allocation the library
+// makes goes through here.
+cudaError_t dev_malloc(void** p, size_t bytes);
+// Frees the scratch pool slots / the cached device tile lists of the
+// current device (tb_release_scratch; the device must be idle).
+void release_pool();
+void release_tile_cache();
+// Free device memory of the current device (cudaMemGetInfo), 0 on error.
+size_t free_device_bytes();
 int sm_count();
 // Counts kernel launches issued by the library (tb_launch_count).
 void note_launch(int n = 1);
@@ -68,6 +86,12 @@ struct Operand {
 
 enum class Split { kPlain = 1, kHiLo = 3 };
 
+// Split products: K-blocks (of 64) the tensor core accumulates in TMEM
+// between two round-to-nearest folds into FP32 registers (its own FP32
+// accumulation truncates): 2 unless TB_SPLIT_KCHUNK (1..64) is set in the
+// environment (read once).
+int split_kchunk();
+
 struct GemmCall {
   Operand a_hi, a_lo, b_hi, b_lo;  // lo used in kHiLo only
   Split split = Split::kPlain;
@@ -80,7 +104,7 @@ struct GemmCall {
   float alpha = 1.f, beta = 0.f;
   int tri = 0, diag = 0;
   float corr_scale = 1.0f / 2048.0f;
-  int kchunk = 2;  // split mode: K-blocks (64) per round-to-nearest fold
+  int kchunk = split_kchunk();  // split mode: K-blocks (64) per round-to-nearest fold
   __half* out_hi = nullptr;
   __half* out_lo = nullptr;
   long long ld_out = 0;
@@ -215,6 +239,16 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
                      void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit = false);
 size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split);
 tb_status trsm_solve(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
+// The recursion as one GEMM launch per leaf product and per update.
+tb_status trsm_solve_launches(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows,
+                              long cols);
+// The recursion as one persistent launch (tb_trsm_dag.cu): same tiles, K
+// ranges and accumulation order, scheduled on the device by progress
+// counters. Eligible when B can be written by TMA (16-byte aligned, ldb a
+// multiple of 4) and A has more than one leaf; TB_TRSM_DAG=0 in the
+// environment turns it off (read once).
+bool trsm_dag_eligible(const TrsmCtx& c, const float* B, long ldb);
+tb_status trsm_solve_dag(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
 // The same solve with B's independent dimension (columns for the left side,
 // rows for the right side) split in two halves solved on the context's
 // stream and the auxiliary stream, so the tail of each launch of one half

@@ -19,9 +19,17 @@
 //    only a host-side stand-in). Make that first call before any stream
 //    capture.
 //  * Sharing: all calls use the same array, which keeps the previous call's
-//    contents; the device error word is cleared at the start of every call.
-//    Calls that overlap on the GPU (different streams, or different host
-//    threads) race on the array and must be serialised by the caller.
+//    contents; the call's own device error block (a second static array) has
+//    its code cleared at the start of every call. Calls that overlap on the
+//    GPU (different streams, or different host threads) race on the array
+//    and must be serialised by the caller.
+//  * Errors: a bounded wait that runs out inside the kernel is recorded in
+//    that error block, which the set-up registers with the library's
+//    runtime, so tb_synchronize reports it (TB_ERROR_TIMEOUT) without
+//    allocating anything.
+//  * Scope: uplo 'L' or 'U', trans 'N' or 'T', TB_PREC_PLAIN or
+//    TB_PREC_SPLIT, nb > 0 (TB_PREC_FP8 and TB_NB_AUTO need scratch of
+//    their own and are rejected); k == 0 or alpha == 0 only scales C.
 #include <cstdio>
 #include <mutex>
 
@@ -56,6 +64,7 @@ tb_status resolve_symbols(Symbols** out) {
     s.scratch = static_cast<unsigned char*>(p);
     TB_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_err));
     s.err = static_cast<int*>(p);
+    register_error_block(s.err);
     s.ready = true;
   }
   *out = &s;
@@ -68,28 +77,28 @@ tb_status resolve_symbols(Symbols** out) {
 extern "C" tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, float alpha, const float* A, long lda,
                                       float beta, float* C, long ldc, long nb, int precision) {
   using namespace tb;
-  if (uplo != 'L' && uplo != 'l') {
-    set_last_error("tb_ssyrk_noalloc: only uplo='L' is supported");
-    return TB_ERROR_NOT_SUPPORTED;
-  }
+  const bool upper = (uplo == 'U' || uplo == 'u');
+  if (!upper && uplo != 'L' && uplo != 'l') return TB_ERROR_INVALID_VALUE;
   const bool t = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');
   if (!t && trans != 'N' && trans != 'n') return TB_ERROR_INVALID_VALUE;
-  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT) return TB_ERROR_INVALID_VALUE;
+  if (precision != TB_PREC_PLAIN && precision != TB_PREC_SPLIT) {
+    set_last_error("tb_ssyrk_noalloc: precision must be TB_PREC_PLAIN or TB_PREC_SPLIT");
+    return TB_ERROR_INVALID_VALUE;
+  }
   if (n < 0 || k < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
   if (ldc < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
   if (lda < ((t ? k : n) > 1 ? (t ? k : n) : 1)) return TB_ERROR_INVALID_VALUE;
   if (n == 0) return TB_SUCCESS;
-  if (k == 0 || alpha == 0.f) {
-    set_last_error("tb_ssyrk_noalloc: k == 0 or alpha == 0 is not supported (use tb_ssyrk)");
-    return TB_ERROR_NOT_SUPPORTED;
-  }
+  cudaStream_t st = current_stream();
+  // nothing to multiply: C = beta C on the referenced triangle (no scratch)
+  if (k == 0 || alpha == 0.f) return beta == 1.f ? TB_SUCCESS : scale_lower(n, beta, C, ldc, st, upper);
   const Split split = precision == TB_PREC_SPLIT ? Split::kHiLo : Split::kPlain;
   const bool hilo = split == Split::kHiLo;
   const long long rows = t ? k : n, cols = t ? n : k;
   const long long ldh = round_up(rows, 64);
   const int bn = gemm_bn(split);
   const int kb = (int)((k + kGemmBK - 1) / kGemmBK);
-  const std::vector<int4> plan = plan_lower((int)n, bn, 0, kb);
+  const std::vector<int4> plan = upper ? plan_upper((int)n, bn, 0, kb) : plan_lower((int)n, bn, 0, kb);
   const size_t tiles_bytes = (size_t)round_up((long long)(plan.size() * sizeof(int4)), 256);
   const size_t one = (size_t)round_up(ldh * cols * (long long)sizeof(__half), 256);
   const size_t need = tiles_bytes + one * (hilo ? 2 : 1);
@@ -100,7 +109,6 @@ extern "C" tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, flo
   }
   Symbols* sym = nullptr;
   TB_TRY(resolve_symbols(&sym));
-  cudaStream_t st = current_stream();
   int4* tiles = reinterpret_cast<int4*>(sym->scratch);
   __half* hi = reinterpret_cast<__half*>(sym->scratch + tiles_bytes);
   __half* lo = hilo ? reinterpret_cast<__half*>(sym->scratch + tiles_bytes + one) : nullptr;
@@ -121,7 +129,7 @@ extern "C" tb_status tb_ssyrk_noalloc(char uplo, char trans, long n, long k, flo
   c.M = c.N = (int)n;
   c.alpha = alpha;
   c.beta = beta;
-  c.tri = 1;
+  c.tri = upper ? 2 : 1;
   c.err = sym->err;
   c.flops = (double)n * (double)(n + 1) * (double)k;
   return gemm_launch(c, st);

@@ -21,6 +21,8 @@
 // slice) feeds every pair.
 #include <algorithm>
 #include <climits>
+#include <cmath>
+#include <mutex>
 #include <cstring>
 #include <cstdio>
 #include <vector>
@@ -118,6 +120,81 @@ __global__ void __launch_bounds__(256) oz_exp_cols_kernel(long long rows, long l
     m = t > m ? t : m;
   }
   if (lane == 0) atomicMax(&e[i], m);
+}
+
+// Dynamic range of the operand rows, for the automatic slice count: per row
+// i, with e_i its largest exponent (|x| < 2^e_i) and r_i its root mean
+// square, d_i = e_i - log2(r_i) is how many bits the row's largest entries
+// sit above its typical one. The largest d_i over the rows is written (in
+// 1/256 bit units) to *out with atomicMax. The sum of squares is kept scaled
+// by 2^-2m for the running maximum exponent m, so no value overflows.
+__device__ __forceinline__ void oz_stat_add(int& m, double& ssq, double v) {
+  if (v == 0.0) return;
+  int ex;
+  frexp(v, &ex);
+  if (ex > m) {
+    ssq = ldexp(ssq, 2 * (m - ex));
+    m = ex;
+  }
+  const double y = ldexp(v, -m);
+  ssq = fma(y, y, ssq);
+}
+__device__ __forceinline__ void oz_stat_merge(int& m, double& ssq, int m2, double s2) {
+  if (s2 == 0.0) return;
+  if (ssq == 0.0) {
+    m = m2;
+    ssq = s2;
+    return;
+  }
+  if (m2 > m) {
+    ssq = ldexp(ssq, 2 * (m - m2)) + s2;
+    m = m2;
+  } else {
+    ssq += ldexp(s2, 2 * (m2 - m));
+  }
+}
+__device__ __forceinline__ void oz_stat_publish(double ssq, long long cnt, int* out) {
+  if (ssq <= 0.0 || cnt <= 0) return;
+  const double d = -0.5 * log2(ssq / (double)cnt);  // e_i - log2(rms_i) >= 0
+  atomicMax(out, (int)ceil(d * 256.0));
+}
+// One thread per row (rows of a column-major matrix: coalesced across threads).
+__global__ void __launch_bounds__(64) oz_spread_rows_kernel(long long rows, long long k, const double* __restrict__ X,
+                                                            long long ldx, int mask, long long koff, int* out) {
+  const long long i = (long long)blockIdx.x * 64 + threadIdx.x;
+  if (i >= rows) return;
+  int m = INT_MIN / 4;
+  double ssq = 0.0;
+  long long cnt = 0;
+  for (long long p = 0; p < k; ++p)
+    if (oz_keep(mask, i, p, koff)) {
+      oz_stat_add(m, ssq, X[i + p * ldx]);
+      ++cnt;
+    }
+  oz_stat_publish(ssq, cnt, out);
+}
+// One warp per row (a column of X, contiguous in memory).
+__global__ void __launch_bounds__(256) oz_spread_cols_kernel(long long rows, long long k, const double* __restrict__ X,
+                                                             long long ldx, int mask, long long koff, int* out) {
+  const long long i = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= rows) return;
+  int m = INT_MIN / 4;
+  double ssq = 0.0;
+  long long cnt = 0;
+  for (long long p = lane; p < k; p += 32)
+    if (oz_keep(mask, i, p, koff)) {
+      oz_stat_add(m, ssq, X[p + i * ldx]);
+      ++cnt;
+    }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const int m2 = __shfl_xor_sync(0xffffffffu, m, o);
+    const double s2 = __shfl_xor_sync(0xffffffffu, ssq, o);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    oz_stat_merge(m, ssq, m2, s2);
+  }
+  if (lane == 0) oz_stat_publish(ssq, cnt, out);
 }
 
 // Slices 16 consecutive K values of one row (already scaled by 2^-e) into S
@@ -993,7 +1070,12 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
   // fold after the GEMM (oz_fold_kernel) when the levels' workspace fits
   const long long ld_r = round_up((long long)M, 32), plane = ld_r * (long long)N;
   int* levels = nullptr;
-  if (raw_level == 0 && oz_split_fold_enabled() && (double)S * plane * 4.0 <= kOzLevelBytesMax)
+  // (at most kOzLevelBytesMax, and no more than half of the device memory
+  // still free unless the pool slot already holds it: an application sharing
+  // the GPU keeps its headroom, and the fused fold needs no workspace)
+  const double level_bytes = (double)S * plane * 4.0;
+  if (raw_level == 0 && oz_split_fold_enabled() && level_bytes <= kOzLevelBytesMax &&
+      (level_bytes <= (double)pool_capacity(2) || level_bytes <= 0.5 * (double)free_device_bytes()))
     levels = static_cast<int*>(pool_get((size_t)S * (size_t)plane * 4, 2));
   OzArgs g;
   memset(&g, 0, sizeof(g));
@@ -1048,6 +1130,54 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
   }
   prof_end(tok, st, flops);
   note_launch();
+  return TB_SUCCESS;
+}
+
+// Automatic slice count. Truncating row i after S slices of 7 bits leaves
+// an error below 2^(e_i - 7S) per entry; relative to the row's root mean
+// square that is 2^(d_i - 7S), which the dot products carry into C at about
+// the same relative size. S is the smallest count with 7S >= 50 + max_i d_i
+// (2^-50 ~ 9e-16 of headroom under the 1e-14 target), at least 8 (the 53
+// bits of the significand) and at most kOzMaxSlices.
+constexpr int kOzAutoBits = 50;
+
+int oz_slices_for_spread(double spread_bits) {
+  int S = (int)std::ceil((kOzAutoBits + spread_bits) / 7.0);
+  return std::max(8, std::min(kOzMaxSlices, S));
+}
+
+// Largest row spread of the operands (bits), one small device word per device.
+tb_status oz_max_spread(const std::vector<OzOperand>& ops, cudaStream_t st, double* spread) {
+  static int* word[64] = {};
+  static std::mutex mu;
+  int dev = 0;
+  TB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return TB_ERROR_NOT_SUPPORTED;
+  int* w = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!word[dev] && dev_malloc(reinterpret_cast<void**>(&word[dev]), 256) != cudaSuccess) {
+      cudaGetLastError();
+      word[dev] = nullptr;
+      return TB_ERROR_ALLOC;
+    }
+    w = word[dev];
+  }
+  TB_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(int), st));
+  for (const OzOperand& o : ops) {
+    if (o.rows == 0 || o.k == 0) continue;
+    if (o.by_cols)
+      oz_spread_cols_kernel<<<(unsigned)((o.rows + 7) / 8), 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff, w);
+    else
+      oz_spread_rows_kernel<<<(unsigned)((o.rows + 63) / 64), 64, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff,
+                                                                          w);
+    TB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+  }
+  int h = 0;
+  TB_CUDA_TRY(cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TB_CUDA_TRY(cudaStreamSynchronize(st));
+  *spread = h / 256.0;
   return TB_SUCCESS;
 }
 
@@ -1115,19 +1245,24 @@ tb_status ozaki_syrk_impl(bool trans, long n, long k, double alpha, const double
                           bool upper = false) {
   const long rows_a = trans ? k : n;
   if (n < 0 || k < 0 || lda < (rows_a > 1 ? rows_a : 1) || ldc < (n > 1 ? n : 1)) return TB_ERROR_INVALID_VALUE;
-  TB_TRY(check_slices(S));
   if (n == 0) return TB_SUCCESS;
-  const long long kc_max = oz_kmax(S);
-  if (raw_level >= 2 && k > kc_max) {
-    set_last_error("ozaki: level products need k <= %lld with %d slices", kc_max, S);
-    return TB_ERROR_NOT_SUPPORTED;
-  }
   OzOperand a;
   a.X = A;
   a.ld = lda;
   a.rows = n;
   a.k = k;
   a.by_cols = trans;
+  if (S <= 0) {
+    double spread = 0;
+    TB_TRY(oz_max_spread({a}, st, &spread));
+    S = oz_slices_for_spread(spread);
+  }
+  TB_TRY(check_slices(S));
+  const long long kc_max = oz_kmax(S);
+  if (raw_level >= 2 && k > kc_max) {
+    set_last_error("ozaki: level products need k <= %lld with %d slices", kc_max, S);
+    return TB_ERROR_NOT_SUPPORTED;
+  }
   const long long K1 = k > 0 ? k : 1;
   const long long ldq = round_up(std::min<long long>(K1, kc_max), kOzBK);
   char* ws = static_cast<char*>(pool_get(oz_planes_bytes(n, ldq, S)));
@@ -1151,8 +1286,21 @@ tb_status ozaki_syr2k_impl(long n, long k, double alpha, const double* A, long l
                            double beta, double* C, long ldc, int S, cudaStream_t st) {
   if (n < 0 || k < 0 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) || ldc < (n > 1 ? n : 1))
     return TB_ERROR_INVALID_VALUE;
-  TB_TRY(check_slices(S));
   if (n == 0) return TB_SUCCESS;
+  if (S <= 0) {
+    OzOperand a0, b0;
+    a0.X = A;
+    a0.ld = lda;
+    a0.rows = n;
+    a0.k = k;
+    b0 = a0;
+    b0.X = B;
+    b0.ld = ldb;
+    double spread = 0;
+    TB_TRY(oz_max_spread({a0, b0}, st, &spread));
+    S = oz_slices_for_spread(spread);
+  }
+  TB_TRY(check_slices(S));
   const long long kc_max = oz_kmax(S) / 2 / kOzBK * kOzBK;  // the concatenated K is twice the chunk
   const long long K1 = k > 0 ? k : 1;
   const long long kh = round_up(std::min<long long>(K1, kc_max), kOzBK);
@@ -1191,7 +1339,6 @@ tb_status ozaki_trmm_impl(bool upper, long m, long n, double alpha, const double
                           long ldb, double* C, long ldc, int S, cudaStream_t st) {
   if (m < 0 || n < 0 || lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1) || ldc < (m > 1 ? m : 1))
     return TB_ERROR_INVALID_VALUE;
-  TB_TRY(check_slices(S));
   if (m == 0 || n == 0) return TB_SUCCESS;
   OzOperand a, b;
   a.X = A;
@@ -1204,6 +1351,12 @@ tb_status ozaki_trmm_impl(bool upper, long m, long n, double alpha, const double
   b.rows = n;
   b.k = m;
   b.by_cols = true;
+  if (S <= 0) {
+    double spread = 0;
+    TB_TRY(oz_max_spread({a, b}, st, &spread));
+    S = oz_slices_for_spread(spread);
+  }
+  TB_TRY(check_slices(S));
   char* ws = static_cast<char*>(pool_get(oz_gemm_ws(m, n, m, S)));
   if (!ws) return TB_ERROR_ALLOC;
   return oz_gemm(a, b, m, upper ? KRange::kRowsUpper : KRange::kRowsLower, false, alpha, C, ldc, 0.0, S,
@@ -1349,14 +1502,17 @@ tb_status ozaki_trsm_impl(bool right, long m, long n, const double* A, long lda,
 // ------------------------------------------------------------------ C ABI
 namespace {
 bool is(char c, char u) { return c == u || c == u + ('a' - 'A'); }
-int slices_or_default(int s) { return s <= 0 ? 10 : s; }
+// TRSM: the products' operands (leaf inverses, X) exist only during the
+// solve, so a non-positive count selects 10 there; the other routines pass
+// it on and choose the count from their operands.
+int trsm_slices(int s) { return s <= 0 ? 10 : s; }
 }  // namespace
 
 extern "C" tb_status tb_dsyrk_ozaki(char uplo, char trans, long n, long k, double alpha, const double* A, long lda,
                                     double beta, double* C, long ldc, int slices) {
   if (!is(uplo, 'L') && !is(uplo, 'U')) return TB_ERROR_INVALID_VALUE;
   if (!is(trans, 'N') && !is(trans, 'T')) return TB_ERROR_INVALID_VALUE;
-  return tb::ozaki_syrk_impl(is(trans, 'T'), n, k, alpha, A, lda, beta, C, ldc, slices_or_default(slices), 0,
+  return tb::ozaki_syrk_impl(is(trans, 'T'), n, k, alpha, A, lda, beta, C, ldc, slices, 0,
                              nullptr, 0, tb::current_stream(), is(uplo, 'U'));
 }
 
@@ -1366,21 +1522,21 @@ extern "C" tb_status tb_dsyr2k_ozaki(char uplo, char trans, long n, long k, doub
     tb::set_last_error("tb_dsyr2k_ozaki: only uplo='L', trans='N' are supported");
     return TB_ERROR_NOT_SUPPORTED;
   }
-  return tb::ozaki_syr2k_impl(n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices_or_default(slices),
+  return tb::ozaki_syr2k_impl(n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices,
                               tb::current_stream());
 }
 
 extern "C" tb_status tb_dtrmm_ozaki(char uplo, long m, long n, double alpha, const double* A, long lda,
                                     const double* B, long ldb, double* C, long ldc, int slices) {
   if (!is(uplo, 'L') && !is(uplo, 'U')) return TB_ERROR_INVALID_VALUE;
-  return tb::ozaki_trmm_impl(is(uplo, 'U'), m, n, alpha, A, lda, B, ldb, C, ldc, slices_or_default(slices),
+  return tb::ozaki_trmm_impl(is(uplo, 'U'), m, n, alpha, A, lda, B, ldb, C, ldc, slices,
                              tb::current_stream());
 }
 
 extern "C" tb_status tb_dtrsm_ozaki(char side, long m, long n, const double* A, long lda, double* B, long ldb,
                                     long nb, int slices) {
   if (!is(side, 'R') && !is(side, 'L')) return TB_ERROR_INVALID_VALUE;
-  return tb::ozaki_trsm_impl(is(side, 'R'), m, n, A, lda, B, ldb, nb, slices_or_default(slices),
+  return tb::ozaki_trsm_impl(is(side, 'R'), m, n, A, lda, B, ldb, nb, trsm_slices(slices),
                              tb::current_stream());
 }
 
@@ -1413,7 +1569,7 @@ void report(const char* fn, tb_status s) {
 void tc_ozimmu_syrk(cublasHandle_t, long int n, long int k, double alpha, double* A, long int lda, double beta,
                     double* C, long int ldc, long int) {
   report("tc_ozimmu_syrk",
-         tb::ozaki_syrk_impl(false, n, k, alpha, A, lda, beta, C, ldc, 10, 0, nullptr, 0, tb::current_stream()));
+         tb::ozaki_syrk_impl(false, n, k, alpha, A, lda, beta, C, ldc, 0, 0, nullptr, 0, tb::current_stream()));
 }
 
 void tc_ozimmu_trsm(cublasHandle_t, long int m, long int n, double* A, long int lda, double* B, long int ldb,
@@ -1423,11 +1579,11 @@ void tc_ozimmu_trsm(cublasHandle_t, long int m, long int n, double* A, long int 
 
 void tc_ozimmu_trmm(cublasHandle_t, long int m, long int n, double alpha, double* A, long int lda, double* B,
                     long int ldb, double* C, long int ldc, long int) {
-  report("tc_ozimmu_trmm", tb::ozaki_trmm_impl(false, m, n, alpha, A, lda, B, ldb, C, ldc, 10, tb::current_stream()));
+  report("tc_ozimmu_trmm", tb::ozaki_trmm_impl(false, m, n, alpha, A, lda, B, ldb, C, ldc, 0, tb::current_stream()));
 }
 
 void tc_ozimmu_syr2k(cublasHandle_t, long int n, long int k, double alpha, double* A, long int lda, double* B,
                      long int ldb, double beta, double* C, long int ldc, long int) {
   report("tc_ozimmu_syr2k",
-         tb::ozaki_syr2k_impl(n, k, alpha, A, lda, B, ldb, beta, C, ldc, 10, tb::current_stream()));
+         tb::ozaki_syr2k_impl(n, k, alpha, A, lda, B, ldb, beta, C, ldc, 0, tb::current_stream()));
 }

@@ -1,10 +1,17 @@
 // Thin inline-PTX layer for sm_100a: mbarriers, TMA tile loads, tcgen05
 // (TMEM allocation, UMMA issue, commit, TMEM loads) and bounded waits.
 //
-// Every wait in this file is bounded: after TB_WAIT_TIMEOUT_NS of spinning it
-// records an error code in a caller-supplied global word, raises a shared
-// abort flag so the other warps of the CTA stop too, and returns false.
-// Nothing here traps.
+// Every wait in this file is bounded: after TB_WAIT_TIMEOUT_NS of spinning
+// (or the shorter limit a test sets in the error block, below) it records an
+// error code in a caller-supplied global word, raises a shared abort flag so
+// the other warps of the CTA stop too, and returns false. Nothing here traps.
+//
+// Device error block (16 bytes, 8-byte aligned; `err` points at word 0):
+//   word 0      error code (kDevErr*), 0 = none; the host reads and clears it
+//   word 1      test hook: 1 + the index of a tile whose operand loads the
+//               GEMM producers do not issue (0 = off), so that the waits for
+//               them run out; set only by tb_debug_stall
+//   words 2-3   wait limit in ns (0 = TB_WAIT_TIMEOUT_NS)
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -62,17 +69,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Wait limit of the bounded waits that report to error block `err`.
+__device__ __forceinline__ uint64_t wait_limit_ns(const int* err) {
+  if (!err) return TB_WAIT_TIMEOUT_NS;
+  const uint64_t v = *reinterpret_cast<const volatile unsigned long long*>(err + 2);
+  return v ? v : TB_WAIT_TIMEOUT_NS;
+}
+// The test hook of error block word 1: whether the producers skip tile `t`.
+__device__ __forceinline__ bool debug_stall_tile(const int* err, int t) {
+  return err && *reinterpret_cast<const volatile int*>(err + 1) == t + 1;
+}
+
 // Bounded wait on phase `parity`. `abort_flag` (shared) lets one timed-out
 // role release all others; `err` (global) records why.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
                                           int code) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
+  const uint64_t limit = wait_limit_ns(err);
   uint32_t n = 0;
   while (!mbar_try_wait(bar, parity)) {
     if ((++n & 255u) == 0) {
       if (*abort_flag) return false;
-      if (globaltimer_ns() - t0 > TB_WAIT_TIMEOUT_NS) {
+      if (globaltimer_ns() - t0 > limit) {
         *abort_flag = 1;
         if (err) atomicCAS(err, 0, code);
         return false;

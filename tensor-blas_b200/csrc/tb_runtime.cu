@@ -21,7 +21,8 @@ constexpr int kMaxDevices = 64;
 struct DeviceState {
   void* pool[kPoolSlots] = {};
   size_t pool_bytes[kPoolSlots] = {};
-  int* err = nullptr;
+  int* err = nullptr;        // the library's device error block (kErrBlockInts ints)
+  int* extra_err = nullptr;  // a second block of this device (the allocation-free entry point's)
   int sms = 0;
   cudaStream_t aux = nullptr;
 };
@@ -58,6 +59,15 @@ cudaEvent_t ev_get() {
 }  // namespace
 
 void note_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+
+namespace {
+std::atomic<unsigned long long> g_allocs{0};
+}  // namespace
+
+cudaError_t dev_malloc(void** p, size_t bytes) {
+  g_allocs.fetch_add(1, std::memory_order_relaxed);
+  return cudaMalloc(p, bytes);
+}
 
 bool profiling() { return g_prof_on; }
 
@@ -130,7 +140,7 @@ void* pool_get(size_t bytes, int slot) {
     s->pool_bytes[slot] = 0;
   }
   size_t want = (size_t)round_up((long long)bytes, 1 << 20);
-  if (cudaMalloc(&s->pool[slot], want) != cudaSuccess) {
+  if (dev_malloc(&s->pool[slot], want) != cudaSuccess) {
     cudaGetLastError();
     s->pool[slot] = nullptr;
     return nullptr;
@@ -139,29 +149,78 @@ void* pool_get(size_t bytes, int slot) {
   return s->pool[slot];
 }
 
+size_t pool_capacity(int slot) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceState* s = state();
+  return (s && slot >= 0 && slot < kPoolSlots) ? s->pool_bytes[slot] : 0;
+}
+
+size_t free_device_bytes() {
+  size_t f = 0, t = 0;
+  if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return f;
+}
+
+void release_pool() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceState* s = state();
+  if (!s) return;
+  for (int i = 0; i < kPoolSlots; ++i) {
+    if (s->pool[i]) cudaFree(s->pool[i]);
+    s->pool[i] = nullptr;
+    s->pool_bytes[i] = 0;
+  }
+}
+
 int* device_error_word() {
   std::lock_guard<std::mutex> lk(g_mu);
   DeviceState* s = state();
   if (!s) return nullptr;
   if (!s->err) {
-    if (cudaMalloc(&s->err, sizeof(int)) != cudaSuccess) {
+    if (dev_malloc(reinterpret_cast<void**>(&s->err), kErrBlockInts * sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
+      s->err = nullptr;
       return nullptr;
     }
-    cudaMemset(s->err, 0, sizeof(int));
+    cudaMemset(s->err, 0, kErrBlockInts * sizeof(int));
   }
   return s->err;
 }
 
+void register_error_block(int* block) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceState* s = state();
+  if (s) s->extra_err = block;
+}
+
+// The error blocks of the current device that exist (none is created here).
+static int error_blocks(int* out[2]) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceState* s = state();
+  int n = 0;
+  if (s && s->err) out[n++] = s->err;
+  if (s && s->extra_err) out[n++] = s->extra_err;
+  return n;
+}
+
 tb_status check_device_error(cudaStream_t stream) {
-  int* w = device_error_word();
   TB_CUDA_TRY(cudaStreamSynchronize(stream));
-  if (!w) return TB_SUCCESS;
-  int h = 0;
-  TB_CUDA_TRY(cudaMemcpy(&h, w, sizeof(int), cudaMemcpyDeviceToHost));
-  if (h != 0) {
-    cudaMemset(w, 0, sizeof(int));
-    set_last_error("device-side bounded wait timed out (code %d)", h);
+  int* blocks[2];
+  const int nb = error_blocks(blocks);
+  int code = 0;
+  for (int i = 0; i < nb; ++i) {
+    int h = 0;
+    TB_CUDA_TRY(cudaMemcpy(&h, blocks[i], sizeof(int), cudaMemcpyDeviceToHost));
+    if (h != 0) {
+      TB_CUDA_TRY(cudaMemset(blocks[i], 0, sizeof(int)));
+      if (!code) code = h;
+    }
+  }
+  if (code) {
+    set_last_error("device-side bounded wait timed out (code %d)", code);
     return TB_ERROR_TIMEOUT;
   }
   return TB_SUCCESS;
@@ -195,6 +254,28 @@ const char* tb_last_error(void) { return tb::g_last_error; }
 tb_status tb_synchronize(void) { return tb::check_device_error(tb::g_stream); }
 
 int tb_version(void) { return 100; }
+
+unsigned long long tb_alloc_count(void) { return tb::g_allocs.load(); }
+
+tb_status tb_release_scratch(void) {
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return tb::cuda_status(e);
+  tb::release_pool();
+  tb::release_tile_cache();
+  return TB_SUCCESS;
+}
+
+tb_status tb_debug_stall(long tile, unsigned long long wait_ns) {
+  if (tile < -1) return TB_ERROR_INVALID_VALUE;
+  // words 1-3 of every error block of this device (word 0, the code, is kept)
+  int* pool_block = tb::device_error_word();
+  if (!pool_block) return TB_ERROR_ALLOC;
+  int* blocks[2];
+  const int nb = tb::error_blocks(blocks);
+  int words[3] = {(int)(tile + 1), (int)(wait_ns & 0xffffffffull), (int)(wait_ns >> 32)};
+  for (int i = 0; i < nb; ++i) TB_CUDA_TRY(cudaMemcpy(blocks[i] + 1, words, sizeof(words), cudaMemcpyHostToDevice));
+  return TB_SUCCESS;
+}
 
 unsigned long long tb_launch_count(void) { return tb::g_launches.load(); }
 

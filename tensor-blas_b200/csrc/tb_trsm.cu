@@ -524,8 +524,16 @@ size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split) {
 }
 
 // Solves one right-hand side block with a prepared context: B is m' x n
-// (right side, m' <= the set-up m) or m x n' (left side, n' <= the set-up n).
+// (right side, m' <= the set-up m) or m x n' (left side, n' <= the set-up n):
+// one persistent launch for all the recursion's products where B's layout
+// allows it (tb_trsm_dag.cu), else one GEMM launch per leaf and update.
 tb_status trsm_solve(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols) {
+  if (trsm_dag_eligible(c, B, ldb)) return trsm_solve_dag(c, leaf_start, B, ldb, rows, cols);
+  return trsm_solve_launches(c, leaf_start, B, ldb, rows, cols);
+}
+
+tb_status trsm_solve_launches(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows,
+                              long cols) {
   if (ldb < (rows > 1 ? rows : 1)) return TB_ERROR_INVALID_VALUE;
   if (rows == 0 || cols == 0) return TB_SUCCESS;
   c.B = B;
@@ -547,8 +555,9 @@ tb_status trsm_solve_2s(TrsmCtx& c, const std::vector<long>& leaf_start, float* 
   // tile, their tails are short, and halving their tile counts cost more
   // than the overlap gained (measured at 16384: plain 6.36 -> 6.11 ms,
   // split 15.45 -> 15.65 ms)
+  if (trsm_dag_eligible(c, B, ldb)) return trsm_solve_dag(c, leaf_start, B, ldb, rows, cols);
   const cudaStream_t st2 = streams > 1 && span >= 4096 && c.split == Split::kPlain ? aux_stream() : nullptr;
-  if (!st2 || ldb < (rows > 1 ? rows : 1)) return trsm_solve(c, leaf_start, B, ldb, rows, cols);
+  if (!st2 || ldb < (rows > 1 ? rows : 1)) return trsm_solve_launches(c, leaf_start, B, ldb, rows, cols);
   const long half = round_up((span + 1) / 2, 128);
   // the second half's scratch: X and R are laid out along the split dimension
   TrsmCtx c2 = c;
@@ -566,9 +575,10 @@ tb_status trsm_solve_2s(TrsmCtx& c, const std::vector<long>& leaf_start, float* 
   if (cudaEventRecord(fork, c.st) != cudaSuccess || cudaStreamWaitEvent(st2, fork, 0) != cudaSuccess) {
     s1 = TB_ERROR_CUDA;
   } else {
-    s2 = c.right ? trsm_solve(c2, leaf_start, B + half, ldb, rows - half, cols)
-                 : trsm_solve(c2, leaf_start, B + half * ldb, ldb, rows, cols - half);
-    s1 = c.right ? trsm_solve(c, leaf_start, B, ldb, half, cols) : trsm_solve(c, leaf_start, B, ldb, rows, half);
+    s2 = c.right ? trsm_solve_launches(c2, leaf_start, B + half, ldb, rows - half, cols)
+                 : trsm_solve_launches(c2, leaf_start, B + half * ldb, ldb, rows, cols - half);
+    s1 = c.right ? trsm_solve_launches(c, leaf_start, B, ldb, half, cols)
+                 : trsm_solve_launches(c, leaf_start, B, ldb, rows, half);
     // the caller's stream continues only after both halves
     if (cudaEventRecord(join, st2) != cudaSuccess || cudaStreamWaitEvent(c.st, join, 0) != cudaSuccess)
       s1 = TB_ERROR_CUDA;

@@ -211,7 +211,7 @@ struct TuneScratch {
   }
   tb_status get(cudaStream_t st, float** out) {
     if (!p) {
-      if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      if (dev_malloc(reinterpret_cast<void**>(&p), bytes) != cudaSuccess) {
         cudaGetLastError();
         p = nullptr;
         set_last_error("autotune: cannot allocate %zu bytes of trial output", bytes);

@@ -82,6 +82,14 @@ lib.tb_autotune_get.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _c_long, _c_lo
                                 ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]
 lib.tb_autotune_get.restype = ctypes.c_int
 lib.tb_strsm_host.restype = ctypes.c_int
+lib.tb_alloc_count.argtypes = []
+lib.tb_alloc_count.restype = ctypes.c_ulonglong
+lib.tb_release_scratch.argtypes = []
+lib.tb_release_scratch.restype = ctypes.c_int
+lib.tb_debug_stall.argtypes = [_c_long, ctypes.c_ulonglong]
+lib.tb_debug_stall.restype = ctypes.c_int
+lib.tb_ssyrk_noalloc.argtypes = lib.tb_ssyrk.argtypes
+lib.tb_ssyrk_noalloc.restype = ctypes.c_int
 
 
 class TensorBLASError(RuntimeError):
@@ -266,6 +274,16 @@ def symm(A, B, alpha=1.0, beta=0.0, C=None, uplo="L", precision=PLAIN):
 
 def synchronize():
     _check(lib.tb_synchronize())
+
+
+def release_scratch():
+    """Wait for the device and free the library's scratch pool and cached tile lists."""
+    _check(lib.tb_release_scratch())
+
+
+def alloc_count():
+    """Device allocations the library has made in this process."""
+    return lib.tb_alloc_count()
 
 
 # ---------------------------------------------------------------- batched uneven instances

@@ -51,6 +51,46 @@ def test_reference_cpp_api_symbols(exported):
         assert n in exported, f"{n} declared in TensorBLAS.h but not exported"
 
 
+def _raw_exports():
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True, check=True).stdout
+    return {p[2] for p in (line.split() for line in out.splitlines()) if len(p) == 3 and p[1] in ("T", "W")}
+
+
+def test_full_mangled_signatures_match_compiled_reference():
+    """Every public entry point of the reference, compiled from its sources
+    (tests/golden/ref_cxx_symbols.txt, recorded by make_ref_symbols.py), is
+    exported under exactly the same mangled name, i.e. with the same
+    parameter types (a long/int mismatch, as in tc_symm's int ldb, would
+    change the name)."""
+    want = open(os.path.join(ROOT, "tests", "golden", "ref_cxx_symbols.txt")).read().split()
+    assert len(want) == 17
+    have = _raw_exports()
+    missing = [w for w in want if w not in have]
+    assert not missing, f"not exported with the reference's signature: {missing}"
+
+
+def test_symbol_fixture_is_current():
+    """When the reference build is present, the fixture still matches it."""
+    import importlib.util
+
+    ref = os.path.join(ROOT, "oracle", "_ref", "libTensorBLAS_ref.so")
+    if not os.path.exists(ref) or not os.path.isdir(os.path.join(ROOT, "oracle", "_ref", "cxx_sym")):
+        pytest.skip("reference build oracle/_ref not present")
+    spec = importlib.util.spec_from_file_location("make_ref_symbols",
+                                                  os.path.join(ROOT, "tests", "golden", "make_ref_symbols.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    want = open(os.path.join(ROOT, "tests", "golden", "ref_cxx_symbols.txt")).read().split()
+    assert mod.reference_symbols(ROOT) == want
+
+
+def test_diagnostic_entry_points_without_gpu(lib):
+    lib.tb_alloc_count.restype = __import__("ctypes").c_ulonglong
+    assert lib.tb_alloc_count() == 0  # nothing allocated without a device
+    lib.tb_debug_stall.argtypes = [__import__("ctypes").c_long, __import__("ctypes").c_ulonglong]
+    assert lib.tb_debug_stall(-2, 0) == 1  # TB_ERROR_INVALID_VALUE before any device access
+
+
 def test_no_cuda_driver_link():
     out = subprocess.run(["ldd", LIB], capture_output=True, text=True).stdout
     assert "libcuda.so" not in out and "libcublas" not in out

@@ -1,8 +1,9 @@
-"""Plain TRSMs with at least 4096 independent columns (left) or rows (right)
-are solved in two halves on two streams; each column's (row's) arithmetic is
-the same either way, so the result must be bit-identical to the one-stream
-solve. The stream count is read once per process (TB_TRSM_STREAMS), so each
-setting runs in its own subprocess."""
+"""On the launch-per-product path (TB_TRSM_DAG=0), plain TRSMs with at least
+4096 independent columns (left) or rows (right) are solved in two halves on
+two streams; each column's (row's) arithmetic is the same either way, so the
+result must be bit-identical to the one-stream solve. The stream count is
+read once per process (TB_TRSM_STREAMS), so each setting runs in its own
+subprocess."""
 import os
 import subprocess
 import sys
@@ -33,7 +34,7 @@ print(hashlib.sha1(X.tobytes()).hexdigest())
 
 
 def _digest(streams, side, m, n):
-    env = dict(os.environ, TB_TRSM_STREAMS=str(streams))
+    env = dict(os.environ, TB_TRSM_STREAMS=str(streams), TB_TRSM_DAG="0")
     out = subprocess.run([sys.executable, "-c", SCRIPT, os.path.join(ROOT, "tensor-blas_b200", "python"), side,
                           str(m), str(n)], env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
