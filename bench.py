@@ -888,9 +888,10 @@ def profile_ozaki(args):
 
 def profile_aux(args):
     """One plain SYRK and TRSM at n (FP32->FP16 conversions, 32x32 and leaf
-    inverses), one Ozaki DSYRK n=k=8192 with 10 slices (exponent and slicing
-    passes) and one FP8 SYR2K n=8192, k=4096 (block quantisation); nothing
-    timed."""
+    inverses), one Ozaki DSYRK n=k=n/2 with 10 slices (exponent, slicing and
+    level-fold passes) and one FP8 SYR2K n/2 x n/4 (block quantisation);
+    nothing timed. At n = 8192 the whole run holds about 2 GB on the device
+    (the size the ncu captures of these kernels use)."""
     import ctypes
 
     import TensorBLAS as TB
@@ -903,7 +904,7 @@ def profile_aux(args):
     TB.synchronize()
     del A, T, B0, C
     torch.cuda.empty_cache()
-    m = 8192
+    m = n // 2
     D = torch.randn(m, m, dtype=torch.float64, device="cuda")
     E = torch.zeros(m, m, dtype=torch.float64, device="cuda")
     L, P = ctypes.c_long, ctypes.c_void_p
@@ -911,10 +912,11 @@ def profile_aux(args):
                                       ctypes.c_int]
     TB._check(TB.lib.tb_dsyrk_ozaki(b"L", b"N", m, m, 1.0, D.data_ptr(), m, 0.0, E.data_ptr(), m, 10))
     del D, E
-    X = torch.randn(4096, m, device="cuda")
-    Y = torch.randn(4096, m, device="cuda")
+    kk = m // 2
+    X = torch.randn(kk, m, device="cuda")
+    Y = torch.randn(kk, m, device="cuda")
     Z = torch.zeros(m, m, device="cuda")
-    TB._check(TB.lib.tb_ssyr2k(b"L", b"N", m, 4096, 1.0, X.data_ptr(), m, Y.data_ptr(), m, 0.0, Z.data_ptr(), m, 256,
+    TB._check(TB.lib.tb_ssyr2k(b"L", b"N", m, kk, 1.0, X.data_ptr(), m, Y.data_ptr(), m, 0.0, Z.data_ptr(), m, 256,
                                TB.FP8))
     TB.synchronize()
     print("profile aux done", flush=True)

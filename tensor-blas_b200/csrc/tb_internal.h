@@ -233,10 +233,43 @@ struct TrsmCtx {
   __half *rh, *rl;  // current leaf block of B
   long long ldr;
   cudaStream_t st;
+  // persistent solve (tb_trsm_dag.cu): per-leaf operand copies of B (slice b
+  // holds leaf block b), progress counters, and whether the set-up launch
+  // already wrote the first copy and zeroed the counters for B = dag_B
+  __half *rfh = nullptr, *rfl = nullptr;
+  long long ldrf = 0;
+  int* dag_ctr = nullptr;
+  const float* dag_B = nullptr;
+  bool dag_prepped = false;
 };
+// Jobs of the one-launch TRSM preparation (trsm_prep_launch, tb_trsm.cu).
+struct PrepConv {  // fp32 rows x cols (lds) -> fp16 hi [lo] (ldd), triangle mode tri (convert_f32_f16)
+  long long rows = 0, cols = 0;
+  const float* src = nullptr;
+  long long lds = 0;
+  __half* hi = nullptr;
+  __half* lo = nullptr;
+  long long ldd = 0;
+  int tri = 0;
+};
+struct PrepJobs {
+  PrepConv conv[2];
+  int nconv = 0;
+  const float* A = nullptr;  // 32 x 32 FP64 inverses of A's diagonal (order n) into D
+  long long lda = 0, n = 0;
+  double* D = nullptr;
+  bool unit = false;
+  int* zero = nullptr;  // nzero ints set to 0
+  long long nzero = 0;
+};
+tb_status trsm_prep_launch(const PrepJobs& jobs, cudaStream_t st);
 // unit: A's diagonal is taken as 1 (diag = 'U'); the stored diagonal is never read.
+// B, ldb (optional): the right-hand side the first solve will take; when it
+// qualifies for the persistent solve, that solve's first operand copy and
+// counter zeroing join the set-up launch.
 tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long nb, Split split, cudaStream_t st,
-                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit = false);
+                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit = false,
+                     float* B = nullptr, long ldb = 0);
 size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split);
 tb_status trsm_solve(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
 // The recursion as one GEMM launch per leaf product and per update.
@@ -245,9 +278,12 @@ tb_status trsm_solve_launches(TrsmCtx& c, const std::vector<long>& leaf_start, f
 // The recursion as one persistent launch (tb_trsm_dag.cu): same tiles, K
 // ranges and accumulation order, scheduled on the device by progress
 // counters. Eligible when B can be written by TMA (16-byte aligned, ldb a
-// multiple of 4) and A has more than one leaf; TB_TRSM_DAG=0 in the
-// environment turns it off (read once).
+// multiple of 4) and A has more than one leaf, and switched on by
+// TB_TRSM_DAG=1 in the environment (read once).
 bool trsm_dag_eligible(const TrsmCtx& c, const float* B, long ldb);
+// Scratch, plan and preparation jobs (first operand copy, zeroed counters)
+// of the persistent solve of B with context c, added to `jobs`.
+tb_status trsm_dag_prepare(TrsmCtx& c, const float* B, long ldb, PrepJobs& jobs);
 tb_status trsm_solve_dag(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols);
 // The same solve with B's independent dimension (columns for the left side,
 // rows for the right side) split in two halves solved on the context's

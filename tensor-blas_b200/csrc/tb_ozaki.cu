@@ -158,20 +158,50 @@ __device__ __forceinline__ void oz_stat_publish(double ssq, long long cnt, int* 
   const double d = -0.5 * log2(ssq / (double)cnt);  // e_i - log2(rms_i) >= 0
   atomicMax(out, (int)ceil(d * 256.0));
 }
-// One thread per row (rows of a column-major matrix: coalesced across threads).
-__global__ void __launch_bounds__(64) oz_spread_rows_kernel(long long rows, long long k, const double* __restrict__ X,
-                                                            long long ldx, int mask, long long koff, int* out) {
-  const long long i = (long long)blockIdx.x * 64 + threadIdx.x;
-  if (i >= rows) return;
+// 32 rows per block (rows of a column-major matrix): lane l of warp w reads
+// row row0 + l at p = w, w + 8, ... (each warp load is 32 consecutive
+// rows), four loads in flight per thread; the eight warps' partial (m, ssq,
+// count) of a row are merged in warp order, so the result is deterministic.
+__global__ void __launch_bounds__(256) oz_spread_rows_kernel(long long rows, long long k, const double* __restrict__ X,
+                                                             long long ldx, int mask, long long koff, int* out) {
+  __shared__ int sm[8][32];
+  __shared__ double ss[8][32];
+  __shared__ long long sc[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long i = (long long)blockIdx.x * 32 + lane;
   int m = INT_MIN / 4;
   double ssq = 0.0;
   long long cnt = 0;
-  for (long long p = 0; p < k; ++p)
-    if (oz_keep(mask, i, p, koff)) {
-      oz_stat_add(m, ssq, X[i + p * ldx]);
-      ++cnt;
+  if (i < rows) {
+    long long p = warp;
+    for (; p + 24 < k; p += 32) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = X[i + (p + 8 * u) * ldx];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (oz_keep(mask, i, p + 8 * u, koff)) {
+          oz_stat_add(m, ssq, v[u]);
+          ++cnt;
+        }
     }
-  oz_stat_publish(ssq, cnt, out);
+    for (; p < k; p += 8)
+      if (oz_keep(mask, i, p, koff)) {
+        oz_stat_add(m, ssq, X[i + p * ldx]);
+        ++cnt;
+      }
+  }
+  sm[warp][lane] = m;
+  ss[warp][lane] = ssq;
+  sc[warp][lane] = cnt;
+  __syncthreads();
+  if (warp == 0 && i < rows) {
+    for (int w = 1; w < 8; ++w) {
+      oz_stat_merge(m, ssq, sm[w][lane], ss[w][lane]);
+      cnt += sc[w][lane];
+    }
+    oz_stat_publish(ssq, cnt, out);
+  }
 }
 // One warp per row (a column of X, contiguous in memory).
 __global__ void __launch_bounds__(256) oz_spread_cols_kernel(long long rows, long long k, const double* __restrict__ X,
@@ -1169,8 +1199,8 @@ tb_status oz_max_spread(const std::vector<OzOperand>& ops, cudaStream_t st, doub
     if (o.by_cols)
       oz_spread_cols_kernel<<<(unsigned)((o.rows + 7) / 8), 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff, w);
     else
-      oz_spread_rows_kernel<<<(unsigned)((o.rows + 63) / 64), 64, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff,
-                                                                          w);
+      oz_spread_rows_kernel<<<(unsigned)((o.rows + 31) / 32), 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff,
+                                                                           w);
     TB_CUDA_TRY(cudaGetLastError());
     note_launch();
   }

@@ -22,8 +22,10 @@
 //    the reference's recursion exactly.
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
+#include "tb_convert.cuh"
 #include "tb_internal.h"
 
 namespace tb {
@@ -38,9 +40,8 @@ constexpr int kLeafMax = 512;  // largest diagonal block inverted explicitly
 // from shared memory. Output: D[t*1024 + i + 32*c] (column-major 32x32).
 template <class T>
 __device__ __forceinline__ void diag_inv32_body(long long n, const T* __restrict__ A, long long lda,
-                                                double* __restrict__ D, long long t, bool unit = false) {
-  __shared__ double L[32][33];
-  const int c = threadIdx.x;
+                                                double* __restrict__ D, long long t, bool unit, double (*L)[33],
+                                                int c) {
   const long long base = t * 32;
   for (int i = 0; i < 32; ++i) {
     const long long gi = base + i, gj = base + c;
@@ -67,7 +68,60 @@ __device__ __forceinline__ void diag_inv32_body(long long n, const T* __restrict
 template <class T>
 __global__ void __launch_bounds__(32) diag_inv32_kernel(long long n, const T* __restrict__ A, long long lda,
                                                         double* __restrict__ D, bool unit) {
-  diag_inv32_body<T>(n, A, lda, D, blockIdx.x, unit);
+  __shared__ double L[32][33];
+  diag_inv32_body<T>(n, A, lda, D, blockIdx.x, unit, L, threadIdx.x);
+}
+
+// The preparation of a TRSM in one launch: FP32 -> FP16 conversions (A's
+// lower part, and for the persistent solve the first leaf block of B), the
+// 32 x 32 FP64 inverses of A's diagonal (warps 0..3 of a block, one
+// sub-block each) and the zeroing of an int array (the persistent solve's
+// progress counters), as consecutive ranges of one 1-D grid. Each job does
+// exactly what its own kernel would (same element arithmetic).
+struct PrepDev {
+  PrepConv conv[2];
+  int conv_vec[2];
+  long long conv_gx[2], conv_base[2], conv_blocks[2];
+  int nconv;
+  const float* A;
+  long long lda, n;
+  double* D;
+  int unit;
+  long long diag_base, diag_blocks;
+  int* zero;
+  long long nzero, zero_base, zero_blocks;
+};
+
+constexpr int kPrepThreads = 256;
+
+__global__ void __launch_bounds__(kPrepThreads) trsm_prep_kernel(const __grid_constant__ PrepDev p) {
+  __shared__ double L[4][32][33];
+  const long long b = blockIdx.x;
+  for (int z = 0; z < p.nconv; ++z)
+    if (b >= p.conv_base[z] && b < p.conv_base[z] + p.conv_blocks[z]) {
+      const long long local = b - p.conv_base[z], gx = p.conv_gx[z];
+      const long long gy = p.conv_blocks[z] / gx;
+      const PrepConv& c = p.conv[z];
+      if (p.conv_vec[z])
+        conv::convert8_body(local % gx, gx, local / gx, gy, c.rows, c.cols, c.src, c.lds, c.hi, c.lo, c.ldd, 2048.f,
+                            c.tri, 0);
+      else
+        conv::convert1_body(local % gx, gx, local / gx, gy, c.rows, c.cols, c.src, c.lds, c.hi, c.lo, c.ldd, 2048.f,
+                            c.tri, 0);
+      return;
+    }
+  if (b >= p.diag_base && b < p.diag_base + p.diag_blocks) {
+    const int warp = threadIdx.x >> 5;
+    if (warp >= 4) return;
+    const long long t = (b - p.diag_base) * 4 + warp;
+    if (t * 32 < p.n || (t == 0 && p.n == 0)) diag_inv32_body<float>(p.n, p.A, p.lda, p.D, t, p.unit != 0, L[warp],
+                                                                     threadIdx.x & 31);
+    return;
+  }
+  if (b >= p.zero_base && b < p.zero_base + p.zero_blocks) {
+    for (long long i = (b - p.zero_base) * kPrepThreads + threadIdx.x; i < p.nzero; i += p.zero_blocks * kPrepThreads)
+      p.zero[i] = 0;
+  }
 }
 
 // Grouped form: block b belongs to the job whose [first, first + count)
@@ -83,7 +137,8 @@ __global__ void __launch_bounds__(32) diag_inv32_grouped_kernel(const DiagJob* _
       hi = mid - 1;
   }
   const DiagJob& jb = jobs[lo];
-  diag_inv32_body<float>(jb.n, jb.A, jb.lda, jb.D, b - jb.first);
+  __shared__ double L[32][33];
+  diag_inv32_body<float>(jb.n, jb.A, jb.lda, jb.D, b - jb.first, false, L, threadIdx.x);
 }
 
 // Column chain j of the inverse of leaf block b (rows/cols [s, s+size)):
@@ -365,6 +420,54 @@ tb_status recurse(TrsmCtx& c, long s, long e, const std::vector<long>& leaf_star
 
 tb_status trsm_prepare_grouped() { return TB_SUCCESS; }
 
+tb_status trsm_prep_launch(const PrepJobs& j, cudaStream_t st) {
+  PrepDev p;
+  memset(&p, 0, sizeof(p));
+  long long next = 0;
+  for (int z = 0; z < j.nconv; ++z) {
+    const PrepConv& c = j.conv[z];
+    if (c.rows <= 0 || c.cols <= 0) continue;
+    const int k = p.nconv++;
+    p.conv[k] = c;
+    // the grid the conversion kernels would use (tb_convert.cu)
+    const bool vec = (c.rows % 8 == 0) && (c.lds % 4 == 0) && (c.ldd % 8 == 0) &&
+                     (reinterpret_cast<uintptr_t>(c.src) % 16 == 0) && (reinterpret_cast<uintptr_t>(c.hi) % 16 == 0) &&
+                     (c.lo == nullptr || reinterpret_cast<uintptr_t>(c.lo) % 16 == 0);
+    const long long units = vec ? c.rows / 8 : c.rows;
+    long long gx = (units + kPrepThreads - 1) / kPrepThreads;
+    if (gx > 1024) gx = 1024;
+    const long long gy = c.cols < 65535 ? c.cols : 65535;
+    p.conv_vec[k] = vec ? 1 : 0;
+    p.conv_gx[k] = gx;
+    p.conv_base[k] = next;
+    p.conv_blocks[k] = gx * gy;
+    next += gx * gy;
+  }
+  if (j.D && j.n > 0) {
+    p.A = j.A;
+    p.lda = j.lda;
+    p.n = j.n;
+    p.D = j.D;
+    p.unit = j.unit ? 1 : 0;
+    p.diag_base = next;
+    p.diag_blocks = ((j.n + 31) / 32 + 3) / 4;
+    next += p.diag_blocks;
+  }
+  if (j.zero && j.nzero > 0) {
+    p.zero = j.zero;
+    p.nzero = j.nzero;
+    p.zero_base = next;
+    p.zero_blocks = std::min<long long>((j.nzero + kPrepThreads - 1) / kPrepThreads, 64);
+    next += p.zero_blocks;
+  }
+  if (next == 0) return TB_SUCCESS;
+  if (next > 0x7fffffffLL) return TB_ERROR_NOT_SUPPORTED;
+  trsm_prep_kernel<<<(unsigned)next, kPrepThreads, 0, st>>>(p);
+  TB_CUDA_TRY(cudaGetLastError());
+  note_launch();
+  return TB_SUCCESS;
+}
+
 // Diagonal-block inverses of many triangular matrices in two launches.
 tb_status trsm_inverses_grouped(const DiagJob* d_diag, int ndiag, long long nblocks, const ChainJob* d_chain,
                                 int nchain, cudaStream_t st) {
@@ -449,7 +552,7 @@ TrsmLayout trsm_layout(TrsmCtx& c, long nleaf) {
 }  // namespace
 
 tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long nb, Split split, cudaStream_t st,
-                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit) {
+                     void* scratch, TrsmCtx& c, std::vector<long>& leaf_start, bool unit, float* B, long ldb) {
   if (m < 0 || n < 0 || nb <= 0) return TB_ERROR_INVALID_VALUE;
   const long nt = right ? n : m;
   if (lda < (nt > 1 ? nt : 1)) return TB_ERROR_INVALID_VALUE;
@@ -496,13 +599,31 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
   double* W64 = reinterpret_cast<double*>(ws + L.o_wg);
   TB_CUDA_TRY(cudaMemcpyAsync(dleaves, leaves.data(), nleaf * sizeof(int2), cudaMemcpyHostToDevice, st));
 
-  // 1. FP16 copy of A's lower part (only off-diagonal leaf blocks are read)
-  if (nleaf > 1) TB_TRY(convert_f32_f16(nt, nt, A, lda, c.ah, c.al, c.lda_h, 2048.f, 2, st));
+  // 1. one launch: the FP16 copy of A's lower part (only off-diagonal leaf
+  // blocks are read), the 32 x 32 FP64 inverses of its diagonal and, when B
+  // is known and takes the persistent solve, that solve's first operand copy
+  // and zeroed counters
+  PrepJobs jobs;
+  if (nleaf > 1) {
+    PrepConv& cv = jobs.conv[jobs.nconv++];
+    cv.rows = nt;
+    cv.cols = nt;
+    cv.src = A;
+    cv.lds = lda;
+    cv.hi = c.ah;
+    cv.lo = c.al;
+    cv.ldd = c.lda_h;
+    cv.tri = 2;
+  }
+  jobs.A = A;
+  jobs.lda = lda;
+  jobs.n = nt;
+  jobs.D = D;
+  jobs.unit = unit;
+  c.dag_prepped = false;
+  if (B && trsm_dag_eligible(c, B, ldb)) TB_TRY(trsm_dag_prepare(c, B, ldb, jobs));
+  TB_TRY(trsm_prep_launch(jobs, st));
   // 2. inverses of the diagonal leaf blocks (FP64), as FP16 hi/lo
-  const long nsub = (nt + 31) / 32;
-  diag_inv32_kernel<float><<<(unsigned)nsub, 32, 0, st>>>(nt, A, lda, D, unit);
-  TB_CUDA_TRY(cudaGetLastError());
-  note_launch();
   const int max_chain = (int)(leaf / 32);
   dim3 grid((unsigned)max_chain, (unsigned)nleaf);
   trtri_chain_kernel<<<grid, kChainThreads, 0, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride, W64);
@@ -596,7 +717,7 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   if (m == 0 || n == 0) return TB_SUCCESS;
   TrsmCtx c;
   std::vector<long> leaf_start;
-  TB_TRY(trsm_setup(right, m, n, A, lda, nb, split, st, nullptr, c, leaf_start));
+  TB_TRY(trsm_setup(right, m, n, A, lda, nb, split, st, nullptr, c, leaf_start, false, B, ldb));
   return trsm_solve_2s(c, leaf_start, B, ldb, m, n);
 }
 
@@ -726,7 +847,7 @@ tb_status trsm_ex_impl(bool right, bool upper, bool trans, bool unit, long m, lo
   if (rev) TB_TRY(reverse(m, n, B, ldb, right, st));
   TrsmCtx c;
   std::vector<long> leaf_start;
-  TB_TRY(trsm_setup(right, m, n, Ause, ldause, nb, split, st, ws + copy_bytes, c, leaf_start, unit));
+  TB_TRY(trsm_setup(right, m, n, Ause, ldause, nb, split, st, ws + copy_bytes, c, leaf_start, unit, B, ldb));
   TB_TRY(trsm_solve_2s(c, leaf_start, B, ldb, m, n));
   if (rev) TB_TRY(reverse(m, n, B, ldb, right, st));
   return TB_SUCCESS;

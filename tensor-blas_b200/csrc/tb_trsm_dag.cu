@@ -38,8 +38,9 @@
 // Tiles: plain updates 128 x 256 (FP16, one accumulator), split tiles
 // (leaf products, and updates of the split precision) 128 x 128 with hi/lo
 // operands and a correction accumulator folded into FP32 registers every
-// split_kchunk() K-blocks, as the GEMM engine does. Shared memory: three 64 KB
-// stages (a plain K-block uses 48 KB of one), two 16 KB epilogue chunks.
+// split_kchunk() K-blocks, as the GEMM engine does. Shared memory: 192 KB of
+// operand stages (four of 48 KB for plain solves, three of 64 KB for split
+// ones) and two 16 KB epilogue chunks.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -75,13 +76,17 @@ struct DagArgs {
   int kchunk;  // split tiles: K-blocks per round-to-nearest fold (the GEMM engine's, split_kchunk())
 };
 
-constexpr int kDagStages = 3;
-constexpr int kDagStageBytes = 65536;
+// Operand stages: plain solves (whose updates are plain 128 x 256 tiles,
+// 48 KB per K-block) use four 48 KB stages, and a split leaf K-block (64 KB:
+// hi and lo of both operands) spans two of them (A hi, A lo, B hi in the
+// first, B lo in the second); split solves use three 64 KB stages.
 constexpr int kDagABytes = 128 * 64 * 2;  // one 128-row x 64-deep FP16 operand block
+constexpr int kDagRingBytes = 3 * 65536;
 constexpr int kDagEpiBytes = 2 * 128 * 32 * 4;
 constexpr int kDagBarBytes = 512;
-constexpr int kDagSmem = kDagStages * kDagStageBytes + kDagEpiBytes + 1024 + kDagBarBytes;
+constexpr int kDagSmem = kDagRingBytes + kDagEpiBytes + 1024 + kDagBarBytes;
 static_assert(kDagSmem <= 232448, "shared memory budget");
+static_assert(4 * 3 * kDagABytes == kDagRingBytes, "four 48 KB stages fill the ring");
 constexpr int kDagThreads = 192;
 constexpr int kDevErrTimeoutDependency = 5;
 
@@ -115,16 +120,95 @@ __device__ __forceinline__ bool dep_wait(const int* ctr, int i, int target, vola
   return true;
 }
 
-template <bool A_MN, bool B_MN>
+// Brings the 128 x 32 box of a tensor at (x, y) into L2 (no shared memory).
+__device__ __forceinline__ void tma_prefetch_l2(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y)
+               : "memory");
+}
+
+// Epilogue of one tile, `nch` 128 x 32 chunks of C at (m0, y0 + 32c): the
+// same arithmetic per element as the GEMM engine's (alpha v + beta old, the
+// fp16 hi/lo side copies), staged in two shared-memory buffers and stored by
+// TMA. With beta != 0 the chunks of C are loaded two ahead: chunk c + 2 is
+// loaded into the buffer of chunk c as soon as chunk c's store has read it,
+// while chunk c + 1 is combined. Side copies leave through plain stores from
+// each thread's registers (a warp writes 32 consecutive rows per column), so
+// both buffers stay free for C; the caller fences them before it publishes
+// the tile. All 128 epilogue threads call it; `vals(c, v)` yields this
+// thread's 32 values of chunk c.
+struct DagEpi {
+  int chunk;        // chunks staged so far (selects the buffer)
+  uint32_t lphase;  // per-buffer phase of the C-load barriers
+};
+
+// Chunk c of the tile: waits for its C (beta != 0), combines, writes the
+// side copies, stages it and has the issuer store it (and request chunk
+// c + 2 into the same buffer).
+__device__ __forceinline__ void dag_chunk(const GemmArgs& P, const StoreK& sk, float* stage, uint64_t* cload,
+                                          DagEpi& ep, int m0, int y0, int c, int nch, int row, long long gi,
+                                          bool issuer, bool side_tile, volatile int* abort_flag, const float* v) {
+  const bool need = sk.beta != 0.0f;
+  const int b = ep.chunk & 1;
+  float* S = stage + b * (128 * 32);
+  const int gj0 = y0 + 32 * c;
+  float r[32];
+  if (need) {
+    mbar_wait(&cload[b], (ep.lphase >> b) & 1u, abort_flag, P.err, kDevErrTimeoutEpilogue);
+    ep.lphase ^= 1u << b;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      r[j] = fmaf(sk.beta, S[j * 128 + row], sk.alpha * v[j]);
+      S[j * 128 + row] = r[j];
+    }
+  } else {
+    if (issuer) bulk_wait_read<1>();  // the store that last used buffer b has read it
+    named_bar_sync(1, 128);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      r[j] = sk.alpha * v[j];
+      S[j * 128 + row] = r[j];
+    }
+  }
+  if (side_tile && gi < sk.out_m && gj0 < sk.out_n) store_fp16_copies(sk, r, gi, gj0);
+  fence_proxy_async_smem();
+  named_bar_sync(1, 128);
+  if (issuer) {
+    tma_store_2d(&P.mapC, S, m0, gj0);
+    bulk_commit();
+    if (need && c + 2 < nch) {
+      bulk_wait_read<0>();  // this chunk's store has read buffer b
+      mbar_arrive_expect_tx(&cload[b], 128 * 32 * 4);
+      tma_load_2d(S, &P.mapC, &cload[b], m0, gj0 + 64);
+    }
+  }
+  ++ep.chunk;
+}
+
+// Requests the first two chunks of C of a beta != 0 tile (issuer only).
+__device__ __forceinline__ void dag_first_loads(const GemmArgs& P, float* stage, uint64_t* cload, const DagEpi& ep,
+                                                int m0, int y0, int nch) {
+  bulk_wait_read<0>();  // earlier stores have read both buffers
+  for (int c = 0; c < 2 && c < nch; ++c) {
+    const int b = (ep.chunk + c) & 1;
+    mbar_arrive_expect_tx(&cload[b], 128 * 32 * 4);
+    tma_load_2d(stage + b * (128 * 32), &P.mapC, &cload[b], m0, y0 + 32 * c);
+  }
+}
+
+template <bool A_MN, bool B_MN, int NST>
 __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_constant__ DagArgs args) {
+  constexpr int SB = kDagRingBytes / NST;       // bytes per stage
+  constexpr bool SPLIT2 = SB < 4 * kDagABytes;  // a split K-block spans two stages
+  static_assert(SB >= 3 * kDagABytes, "a plain K-block fits one stage");
   constexpr uint32_t IDESC_PLAIN = idesc_f16(128, 256, false, A_MN, B_MN);
   constexpr uint32_t IDESC_SPLIT = idesc_f16(128, 128, false, A_MN, B_MN);
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  float* stage_c = reinterpret_cast<float*>(smem + kDagStages * kDagStageBytes);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kDagStages * kDagStageBytes + kDagEpiBytes);
-  uint64_t* empty = full + kDagStages;
-  uint64_t* tfull = empty + kDagStages;  // [2]
+  float* stage_c = reinterpret_cast<float*>(smem + kDagRingBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kDagRingBytes + kDagEpiBytes);
+  uint64_t* empty = full + NST;
+  uint64_t* tfull = empty + NST;  // [2]
   uint64_t* tempty = tfull + 2;          // [2]
   uint64_t* drain = tempty + 2;          // [1]
   uint64_t* cload = drain + 1;           // [2]
@@ -137,7 +221,7 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kDagStages; ++s) {
+    for (int s = 0; s < NST; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -197,36 +281,58 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
         fence_proxy_async_global();  // the data behind the counters, for the TMA loads below
         const GemmArgs& P = args.ops[task.meta.x];
         const bool split = task.meta.y != 0;
+        if (P.beta != 0.0f)  // the epilogue reads this tile of C: bring it into L2 while the MMAs run
+          for (int c0 = 0; c0 < (split ? 128 : 256) && task.tile.y + c0 < P.N; c0 += 32)
+            tma_prefetch_l2(&P.mapC, task.tile.x, task.tile.y + c0);
+        // claims the next stage: waits until it is free, records it for the abort path
+        auto take = [&](int& st_idx) -> bool {
+          if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) return false;
+          st_idx = s;
+          issued_mask |= 1u << s;
+          phase_mask = (phase_mask & ~(1u << s)) | (ph << s);
+          if (++s == NST) {
+            s = 0;
+            ph ^= 1u;
+          }
+          return true;
+        };
         for (int kb = task.tile.z; kb < task.tile.w; ++kb) {
-          if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, args.err, kDevErrTimeoutProducer)) {
+          const int k = P.k_off + kb * 64;
+          int s1 = 0, s2 = 0;
+          if (!take(s1)) {
             ok = false;
             break;
           }
-          uint8_t* st = smem + s * kDagStageBytes;
-          const int k = P.k_off + kb * 64;
+          uint8_t* st = smem + s1 * SB;
           if (split) {
-            mbar_arrive_expect_tx(&full[s], 4 * kDagABytes);
-            load_operand<A_MN, 128>(st, &P.mapA[0], &full[s], P.a_off + task.tile.x, k);
-            load_operand<A_MN, 128>(st + kDagABytes, &P.mapA[1], &full[s], P.a_off + task.tile.x, k);
-            load_operand<B_MN, 128>(st + 2 * kDagABytes, &P.mapB[0], &full[s], P.b_off + task.tile.y, k);
-            load_operand<B_MN, 128>(st + 3 * kDagABytes, &P.mapB[1], &full[s], P.b_off + task.tile.y, k);
+            uint8_t* st_lo = st + 3 * kDagABytes;
+            if (SPLIT2) {
+              if (!take(s2)) {
+                ok = false;
+                break;
+              }
+              st_lo = smem + s2 * SB;
+              mbar_arrive_expect_tx(&full[s1], 3 * kDagABytes);
+              mbar_arrive_expect_tx(&full[s2], kDagABytes);
+            } else {
+              mbar_arrive_expect_tx(&full[s1], 4 * kDagABytes);
+            }
+            uint64_t* bar_lo = SPLIT2 ? &full[s2] : &full[s1];
+            load_operand<A_MN, 128>(st, &P.mapA[0], &full[s1], P.a_off + task.tile.x, k);
+            load_operand<A_MN, 128>(st + kDagABytes, &P.mapA[1], &full[s1], P.a_off + task.tile.x, k);
+            load_operand<B_MN, 128>(st + 2 * kDagABytes, &P.mapB[0], &full[s1], P.b_off + task.tile.y, k);
+            load_operand<B_MN, 128>(st_lo, &P.mapB[1], bar_lo, P.b_off + task.tile.y, k);
           } else {
-            mbar_arrive_expect_tx(&full[s], 3 * kDagABytes);
-            load_operand<A_MN, 128>(st, &P.mapA[0], &full[s], P.a_off + task.tile.x, k);
-            load_operand<B_MN, 256>(st + kDagABytes, &P.mapB[0], &full[s], P.b_off + task.tile.y, k);
-          }
-          issued_mask |= 1u << s;
-          phase_mask = (phase_mask & ~(1u << s)) | (ph << s);
-          if (++s == kDagStages) {
-            s = 0;
-            ph ^= 1u;
+            mbar_arrive_expect_tx(&full[s1], 3 * kDagABytes);
+            load_operand<A_MN, 128>(st, &P.mapA[0], &full[s1], P.a_off + task.tile.x, k);
+            load_operand<B_MN, 256>(st + kDagABytes, &P.mapB[0], &full[s1], P.b_off + task.tile.y, k);
           }
         }
         t = t_next;
       }
       if (!ok) {
         // every copy in flight lands before the CTA exits
-        for (int i = 0; i < kDagStages; ++i) {
+        for (int i = 0; i < NST; ++i) {
           if (!((issued_mask >> i) & 1u)) continue;
           const uint64_t t0 = globaltimer_ns();
           while (!mbar_try_wait(&full[i], (phase_mask >> i) & 1u)) {
@@ -270,13 +376,25 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
           }
           tc_fence_after();
           const uint32_t d0 = tmem_base + (uint32_t)(buf * 256);
+          // waits for the next stage's operands
+          auto next_full = [&](int& st_idx) -> bool {
+            if (!mbar_wait(&full[s], ph, abort_flag, args.err, kDevErrTimeoutMma)) return false;
+            st_idx = s;
+            if (++s == NST) {
+              s = 0;
+              ph ^= 1u;
+            }
+            return true;
+          };
           for (int kb = c0; kb < c1; ++kb) {
-            if (!mbar_wait(&full[s], ph, abort_flag, args.err, kDevErrTimeoutMma)) {
+            int s1 = 0, s2 = 0;
+            if (!next_full(s1) || (split && SPLIT2 && !next_full(s2))) {
               ok = false;
               break;
             }
             tc_fence_after();
-            const uint32_t st = smem_u32(smem + s * kDagStageBytes);
+            const uint32_t st = smem_u32(smem + s1 * SB);
+            const uint32_t st_lo = (split && SPLIT2) ? smem_u32(smem + s2 * SB) : st + 3 * kDagABytes;
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
               const uint32_t acc = (kb > c0 || kk > 0) ? 1u : 0u;
@@ -284,7 +402,7 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
               if (split) {
                 const uint64_t db = operand_desc<B_MN>(st + 2 * kDagABytes, kk);
                 const uint64_t da_lo = operand_desc<A_MN>(st + kDagABytes, kk);
-                const uint64_t db_lo = operand_desc<B_MN>(st + 3 * kDagABytes, kk);
+                const uint64_t db_lo = operand_desc<B_MN>(st_lo, kk);
                 umma_f16(d0, da, db, IDESC_SPLIT, acc);
                 umma_f16(d0 + 128, da, db_lo, IDESC_SPLIT, acc);
                 umma_f16(d0 + 128, da_lo, db, IDESC_SPLIT, 1u);
@@ -293,11 +411,8 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
               }
             }
             any = true;
-            tc_commit(&empty[s]);
-            if (++s == kDagStages) {
-              s = 0;
-              ph ^= 1u;
-            }
+            tc_commit(&empty[s1]);
+            if (split && SPLIT2) tc_commit(&empty[s2]);
           }
           if (!ok) break;
           tc_commit(&tfull[buf]);
@@ -321,7 +436,7 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const bool issuer = (warp == 2 && lane == 0);
-    EpiState es{0, 0u, false};
+    DagEpi ep{0, 0u};
     int it = 0;
     int tq = 0;
     uint32_t tq_ph = 0;
@@ -340,32 +455,53 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
       const DagTask task = args.tasks[t];
       const GemmArgs& P = args.ops[task.meta.x];
       const bool split = task.meta.y != 0;
-      const bool need_load = P.beta != 0.0f;
-      if (issuer && need_load) {
-        // C (this tile of B) was last written by other CTAs' TMA stores
-        ld_acquire(args.ctr + (task.dep.z >= 0 ? task.dep.z : 0));
-        if (task.dep.x >= 0) ld_acquire(args.ctr + task.dep.x);
+      const int bn = split ? 128 : 256;
+      const int nch = min(bn, P.N - task.tile.y + 31) / 32;
+      // the tile writes fp16 side copies: rows below out_m and columns below out_n of the op
+      const bool side_tile = P.out_hi != nullptr && task.tile.x < P.out_m && task.tile.y < P.out_n;
+      if (issuer && P.beta != 0.0f) {
+        // C (this tile of B) was last written by the earlier updates of this
+        // tile on other CTAs: the producer hands the tile over before its own
+        // dependency wait, and the first C chunks are loaded before the
+        // accumulator is ready, so the epilogue waits for them itself
+        dep_wait(args.ctr, task.dep.z, task.dep.w, abort_flag, args.err);
         fence_proxy_async_global();
       }
       if (!split) {
         const int buf = it & 1;
         const uint32_t tph = (uint32_t)(it >> 1) & 1u;
         ++it;
-        if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) break;
+        // the first C chunks are requested before the accumulator is ready
+        const StoreK sk(P);
+        const long long gi = (long long)task.tile.x + row;
+        if (issuer && sk.beta != 0.0f) dag_first_loads(P, stage_c, cload, ep, task.tile.x, task.tile.y, nch);
+        if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) {
+          // gave up: the C loads requested above land before the CTA exits
+          if (issuer && sk.beta != 0.0f)
+            for (int c = 0; c < 2 && c < nch; ++c) {
+              const int b = (ep.chunk + c) & 1;
+              const uint64_t t0 = globaltimer_ns();
+              while (!mbar_try_wait(&cload[b], (ep.lphase >> b) & 1u))
+                if (globaltimer_ns() - t0 > 1000000000ull) {
+                  if (args.err) atomicCAS(args.err, 0, kDevErrTimeoutTeardown);
+                  break;
+                }
+            }
+          break;
+        }
         tc_fence_after();
         const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * 256);
 #pragma unroll 1
-        for (int c0 = 0; c0 < 256; c0 += 32) {
+        for (int c = 0; c < nch; ++c) {
           float v[32];
-          tmem_ld32(tacc + c0, v);
-          if (c0 == 256 - 32) {
+          tmem_ld32(tacc + 32 * c, v);
+          if (c == nch - 1) {  // the accumulator is read: hand it back to the MMA warp
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[buf]);
           }
-          if (task.tile.y + c0 < P.N)
-            epilogue_chunk_tma(P, stage_c, cload, es, v, task.tile.x, task.tile.y + c0, row, need_load, issuer,
-                               abort_flag);
+          dag_chunk(P, sk, stage_c, cload, ep, task.tile.x, task.tile.y, c, nch, row, gi, issuer, side_tile,
+                    abort_flag, v);
         }
       } else {
         float acc[128];
@@ -393,17 +529,24 @@ __global__ void __launch_bounds__(kDagThreads, 1) trsm_dag_kernel(const __grid_c
           if (lane == 0) mbar_arrive(&tempty[buf]);
         }
         if (!ok) break;
+        const StoreK sk(P);
+        const long long gi = (long long)task.tile.x + row;
+        if (issuer && sk.beta != 0.0f) dag_first_loads(P, stage_c, cload, ep, task.tile.x, task.tile.y, nch);
 #pragma unroll
-        for (int c0 = 0; c0 < 128; c0 += 32)
-          if (task.tile.y + c0 < P.N)
-            epilogue_chunk_tma(P, stage_c, cload, es, acc + c0, task.tile.x, task.tile.y + c0, row, need_load, issuer,
-                               abort_flag);
+        for (int c = 0; c < 4; ++c)
+          if (c < nch)
+            dag_chunk(P, sk, stage_c, cload, ep, task.tile.x, task.tile.y, c, nch, row, gi, issuer, side_tile,
+                      abort_flag, acc + 32 * c);
       }
-      if (issuer && task.meta.z >= 0) {
-        // the tile's stores (B and the side copies) have landed: publish
-        bulk_wait<0>();
-        fence_proxy_async_global();
-        red_release_add(args.ctr + task.meta.z, 1);
+      if (task.meta.z >= 0) {
+        // publish: every thread's side-copy stores, then the TMA stores, have landed
+        if (side_tile) __threadfence();
+        named_bar_sync(1, 128);
+        if (issuer) {
+          bulk_wait<0>();
+          fence_proxy_async_global();
+          red_release_add(args.ctr + task.meta.z, 1);
+        }
       }
     }
     if (issuer) bulk_wait<0>();
@@ -729,18 +872,18 @@ std::string check_plan(const DagPlan& plan, const std::vector<DagOp>& ops) {
 std::mutex g_plan_mu;
 std::map<PlanKey, DagPlan> g_plans;
 
-template <bool A_MN, bool B_MN>
+template <bool A_MN, bool B_MN, int NST>
 tb_status launch_dag(const DagArgs& a, int grid, cudaStream_t st, double flops) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    TB_CUDA_TRY(cudaFuncSetAttribute(trsm_dag_kernel<A_MN, B_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TB_CUDA_TRY(cudaFuncSetAttribute(trsm_dag_kernel<A_MN, B_MN, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      kDagSmem));
     attr_set[dev] = true;
   }
   void* tok = prof_begin(st);
-  trsm_dag_kernel<A_MN, B_MN><<<grid, kDagThreads, kDagSmem, st>>>(a);
+  trsm_dag_kernel<A_MN, B_MN, NST><<<grid, kDagThreads, kDagSmem, st>>>(a);
   TB_CUDA_TRY(cudaGetLastError());
   prof_end(tok, st, flops);
   note_launch();
@@ -749,11 +892,16 @@ tb_status launch_dag(const DagArgs& a, int grid, cudaStream_t st, double flops) 
 
 }  // namespace
 
+// Off by default: on a B200 the persistent solve of m = n = 16384 (nb 512)
+// took 7.8 ms against 6.3 ms for the launch-per-product recursion with its
+// two streams (its small tiles pay ~20 us each of epilogue and dependency
+// latency, and MMA and epilogue overlap poorly). TB_TRSM_DAG=1 in the
+// environment turns it on (read once).
 bool trsm_dag_enabled() {
   static int on = -1;
   if (on < 0) {
     const char* e = getenv("TB_TRSM_DAG");
-    on = (e && e[0] == '0') ? 0 : 1;
+    on = (e && e[0] == '1') ? 1 : 0;
   }
   return on == 1;
 }
@@ -767,49 +915,105 @@ bool trsm_dag_eligible(const TrsmCtx& c, const float* B, long ldb) {
   return c.nt > c.leaf;
 }
 
+namespace {
+
+// The persistent solve's scratch in pool slot 3: the per-leaf operand
+// copies (hi, lo), the counters (plus the claim counter) and the op
+// descriptors.
+struct DagScratch {
+  long long ldrf;
+  size_t rf_bytes, ctr_bytes, ops_bytes;
+};
+
+DagScratch dag_scratch(const TrsmCtx& c, const DagPlan& plan, size_t nops) {
+  DagScratch d;
+  // left: K-major, element (j, k) at [k + j * ld]; right: MN-major, element (i, k) at [i + k * ld]
+  d.ldrf = c.right ? round_up(c.m, 64) : round_up(c.nt, 64);
+  const long long rf_elems = d.ldrf * (c.right ? c.nt : c.n);
+  d.rf_bytes = (size_t)round_up(rf_elems * 2, 256);
+  d.ctr_bytes = (size_t)round_up((long long)(plan.num_counters + 1) * 4, 256);
+  d.ops_bytes = (size_t)round_up((long long)(nops * sizeof(GemmArgs)), 256);
+  return d;
+}
+
+const DagPlan& dag_plan(TrsmCtx& c, size_t* nops) {
+  const long indep = c.right ? c.m : c.n;
+  const int workers = sm_count();
+  const PlanKey key{c.right ? 1 : 0, indep, c.nt, c.leaf, c.split == Split::kHiLo ? 1 : 0, workers};
+  std::vector<DagOp> ops;  // shapes only: the plan does not depend on the buffers
+  build_ops(c, nullptr, nullptr, c.right ? round_up(c.m, 64) : round_up(c.nt, 64), 0, c.nt, ops);
+  *nops = ops.size();
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = g_plans.find(key);
+  if (it == g_plans.end()) it = g_plans.emplace(key, make_plan(c, ops, workers)).first;
+  return it->second;
+}
+
+}  // namespace
+
+tb_status trsm_dag_prepare(TrsmCtx& c, const float* B, long ldb, PrepJobs& jobs) {
+  size_t nops = 0;
+  const DagPlan& plan = dag_plan(c, &nops);
+  const DagScratch d = dag_scratch(c, plan, nops);
+  char* ws = static_cast<char*>(pool_get(2 * d.rf_bytes + d.ctr_bytes + d.ops_bytes, 3));
+  if (!ws) {
+    set_last_error("trsm: cannot allocate %zu bytes of scratch", 2 * d.rf_bytes + d.ctr_bytes + d.ops_bytes);
+    return TB_ERROR_ALLOC;
+  }
+  c.rfh = reinterpret_cast<__half*>(ws);
+  c.rfl = reinterpret_cast<__half*>(ws + d.rf_bytes);
+  c.ldrf = d.ldrf;
+  c.dag_ctr = reinterpret_cast<int*>(ws + 2 * d.rf_bytes);
+  if (jobs.nconv >= 2) return TB_ERROR_NOT_SUPPORTED;
+  // the first leaf's operand comes from B itself
+  PrepConv& cv = jobs.conv[jobs.nconv++];
+  const long nbl0 = std::min<long>(c.leaf, c.nt);
+  cv.rows = c.right ? c.m : nbl0;
+  cv.cols = c.right ? nbl0 : c.n;
+  cv.src = B;
+  cv.lds = ldb;
+  cv.hi = c.rfh;
+  cv.lo = c.rfl;
+  cv.ldd = d.ldrf;
+  cv.tri = 0;
+  jobs.zero = c.dag_ctr;
+  jobs.nzero = plan.num_counters + 1;
+  c.dag_B = B;
+  c.dag_prepped = true;
+  return TB_SUCCESS;
+}
+
 tb_status trsm_solve_dag(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols) {
   if (ldb < (rows > 1 ? rows : 1)) return TB_ERROR_INVALID_VALUE;
   if (rows == 0 || cols == 0) return TB_SUCCESS;
+  const long prep_m = c.m, prep_n = c.n;
   c.B = B;
   c.ldb = ldb;
   if (c.right)
     c.m = rows;
   else
     c.n = cols;
-  const long indep = c.right ? c.m : c.n;
-  // full-size FP16 hi/lo copy of B's leaf blocks (left: K-major, element
-  // (j, k) at [k + j * ld]; right: MN-major, element (i, k) at [i + k * ld])
-  const long long ldrf = c.right ? round_up(c.m, 64) : round_up(c.nt, 64);
-  const long long rf_elems = ldrf * (c.right ? c.nt : c.n);
-  const int workers = sm_count();
-  const PlanKey key{c.right ? 1 : 0, indep, c.nt, c.leaf, c.split == Split::kHiLo ? 1 : 0, workers};
-
-  std::vector<DagOp> ops;
-  __half* rfh = nullptr;
-  __half* rfl = nullptr;
-  // op descriptors are built with placeholder copies first to size the scratch
-  const size_t rf_bytes = (size_t)round_up(rf_elems * 2, 256);
-  build_ops(c, nullptr, nullptr, ldrf, 0, c.nt, ops);
-  const DagPlan* plan = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_plan_mu);
-    auto it = g_plans.find(key);
-    if (it == g_plans.end()) it = g_plans.emplace(key, make_plan(c, ops, workers)).first;
-    plan = &it->second;
+  // the set-up launch prepared this solve when it knew B (same B and shape);
+  // otherwise one preparation launch here
+  const bool prepped = c.dag_prepped && c.dag_B == B && prep_m == c.m && prep_n == c.n;
+  c.dag_prepped = false;
+  if (!prepped) {
+    PrepJobs jobs;
+    TB_TRY(trsm_dag_prepare(c, B, ldb, jobs));
+    c.dag_prepped = false;
+    TB_TRY(trsm_prep_launch(jobs, c.st));
   }
-  const size_t ctr_bytes = (size_t)round_up((long long)(plan->num_counters + 1) * 4, 256);
-  const size_t ops_bytes = (size_t)round_up((long long)(ops.size() * sizeof(GemmArgs)), 256);
-  char* ws = static_cast<char*>(pool_get(2 * rf_bytes + ctr_bytes + ops_bytes, 3));
-  if (!ws) {
-    set_last_error("trsm: cannot allocate %zu bytes of scratch", 2 * rf_bytes + ctr_bytes + ops_bytes);
+  size_t nops = 0;
+  const DagPlan& plan = dag_plan(c, &nops);
+  const DagScratch d = dag_scratch(c, plan, nops);
+  char* ws = static_cast<char*>(pool_get(2 * d.rf_bytes + d.ctr_bytes + d.ops_bytes, 3));
+  if (!ws || reinterpret_cast<__half*>(ws) != c.rfh) {
+    set_last_error("trsm: persistent-solve scratch moved between preparation and solve");
     return TB_ERROR_ALLOC;
   }
-  rfh = reinterpret_cast<__half*>(ws);
-  rfl = reinterpret_cast<__half*>(ws + rf_bytes);
-  int* ctr = reinterpret_cast<int*>(ws + 2 * rf_bytes);
-  GemmArgs* d_ops = reinterpret_cast<GemmArgs*>(ws + 2 * rf_bytes + ctr_bytes);
-  ops.clear();
-  build_ops(c, rfh, rfl, ldrf, 0, c.nt, ops);
+  GemmArgs* d_ops = reinterpret_cast<GemmArgs*>(ws + 2 * d.rf_bytes + d.ctr_bytes);
+  std::vector<DagOp> ops;
+  build_ops(c, c.rfh, c.rfl, c.ldrf, 0, c.nt, ops);
   std::vector<GemmArgs> hops(ops.size());
   double flops = 0;
   for (size_t i = 0; i < ops.size(); ++i) {
@@ -821,27 +1025,25 @@ tb_status trsm_solve_dag(TrsmCtx& c, const std::vector<long>& leaf_start, float*
   for (size_t i = 0; i < ops.size(); ++i)
     if (!hops[i].tma_c || (ops[i].call.out_hi && !hops[i].tma_out))
       return trsm_solve_launches(c, leaf_start, B, ldb, rows, cols);
-  const int4* d_tasks = upload_tiles(plan->packed, c.st);
+  const int4* d_tasks = upload_tiles(plan.packed, c.st);
   if (!d_tasks) return TB_ERROR_ALLOC;
   TB_CUDA_TRY(cudaMemcpyAsync(d_ops, hops.data(), hops.size() * sizeof(GemmArgs), cudaMemcpyHostToDevice, c.st));
-  TB_CUDA_TRY(cudaMemsetAsync(ctr, 0, (size_t)(plan->num_counters + 1) * 4, c.st));
-  // the first leaf's operand comes from B itself
-  const long nbl0 = std::min<long>(c.leaf, c.nt);
-  if (c.right)
-    TB_TRY(convert_f32_f16(c.m, nbl0, c.B, c.ldb, rfh, rfl, ldrf, 2048.f, 0, c.st));
-  else
-    TB_TRY(convert_f32_f16(nbl0, c.n, c.B, c.ldb, rfh, rfl, ldrf, 2048.f, 0, c.st));
   DagArgs a;
   a.ops = d_ops;
   a.tasks = reinterpret_cast<const DagTask*>(d_tasks);
-  a.num_tasks = plan->num_tasks;
-  a.claim = ctr + plan->num_counters;
-  a.ctr = ctr;
+  a.num_tasks = plan.num_tasks;
+  a.claim = c.dag_ctr + plan.num_counters;
+  a.ctr = c.dag_ctr;
   a.err = device_error_word();
   a.kchunk = split_kchunk();
-  const int grid = std::min(workers, plan->num_tasks);
-  if (c.right) return launch_dag<true, true>(a, grid, c.st, flops);
-  return launch_dag<true, false>(a, grid, c.st, flops);
+  const int grid = std::min(sm_count(), plan.num_tasks);
+  // plain solves: four 48 KB stages; split solves: three 64 KB stages
+  if (c.split == Split::kPlain) {
+    if (c.right) return launch_dag<true, true, 4>(a, grid, c.st, flops);
+    return launch_dag<true, false, 4>(a, grid, c.st, flops);
+  }
+  if (c.right) return launch_dag<true, true, 3>(a, grid, c.st, flops);
+  return launch_dag<true, false, 3>(a, grid, c.st, flops);
 }
 
 }  // namespace tb
