@@ -51,11 +51,14 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the other configurations")
     p.add_argument("--profile-step", action="store_true",
                    help="run one untimed step (plain, then split) and exit: the command profiled with ncu")
+    p.add_argument("--plain-only", action="store_true", help="--profile-step: the plain step alone")
     p.add_argument("--profile-aux", action="store_true",
                    help="run the non-GEMM kernels once each (conversions, TRSM leaf inverses, Ozaki slicing, FP8 "
                         "quantisation) at bench sizes and exit: the command their ncu summaries come from")
     p.add_argument("--profile-gemm", type=int, default=0, metavar="N",
                    help="run three plain N x N x N SGEMMs and exit (the GEMM-engine ncu captures)")
+    p.add_argument("--profile-syrk", type=int, default=0, metavar="N",
+                   help="run two plain SYRKs n = k = N and exit (the SYRK DRAM captures)")
     p.add_argument("--profile-ozaki", type=int, default=0, metavar="N",
                    help="run two FP64 Ozaki DSYRKs n = k = N with 8 slices and exit (the Ozaki-engine ncu captures)")
     return p.parse_args()
@@ -243,7 +246,7 @@ def run_mine(args, world, rank, local):
         TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, prec)
         TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, prec)
 
-    def timed(prec, steps, warmup, profile=False):
+    def timed(prec, steps, warmup):
         for _ in range(warmup):
             Bw.copy_(B0)
             step(prec)
@@ -252,8 +255,6 @@ def run_mine(args, world, rank, local):
         torch.cuda.synchronize()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         l0 = TB.lib.tb_launch_count()
-        if profile:
-            TB.lib.tb_profile_begin()
         for e0, e1 in evs:
             Bw.copy_(B0)                     # restore B (TRSM overwrites it); outside the event window
             e0.record(stream)
@@ -261,21 +262,16 @@ def run_mine(args, world, rank, local):
             e1.record(stream)
         torch.cuda.synchronize()
         launches = TB.lib.tb_launch_count() - l0
-        prof = None
-        if profile:
-            ms, fl, cnt = TB.ctypes.c_double(), TB.ctypes.c_double(), TB.ctypes.c_long()
-            TB.lib.tb_profile_end(TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
-            prof = (ms.value, fl.value, cnt.value)
         barrier(world)
         TB.synchronize()
         ms_total = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-        return ms_total, launches, prof
+        return ms_total, launches
 
 
     # ---- plain (headline), then chosen (split); clocks sampled over both timed regions
     sampler = Clocks(physical_gpu(local))
-    ms_plain, launches, prof = timed(TB.PLAIN, args.steps, args.warmup, profile=True)
-    ms_split, _, _ = timed(TB.SPLIT, args.steps, args.warmup)
+    ms_plain, launches = timed(TB.PLAIN, args.steps, args.warmup)
+    ms_split, _ = timed(TB.SPLIT, args.steps, args.warmup)
     clk = sampler.stop()
     ms_plain = max_over_ranks(ms_plain, world)
     ms_split = max_over_ranks(ms_split, world)
@@ -300,21 +296,22 @@ def run_mine(args, world, rank, local):
         trsm_only[name] = {"ms": ms_t, "tflops": float(n) ** 3 / (ms_t * 1e-3) / 1e12, "errors_vs_fp64": e}
 
     ms_syrk = _median_ms(lambda: TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN), 5)
-    # per-kernel rooflines: the step's two GEMM kernels timed on their own
-    # (event-timed launches between tb_profile_begin / end; 5 calls each)
+    # per-kernel rooflines: 5 plain steps (SYRK + TRSM) with every GEMM-engine
+    # launch event-timed on its own stream (tb_profile_begin / end), split by
+    # kernel (tb_profile_kernel): launch durations, algorithmic flops, launches
+    TB.lib.tb_profile_begin()
+    for _ in range(5):
+        Bw.copy_(B0)
+        step(TB.PLAIN)
+    torch.cuda.synchronize()
+    ms, fl, cnt = TB.ctypes.c_double(), TB.ctypes.c_double(), TB.ctypes.c_long()
+    TB.lib.tb_profile_end(TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
+    prof = (ms.value / 5, fl.value / 5, cnt.value / 5)
     kernels = {}
-    for name, call in (("syrk", lambda: TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN)),
-                       ("trsm", lambda: TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, TB.PLAIN))):
-        call()
-        TB.synchronize()
-        TB.lib.tb_profile_begin()
-        for _ in range(5):
-            Bw.copy_(B0)
-            call()
-        torch.cuda.synchronize()
-        ms, fl, cnt = TB.ctypes.c_double(), TB.ctypes.c_double(), TB.ctypes.c_long()
-        TB.lib.tb_profile_end(TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
-        kernels[name] = (ms.value / 5, fl.value / 5, cnt.value / 5)
+    for kind in range(4):
+        TB.lib.tb_profile_kernel(kind, TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
+        if cnt.value:
+            kernels[kind] = (ms.value / 5, fl.value / 5, cnt.value / 5)
 
     value = world * args.steps * flops_step / (ms_plain * 1e-3) / 1e12
     value_split = world * args.steps * flops_step / (ms_split * 1e-3) / 1e12
@@ -367,26 +364,32 @@ def run_mine(args, world, rank, local):
     burst, sustained, peak_src = measured_peaks()
     gemm_ms, gemm_flops, gemm_launches = prof
     tr = traffic_summary() or {}
-    names = {"syrk": "tb::gemm_pair_kernel (plain SYRK: one launch over the lower-triangle tile list)",
-             "trsm": "tb::trsm_dag_kernel (plain TRSM: one persistent launch for every leaf product and update)"}
+    names = {0: "tb::gemm_kernel (single-CTA tiles: TRSM leaf products and K <= 1024 updates)",
+             1: "tb::gemm_pair_kernel (CTA-pair 256 x 256 tiles: SYRK bands and long-K TRSM updates)",
+             2: "tb::trsm_dag_kernel (persistent TRSM solve)",
+             3: "tb::oz_* (Ozaki INT8 engine)"}
+    keys = {0: "gemm_kernel", 1: "gemm_pair_kernel", 2: "trsm_dag_kernel", 3: "ozaki"}
     per_kernel = {}
-    for key, (ms, fl, cnt) in kernels.items():
+    for kind, (ms, fl, cnt) in kernels.items():
         ach = fl / (ms * 1e-3) / 1e12 if ms > 0 else None
-        t = tr.get(key, {})
-        per_kernel[key] = {"bound": "tensor", "kernel": names[key], "achieved": ach, "peak": burst,
-                           "unit": "TFLOP/s", "frac": (ach / burst) if ach and burst else None,
-                           "ms_per_launch": ms / cnt if cnt else None, "launches_per_call": cnt,
-                           "flops_per_launch": fl / cnt if cnt else None,
-                           "traffic": t.get("bytes_per_launch"), "traffic_note": t.get("note")}
-    dominant = max(per_kernel, key=lambda k: kernels[k][0])
+        t = tr.get(keys[kind], {})
+        per_kernel[keys[kind]] = {
+            "bound": "tensor", "kernel": names[kind], "achieved": ach, "peak": burst, "unit": "TFLOP/s",
+            "frac": (ach / burst) if ach and burst else None, "launches_per_step": cnt,
+            "ms_per_step": ms, "flops_per_launch": fl / cnt if cnt else None,
+            "share_of_step_gemm_time": ms / sum(v[0] for v in kernels.values()),
+            "traffic": t.get("bytes_per_launch"), "traffic_note": t.get("note")}
+    dominant = keys[max(kernels, key=lambda k: kernels[k][0])]
     roof = dict(per_kernel[dominant])
-    roof.update({"peak_source": f"{peak_src} bf16_tflops (burst: each kernel timed alone; sustained {sustained})",
-                 "achieved_note": "algorithmic flops per launch (nominal BLAS3 counts of the tiles' products) / "
-                                  "the launch's CUDA-event duration, 5 calls",
+    roof.update({"peak_source": f"{peak_src} bf16_tflops (burst: each launch timed alone; sustained {sustained})",
+                 "achieved_note": "algorithmic flops of the kernel's launches in one plain step (nominal BLAS3 "
+                                  "counts of the tiles' products) / the device time during which at least one "
+                                  "of them ran (union of their CUDA-event intervals; the SYRK row bands and the "
+                                  "TRSM's two streams overlap launches), 5 steps",
                  "step_gemm": {"achieved": gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None,
-                               "launches_per_step": gemm_launches / args.steps,
-                               "note": "all GEMM launches of the timed step: flops / union of their intervals"},
-                 "other_kernel": per_kernel[[k for k in per_kernel if k != dominant][0]]})
+                               "launches_per_step": gemm_launches,
+                               "note": "all GEMM launches of the step: flops / union of their intervals"},
+                 "other_kernels": {k: v for k, v in per_kernel.items() if k != dominant}})
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_plain / args.steps, "higher_is_better": True,
@@ -833,19 +836,34 @@ def ctypes_P():
 
 
 def profile_step(args):
-    """One plain and one split step on fresh inputs, nothing timed (the
-    command the committed ncu summaries were captured from)."""
+    """One plain and one split step (plain only with --plain-only) on fresh
+    inputs, nothing timed (the command the committed ncu summaries were
+    captured from)."""
     import TensorBLAS as TB
 
     n = args.n
     A, T, B0 = make_inputs(n)
     C = torch.zeros(n, n, device="cuda")
-    for prec in (TB.PLAIN, TB.SPLIT):
+    for prec in (TB.PLAIN,) if args.plain_only else (TB.PLAIN, TB.SPLIT):
         Bw = B0.clone()
         TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, prec)
         TB.strsm("L", T, Bw, n, n, n, n, args.nb_trsm, prec)
         TB.synchronize()
     print("profile step done", flush=True)
+
+
+def profile_syrk(args):
+    """Two untimed plain SYRKs n = k = args.profile_syrk (lower, 'N', nb 256),
+    nothing timed: the command the SYRK DRAM captures come from."""
+    import TensorBLAS as TB
+
+    n = args.profile_syrk
+    A, _, _ = make_inputs(n)
+    C = torch.zeros(n, n, device="cuda")
+    for _ in range(2):
+        TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN)
+    TB.synchronize()
+    print("profile syrk done", flush=True)
 
 
 def profile_gemm(args):
@@ -933,6 +951,9 @@ def main():
         return
     if args.profile_ozaki:
         profile_ozaki(args)
+        return
+    if args.profile_syrk:
+        profile_syrk(args)
         return
     if args.profile_step:
         profile_step(args)

@@ -86,6 +86,12 @@ TB_API tb_status tb_debug_trsm_plan(char side, long m, long n, long nb, int prec
  * algorithmic flops, launches. */
 TB_API tb_status tb_profile_begin(void);
 TB_API tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launches);
+/* The launches of the last begin/end window by kernel: kind 0 the single-CTA
+ * GEMM kernel, 1 the CTA-pair GEMM kernel, 2 the persistent TRSM kernel, 3
+ * the Ozaki INT8 kernels. Device ms during which at least one launch of that
+ * kernel ran (the union of their intervals), their algorithmic flops and
+ * their number. */
+TB_API tb_status tb_profile_kernel(int kind, double* ms, double* flops, long* launches);
 
 /*
  * GEMM: C = alpha * op(A) * op(B) + beta * C, op(A) m x k, op(B) k x n, all
@@ -132,6 +138,11 @@ TB_API tb_status tb_autotune_put(const char* routine, const char* flags, long a,
                                  int engine, double ms);
 TB_API tb_status tb_autotune_get(const char* routine, const char* flags, long a, long b, int precision, long* nb,
                                  int* engine);
+/* The same with the split-K count of a plain 'N' SYRK (1: one pass). */
+TB_API tb_status tb_autotune_put_ex(const char* routine, const char* flags, long a, long b, int precision, long nb,
+                                    int engine, int splitk, double ms);
+TB_API tb_status tb_autotune_get_ex(const char* routine, const char* flags, long a, long b, int precision, long* nb,
+                                    int* engine, int* splitk);
 
 /*
  * TRSM with a lower-triangular, non-unit A, B overwritten by X:

@@ -6,6 +6,7 @@
 //
 // The split form writes hi = fp16(x) and lo = fp16((x - hi) * lo_scale), the
 // error-corrected FP16 pair of Ootomo & Yokota (IJHPCA 2022).
+#include <algorithm>
 #include "tb_convert.cuh"
 #include "tb_internal.h"
 
@@ -87,6 +88,9 @@ tb_status convert_f32_f16(long long rows, long long cols, const float* src, long
   long long gx = (units + threads - 1) / threads;
   if (gx > 1024) gx = 1024;
   long long gy = cols < 65535 ? cols : 65535;
+  // whole matrices on the vector path: about 16 blocks per SM, each thread
+  // walking many columns (convert8_body keeps four columns' loads in flight)
+  if (vec && tri == 0) gy = std::max<long long>(1, std::min<long long>(gy, (16LL * sm_count() + gx - 1) / gx));
   dim3 grid((unsigned)gx, (unsigned)gy);
   if (vec)
     convert8_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri, dup);

@@ -27,12 +27,71 @@ __device__ __forceinline__ uint32_t pack2(__half a, __half b) {
 // other triangle only within 256 of the diagonal.
 constexpr long long kTriBand = 256;
 
+// Eight converted values of one column to hi (and lo), and their copies `dup`
+// elements further on.
+__device__ __forceinline__ void store8(const float* f, __half* __restrict__ hi, __half* __restrict__ lo,
+                                       long long off, long long dup, float lo_scale) {
+  __half h[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) h[e] = __float2half_rn(f[e]);
+  uint4 o;
+  o.x = pack2(h[0], h[1]);
+  o.y = pack2(h[2], h[3]);
+  o.z = pack2(h[4], h[5]);
+  o.w = pack2(h[6], h[7]);
+  *reinterpret_cast<uint4*>(hi + off) = o;
+  if (dup) *reinterpret_cast<uint4*>(hi + dup + off) = o;
+  if (lo) {
+    __half l[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) l[e] = __float2half_rn((f[e] - __half2float(h[e])) * lo_scale);
+    uint4 q;
+    q.x = pack2(l[0], l[1]);
+    q.y = pack2(l[2], l[3]);
+    q.z = pack2(l[4], l[5]);
+    q.w = pack2(l[6], l[7]);
+    *reinterpret_cast<uint4*>(lo + off) = q;
+    if (dup) *reinterpret_cast<uint4*>(lo + dup + off) = q;
+  }
+}
+
 // Vector path: rows % 8 == 0, lds % 4 == 0, ldd % 8 == 0, 16-byte aligned bases.
+// Whole matrices (tri 0): a thread owns 8 rows and walks the columns by,
+// by + gy, ... four at a time, with the four columns' loads (128 bytes) in
+// flight together; grids of a few blocks per SM then keep enough bytes in
+// flight to run at the HBM rate.
 __device__ __forceinline__ void convert8_body(long long bx, long long gx, long long by, long long gy, long long rows,
                                               long long cols, const float* __restrict__ src, long long lds,
                                               __half* __restrict__ hi, __half* __restrict__ lo, long long ldd,
                                               float lo_scale, int tri, long long dup) {
   const long long rows8 = rows >> 3;
+  if (tri == 0) {
+    for (long long v = bx * blockDim.x + threadIdx.x; v < rows8; v += gx * blockDim.x) {
+      const long long i = v << 3;
+      long long j = by;
+      for (; j + 3 * gy < cols; j += 4 * gy) {
+        float4 a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float* s = src + i + (j + u * gy) * lds;
+          a[u] = ld_stream(s);
+          b[u] = ld_stream(s + 4);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float f[8] = {a[u].x, a[u].y, a[u].z, a[u].w, b[u].x, b[u].y, b[u].z, b[u].w};
+          store8(f, hi, lo, i + (j + u * gy) * ldd, dup, lo_scale);
+        }
+      }
+      for (; j < cols; j += gy) {
+        const float* s = src + i + j * lds;
+        const float4 a = ld_stream(s), b = ld_stream(s + 4);
+        const float f[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        store8(f, hi, lo, i + j * ldd, dup, lo_scale);
+      }
+    }
+    return;
+  }
   for (long long j = by; j < cols; j += gy) {
     long long v0 = bx * blockDim.x + threadIdx.x, vend = rows8;
     if (tri == 2) v0 += (j >> 3);  // rows i >= j (rounded down to 8)
@@ -52,28 +111,7 @@ __device__ __forceinline__ void convert8_body(long long bx, long long gx, long l
         for (int e = 0; e < 8; ++e)
           if (i + e > j) f[e] = 0.f;
       }
-      __half h[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) h[e] = __float2half_rn(f[e]);
-      uint4 o;
-      o.x = pack2(h[0], h[1]);
-      o.y = pack2(h[2], h[3]);
-      o.z = pack2(h[4], h[5]);
-      o.w = pack2(h[6], h[7]);
-      *reinterpret_cast<uint4*>(hi + i + j * ldd) = o;
-      if (dup) *reinterpret_cast<uint4*>(hi + dup + i + j * ldd) = o;
-      if (lo) {
-        __half l[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) l[e] = __float2half_rn((f[e] - __half2float(h[e])) * lo_scale);
-        uint4 q;
-        q.x = pack2(l[0], l[1]);
-        q.y = pack2(l[2], l[3]);
-        q.z = pack2(l[4], l[5]);
-        q.w = pack2(l[6], l[7]);
-        *reinterpret_cast<uint4*>(lo + i + j * ldd) = q;
-        if (dup) *reinterpret_cast<uint4*>(lo + dup + i + j * ldd) = q;
-      }
+      store8(f, hi, lo, i + j * ldd, dup, lo_scale);
     }
   }
 }

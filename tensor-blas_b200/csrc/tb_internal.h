@@ -30,9 +30,9 @@ void set_last_error(const char* fmt, ...);
 
 // ------------------------------------------------------------------ streams / pool
 cudaStream_t current_stream();
-// A second (non-blocking) stream per device for work the library splits in
-// two; joined back into the caller's stream before a routine returns.
-cudaStream_t aux_stream();
+// Two more (non-blocking) streams per device (i = 0, 1) for work the library
+// splits; joined back into the caller's stream before a routine returns.
+cudaStream_t aux_stream(int i = 0);
 // Device scratch owned by the library (grow-only, per device and slot).
 // Slot 0 serves the routines' own scratch; slot 1 the host-memory entry
 // points' staging buffers, which live across routine calls; slot 2 the Ozaki
@@ -65,9 +65,11 @@ size_t free_device_bytes();
 int sm_count();
 // Counts kernel launches issued by the library (tb_launch_count).
 void note_launch(int n = 1);
-// Event timing of GEMM-engine launches between tb_profile_begin/end.
+// Event timing of GEMM-engine launches between tb_profile_begin/end, by
+// kernel (the kinds of tb_profile_kernel).
+enum ProfKind { kProfGemm = 0, kProfPair = 1, kProfDag = 2, kProfOzaki = 3, kProfKinds = 4 };
 bool profiling();
-void* prof_begin(cudaStream_t st);
+void* prof_begin(cudaStream_t st, ProfKind kind);
 void prof_end(void* token, cudaStream_t st, double flops);
 
 inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
@@ -88,7 +90,7 @@ enum class Split { kPlain = 1, kHiLo = 3 };
 
 // Split products: K-blocks (of 64) the tensor core accumulates in TMEM
 // between two round-to-nearest folds into FP32 registers (its own FP32
-// accumulation truncates): 2 unless TB_SPLIT_KCHUNK (1..64) is set in the
+// accumulation truncates): 4 unless TB_SPLIT_KCHUNK (1..64) is set in the
 // environment (read once).
 int split_kchunk();
 
@@ -241,6 +243,9 @@ struct TrsmCtx {
   int* dag_ctr = nullptr;
   const float* dag_B = nullptr;
   bool dag_prepped = false;
+  // launch-per-product path: the set-up launch already wrote the first leaf's
+  // operand copy (rh / rl) from the B it was given
+  bool r0_ready = false;
 };
 // Jobs of the one-launch TRSM preparation (trsm_prep_launch, tb_trsm.cu).
 struct PrepConv {  // fp32 rows x cols (lds) -> fp16 hi [lo] (ldd), triangle mode tri (convert_f32_f16)
@@ -317,6 +322,17 @@ struct TuneChoice {
   long nb;
   int engine;  // 0 single-CTA tiles, 1 CTA pairs
   double ms;
+  int splitk = 1;  // SYRK: K parts of a split-K launch (1: one pass)
+};
+// Split-K SYRK of this thread (the autotuner's trials and choice): parts of
+// K, 1 = one pass. Applies to plain 'N' SYRKs of order <= kSplitKMaxN.
+constexpr long kSplitKMaxN = 4096;
+void set_splitk_override(int splits);
+int splitk_override();
+struct SplitKScope {
+  int saved;
+  explicit SplitKScope(int s) : saved(splitk_override()) { set_splitk_override(s); }
+  ~SplitKScope() { set_splitk_override(saved); }
 };
 std::string tune_key(const char* routine, const char* flags, long a, long b, int precision);
 // The cached choice for `key`, or the fastest of `candidates` under `trial`

@@ -158,47 +158,52 @@ __device__ __forceinline__ void oz_stat_publish(double ssq, long long cnt, int* 
   const double d = -0.5 * log2(ssq / (double)cnt);  // e_i - log2(rms_i) >= 0
   atomicMax(out, (int)ceil(d * 256.0));
 }
-// 32 rows per block (rows of a column-major matrix): lane l of warp w reads
-// row row0 + l at p = w, w + 8, ... (each warp load is 32 consecutive
-// rows), four loads in flight per thread; the eight warps' partial (m, ssq,
-// count) of a row are merged in warp order, so the result is deterministic.
+// 16 rows per block (rows of a column-major matrix): half-warp h of warp w
+// reads the 16 rows at column phase c = 2w + h, columns p = c, c + 16, ...
+// (each half-warp load is 128 contiguous bytes), eight loads in flight per
+// thread; the 16 phases' partial (m, ssq, count) of a row are merged in
+// phase order, so the result is deterministic.
 __global__ void __launch_bounds__(256) oz_spread_rows_kernel(long long rows, long long k, const double* __restrict__ X,
                                                              long long ldx, int mask, long long koff, int* out) {
-  __shared__ int sm[8][32];
-  __shared__ double ss[8][32];
-  __shared__ long long sc[8][32];
+  __shared__ int sm[16][16];
+  __shared__ double ss[16][16];
+  __shared__ long long sc[16][16];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long i = (long long)blockIdx.x * 32 + lane;
+  const int r = lane & 15, c = 2 * warp + (lane >> 4);
+  const long long i = (long long)blockIdx.x * 16 + r;
   int m = INT_MIN / 4;
   double ssq = 0.0;
   long long cnt = 0;
   if (i < rows) {
-    long long p = warp;
-    for (; p + 24 < k; p += 32) {
-      double v[4];
+    long long p = c;
+    for (; p + 7 * 16 < k; p += 8 * 16) {
+      double v[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = X[i + (p + 8 * u) * ldx];
+      for (int u = 0; u < 8; ++u) v[u] = __ldcs(X + i + (p + 16 * u) * ldx);
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (oz_keep(mask, i, p + 8 * u, koff)) {
+      for (int u = 0; u < 8; ++u)
+        if (oz_keep(mask, i, p + 16 * u, koff)) {
           oz_stat_add(m, ssq, v[u]);
           ++cnt;
         }
     }
-    for (; p < k; p += 8)
+    for (; p < k; p += 16)
       if (oz_keep(mask, i, p, koff)) {
         oz_stat_add(m, ssq, X[i + p * ldx]);
         ++cnt;
       }
   }
-  sm[warp][lane] = m;
-  ss[warp][lane] = ssq;
-  sc[warp][lane] = cnt;
+  sm[c][r] = m;
+  ss[c][r] = ssq;
+  sc[c][r] = cnt;
   __syncthreads();
-  if (warp == 0 && i < rows) {
-    for (int w = 1; w < 8; ++w) {
-      oz_stat_merge(m, ssq, sm[w][lane], ss[w][lane]);
-      cnt += sc[w][lane];
+  if (threadIdx.x < 16 && i < rows) {
+    m = sm[0][r];
+    ssq = ss[0][r];
+    cnt = sc[0][r];
+    for (int q = 1; q < 16; ++q) {
+      oz_stat_merge(m, ssq, sm[q][r], ss[q][r]);
+      cnt += sc[q][r];
     }
     oz_stat_publish(ssq, cnt, out);
   }
@@ -212,7 +217,19 @@ __global__ void __launch_bounds__(256) oz_spread_cols_kernel(long long rows, lon
   int m = INT_MIN / 4;
   double ssq = 0.0;
   long long cnt = 0;
-  for (long long p = lane; p < k; p += 32)
+  long long p = lane;
+  for (; p + 3 * 32 < k; p += 4 * 32) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = __ldcs(X + p + 32 * u + i * ldx);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (oz_keep(mask, i, p + 32 * u, koff)) {
+        oz_stat_add(m, ssq, v[u]);
+        ++cnt;
+      }
+  }
+  for (; p < k; p += 32)
     if (oz_keep(mask, i, p, koff)) {
       oz_stat_add(m, ssq, X[p + i * ldx]);
       ++cnt;
@@ -861,25 +878,49 @@ __global__ void __launch_bounds__(256) oz_fold_kernel(const int4* __restrict__ t
   const long long i = (long long)tile.x + (int)(threadIdx.x % tile_rows);
   if (i >= M) return;
   const int ei = oz_row_exp(eA, i);
-  for (int c = c0 + (int)(threadIdx.x / tile_rows); c < c0 + kOzFoldSlab; c += 256 / tile_rows) {
-    const long long j = (long long)tile.y + c;
-    if (j >= N || (tri == 1 && j > i)) break;  // columns only grow
-    if (tri == 2 && j < i) continue;
-    double* const cp = C + i + j * ldc;
-    if (empty) {
+  const int step = 256 / tile_rows;
+  if (empty) {
+    for (int c = c0 + (int)(threadIdx.x / tile_rows); c < c0 + kOzFoldSlab; c += step) {
+      const long long j = (long long)tile.y + c;
+      if (j >= N || (tri == 1 && j > i)) break;  // columns only grow
+      if (tri == 2 && j < i) continue;
+      double* const cp = C + i + j * ldc;
       if (b != 1.0) *cp = b == 0.0 ? 0.0 : b * *cp;
-      continue;
     }
-    const int ej = oz_row_exp(eB, j);
-    const int* const p = raw + i + j * ld_raw;
-    int v[kOzMaxSlices];
+    return;
+  }
+  // four columns per pass: every level sum and C value of the four is
+  // requested before the first fold, so S + 1 loads per column are in flight
+  // together (the per-element arithmetic and its order are unchanged)
+  constexpr int U = 4;
+  for (int cb = c0 + (int)(threadIdx.x / tile_rows); cb < c0 + kOzFoldSlab; cb += U * step) {
+    bool act[U];
+    long long jj[U];
+    int v[U][kOzMaxSlices];
+    double old[U];
 #pragma unroll
-    for (int l = 0; l < kOzMaxSlices; ++l) v[l] = l < S ? p[l * plane] : 0;
-    double acc = b * (b != 0.0 ? *cp : 0.0);
+    for (int u = 0; u < U; ++u) {
+      const int c = cb + u * step;
+      jj[u] = (long long)tile.y + c;
+      act[u] = c < c0 + kOzFoldSlab && jj[u] < N && !(tri == 1 && jj[u] > i) && !(tri == 2 && jj[u] < i);
+      old[u] = 0.0;
+      if (act[u]) {
+        const int* const p = raw + i + jj[u] * ld_raw;
 #pragma unroll
-    for (int l = 0; l < kOzMaxSlices; ++l)
-      if (l < S) acc = fma(alpha * pow2i(ei + ej - 7 * (l + 2)), (double)v[l], acc);
-    *cp = acc;
+        for (int l = 0; l < kOzMaxSlices; ++l) v[u][l] = l < S ? __ldcs(p + l * plane) : 0;
+        if (b != 0.0) old[u] = C[i + jj[u] * ldc];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!act[u]) continue;
+      const int ej = oz_row_exp(eB, jj[u]);
+      double acc = b * old[u];
+#pragma unroll
+      for (int l = 0; l < kOzMaxSlices; ++l)
+        if (l < S) acc = fma(alpha * pow2i(ei + ej - 7 * (l + 2)), (double)v[u][l], acc);
+      C[i + jj[u] * ldc] = acc;
+    }
   }
 }
 
@@ -1141,7 +1182,7 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
     TB_CUDA_TRY(cudaFuncSetAttribute(oz_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzPairSmem));
     attr[dev] = true;
   }
-  void* tok = prof_begin(st);
+  void* tok = prof_begin(st, kProfOzaki);
   if (pair) {
     const int pairs_max = sm_count() / 2;
     const int pairs = g.num_tiles < pairs_max ? g.num_tiles : pairs_max;
@@ -1199,7 +1240,7 @@ tb_status oz_max_spread(const std::vector<OzOperand>& ops, cudaStream_t st, doub
     if (o.by_cols)
       oz_spread_cols_kernel<<<(unsigned)((o.rows + 7) / 8), 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff, w);
     else
-      oz_spread_rows_kernel<<<(unsigned)((o.rows + 31) / 32), 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff,
+      oz_spread_rows_kernel<<<(unsigned)((o.rows + 15) / 16), 256, 0, st>>>(o.rows, o.k, o.X, o.ld, o.mask, o.koff,
                                                                            w);
     TB_CUDA_TRY(cudaGetLastError());
     note_launch();

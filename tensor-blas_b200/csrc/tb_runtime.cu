@@ -24,7 +24,7 @@ struct DeviceState {
   int* err = nullptr;        // the library's device error block (kErrBlockInts ints)
   int* extra_err = nullptr;  // a second block of this device (the allocation-free entry point's)
   int sms = 0;
-  cudaStream_t aux = nullptr;
+  cudaStream_t aux[2] = {nullptr, nullptr};
 };
 DeviceState g_dev[kMaxDevices];
 std::mutex g_mu;
@@ -42,7 +42,12 @@ std::atomic<unsigned long long> g_launches{0};
 struct ProfRec {
   cudaEvent_t a, b;
   double flops;
+  int kind;  // ProfKind
 };
+// Per kind, for the last tb_profile_end: the union of the launches'
+// intervals (ms), their flops and their number.
+double g_prof_kind_ms[kProfKinds], g_prof_kind_flops[kProfKinds];
+long g_prof_kind_n[kProfKinds];
 bool g_prof_on = false;
 std::vector<ProfRec> g_prof_live;     // recorded since tb_profile_begin
 std::vector<cudaEvent_t> g_ev_free;  // recycled events
@@ -71,12 +76,13 @@ cudaError_t dev_malloc(void** p, size_t bytes) {
 
 bool profiling() { return g_prof_on; }
 
-void* prof_begin(cudaStream_t st) {
+void* prof_begin(cudaStream_t st, ProfKind kind) {
   if (!g_prof_on) return nullptr;
   ProfRec r;
   r.a = ev_get();
   r.b = ev_get();
   r.flops = 0;
+  r.kind = (int)kind;
   cudaEventRecord(r.a, st);
   g_prof_live.push_back(r);
   return reinterpret_cast<void*>(g_prof_live.size());
@@ -104,15 +110,15 @@ tb_status cuda_status(cudaError_t e) {
 
 cudaStream_t current_stream() { return g_stream; }
 
-cudaStream_t aux_stream() {
+cudaStream_t aux_stream(int i) {
   DeviceState* s = state();
-  if (!s) return nullptr;
+  if (!s || i < 0 || i > 1) return nullptr;
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!s->aux && cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess) {
+  if (!s->aux[i] && cudaStreamCreateWithFlags(&s->aux[i], cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
-    s->aux = nullptr;
+    s->aux[i] = nullptr;
   }
-  return s->aux;
+  return s->aux[i];
 }
 
 int sm_count() {
@@ -285,30 +291,13 @@ tb_status tb_profile_begin(void) {
   return TB_SUCCESS;
 }
 
-tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launches) {
-  tb::g_prof_on = false;
-  double fl = 0;
-  long cnt = 0;
-  tb_status st = TB_SUCCESS;
-  // launch intervals relative to the first launch's start event; launches on
-  // different streams may overlap, so the device time is their union
-  std::vector<std::pair<double, double>> iv;
-  const cudaEvent_t ref = tb::g_prof_live.empty() ? nullptr : tb::g_prof_live.front().a;
-  for (auto& r : tb::g_prof_live)
-    if (cudaEventSynchronize(r.b) != cudaSuccess) st = TB_ERROR_CUDA;
-  for (auto& r : tb::g_prof_live) {
-    float t0 = 0, t1 = 0;
-    if (cudaEventElapsedTime(&t0, ref, r.a) == cudaSuccess && cudaEventElapsedTime(&t1, ref, r.b) == cudaSuccess) {
-      iv.push_back({t0, t1});
-      fl += r.flops;
-      ++cnt;
-    }
-  }
-  for (auto& r : tb::g_prof_live) {
-    tb::g_ev_free.push_back(r.a);
-    tb::g_ev_free.push_back(r.b);
-  }
-  tb::g_prof_live.clear();
+}  // extern "C"
+
+namespace tb {
+namespace {
+// Total length of the union of intervals (launches on several streams may
+// overlap; the device time is counted once).
+double union_ms(std::vector<std::pair<double, double>> iv) {
   std::sort(iv.begin(), iv.end());
   double ms = 0, cur0 = 0, cur1 = -1e300;
   for (const auto& x : iv) {
@@ -321,10 +310,61 @@ tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launche
     }
   }
   if (cur1 > cur0) ms += cur1 - cur0;
+  return ms;
+}
+}  // namespace
+}  // namespace tb
+
+extern "C" {
+tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launches) {
+  tb::g_prof_on = false;
+  double fl = 0;
+  long cnt = 0;
+  tb_status st = TB_SUCCESS;
+  // launch intervals relative to the first launch's start event; launches on
+  // different streams may overlap, so the device time is their union
+  std::vector<std::pair<double, double>> iv;
+  const cudaEvent_t ref = tb::g_prof_live.empty() ? nullptr : tb::g_prof_live.front().a;
+  for (auto& r : tb::g_prof_live)
+    if (cudaEventSynchronize(r.b) != cudaSuccess) st = TB_ERROR_CUDA;
+  for (int k = 0; k < tb::kProfKinds; ++k) {
+    tb::g_prof_kind_ms[k] = tb::g_prof_kind_flops[k] = 0;
+    tb::g_prof_kind_n[k] = 0;
+  }
+  std::vector<std::pair<double, double>> kind_iv[tb::kProfKinds];
+  for (auto& r : tb::g_prof_live) {
+    float t0 = 0, t1 = 0;
+    if (cudaEventElapsedTime(&t0, ref, r.a) == cudaSuccess && cudaEventElapsedTime(&t1, ref, r.b) == cudaSuccess) {
+      iv.push_back({t0, t1});
+      kind_iv[r.kind].push_back({t0, t1});
+      fl += r.flops;
+      ++cnt;
+      tb::g_prof_kind_flops[r.kind] += r.flops;
+      ++tb::g_prof_kind_n[r.kind];
+    }
+  }
+  for (auto& r : tb::g_prof_live) {
+    tb::g_ev_free.push_back(r.a);
+    tb::g_ev_free.push_back(r.b);
+  }
+  tb::g_prof_live.clear();
+  const double ms = tb::union_ms(iv);
+  for (int k = 0; k < tb::kProfKinds; ++k) tb::g_prof_kind_ms[k] = tb::union_ms(kind_iv[k]);
   if (gemm_ms) *gemm_ms = ms;
   if (gemm_flops) *gemm_flops = fl;
   if (gemm_launches) *gemm_launches = cnt;
   return st;
+}
+
+tb_status tb_profile_kernel(int kind, double* ms, double* flops, long* launches) {
+  if (kind < 0 || kind >= tb::kProfKinds) {
+    tb::set_last_error("tb_profile_kernel: kind %d out of range", kind);
+    return TB_ERROR_INVALID_VALUE;
+  }
+  if (ms) *ms = tb::g_prof_kind_ms[kind];
+  if (flops) *flops = tb::g_prof_kind_flops[kind];
+  if (launches) *launches = tb::g_prof_kind_n[kind];
+  return TB_SUCCESS;
 }
 
 }  // extern "C"

@@ -94,8 +94,14 @@ struct PrepDev {
 
 constexpr int kPrepThreads = 256;
 
+// Launches with the diagonal-inverse job get 4 x 32 x 33 doubles of dynamic
+// shared memory (the conversion-only launches none, so their blocks pack
+// densely on the SMs).
+constexpr int kPrepDiagSmem = 4 * 32 * 33 * (int)sizeof(double);
+
 __global__ void __launch_bounds__(kPrepThreads) trsm_prep_kernel(const __grid_constant__ PrepDev p) {
-  __shared__ double L[4][32][33];
+  extern __shared__ double prep_smem[];
+  double(*L)[32][33] = reinterpret_cast<double(*)[32][33]>(prep_smem);
   const long long b = blockIdx.x;
   for (int z = 0; z < p.nconv; ++z)
     if (b >= p.conv_base[z] && b < p.conv_base[z] + p.conv_blocks[z]) {
@@ -114,8 +120,7 @@ __global__ void __launch_bounds__(kPrepThreads) trsm_prep_kernel(const __grid_co
     const int warp = threadIdx.x >> 5;
     if (warp >= 4) return;
     const long long t = (b - p.diag_base) * 4 + warp;
-    if (t * 32 < p.n || (t == 0 && p.n == 0)) diag_inv32_body<float>(p.n, p.A, p.lda, p.D, t, p.unit != 0, L[warp],
-                                                                     threadIdx.x & 31);
+    if (t * 32 < p.n) diag_inv32_body<float>(p.n, p.A, p.lda, p.D, t, p.unit != 0, L[warp], threadIdx.x & 31);
     return;
   }
   if (b >= p.zero_base && b < p.zero_base + p.zero_blocks) {
@@ -311,7 +316,7 @@ tb_status leaf_solve(TrsmCtx& c, int bidx, long s, long e) {
   GemmCall g;
   g.split = Split::kHiLo;
   const bool split_x = c.split == Split::kHiLo;
-  const bool need_convert = (s == 0);
+  const bool need_convert = (s == 0) && !c.r0_ready;  // the set-up launch may have converted it
   if (c.right) {
     // R = B[:, s:e] (m x nbl) -> FP16 hi/lo; X_b = R * W^T
     if (need_convert) TB_TRY(convert_f32_f16(c.m, nbl, c.B + s * c.ldb, c.ldb, c.rh, c.rl, c.ldr, 2048.f, 0, c.st));
@@ -436,7 +441,8 @@ tb_status trsm_prep_launch(const PrepJobs& j, cudaStream_t st) {
     const long long units = vec ? c.rows / 8 : c.rows;
     long long gx = (units + kPrepThreads - 1) / kPrepThreads;
     if (gx > 1024) gx = 1024;
-    const long long gy = c.cols < 65535 ? c.cols : 65535;
+    long long gy = c.cols < 65535 ? c.cols : 65535;
+    if (vec && c.tri == 0) gy = std::max<long long>(1, std::min<long long>(gy, (16LL * sm_count() + gx - 1) / gx));
     p.conv_vec[k] = vec ? 1 : 0;
     p.conv_gx[k] = gx;
     p.conv_base[k] = next;
@@ -462,7 +468,7 @@ tb_status trsm_prep_launch(const PrepJobs& j, cudaStream_t st) {
   }
   if (next == 0) return TB_SUCCESS;
   if (next > 0x7fffffffLL) return TB_ERROR_NOT_SUPPORTED;
-  trsm_prep_kernel<<<(unsigned)next, kPrepThreads, 0, st>>>(p);
+  trsm_prep_kernel<<<(unsigned)next, kPrepThreads, p.diag_blocks > 0 ? kPrepDiagSmem : 0, st>>>(p);
   TB_CUDA_TRY(cudaGetLastError());
   note_launch();
   return TB_SUCCESS;
@@ -599,13 +605,13 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
   double* W64 = reinterpret_cast<double*>(ws + L.o_wg);
   TB_CUDA_TRY(cudaMemcpyAsync(dleaves, leaves.data(), nleaf * sizeof(int2), cudaMemcpyHostToDevice, st));
 
-  // 1. one launch: the FP16 copy of A's lower part (only off-diagonal leaf
-  // blocks are read), the 32 x 32 FP64 inverses of its diagonal and, when B
-  // is known and takes the persistent solve, that solve's first operand copy
-  // and zeroed counters
-  PrepJobs jobs;
+  // 1. on the caller's stream, one conversion launch: the FP16 copy of A's
+  // lower part (only off-diagonal leaf blocks are read) and, when B is known,
+  // the first leaf's operand copy (the persistent solve's, with its zeroed
+  // counters, when B takes that path)
+  PrepJobs conv;
   if (nleaf > 1) {
-    PrepConv& cv = jobs.conv[jobs.nconv++];
+    PrepConv& cv = conv.conv[conv.nconv++];
     cv.rows = nt;
     cv.cols = nt;
     cv.src = A;
@@ -615,21 +621,58 @@ tb_status trsm_setup(bool right, long m, long n, const float* A, long lda, long 
     cv.ldd = c.lda_h;
     cv.tri = 2;
   }
-  jobs.A = A;
-  jobs.lda = lda;
-  jobs.n = nt;
-  jobs.D = D;
-  jobs.unit = unit;
   c.dag_prepped = false;
-  if (B && trsm_dag_eligible(c, B, ldb)) TB_TRY(trsm_dag_prepare(c, B, ldb, jobs));
-  TB_TRY(trsm_prep_launch(jobs, st));
-  // 2. inverses of the diagonal leaf blocks (FP64), as FP16 hi/lo
-  const int max_chain = (int)(leaf / 32);
-  dim3 grid((unsigned)max_chain, (unsigned)nleaf);
-  trtri_chain_kernel<<<grid, kChainThreads, 0, st>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride, W64);
-  TB_CUDA_TRY(cudaGetLastError());
-  note_launch();
-  return TB_SUCCESS;
+  c.r0_ready = false;
+  if (B && trsm_dag_eligible(c, B, ldb)) {
+    TB_TRY(trsm_dag_prepare(c, B, ldb, conv));
+  } else if (B) {
+    PrepConv& cv = conv.conv[conv.nconv++];
+    const long nbl0 = std::min<long>(leaf, nt);
+    cv.rows = right ? m : nbl0;
+    cv.cols = right ? nbl0 : n;
+    cv.src = B;
+    cv.lds = ldb;
+    cv.hi = c.rh;
+    cv.lo = c.rl;
+    cv.ldd = c.ldr;
+    c.r0_ready = true;
+  }
+  // 2. beside it, on an auxiliary stream: the 32 x 32 FP64 inverses of A's
+  // diagonal and the leaf chains (they read only A and each other), joined
+  // back into the caller's stream before the solve
+  const cudaStream_t sa = aux_stream(1);
+  cudaEvent_t fork = nullptr, join = nullptr;
+  if (sa) {
+    TB_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    TB_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  }
+  const cudaStream_t si = sa ? sa : st;
+  tb_status rs = TB_SUCCESS;
+  if (sa && (cudaEventRecord(fork, st) != cudaSuccess || cudaStreamWaitEvent(sa, fork, 0) != cudaSuccess))
+    rs = TB_ERROR_CUDA;
+  if (rs == TB_SUCCESS) {
+    PrepJobs inv;
+    inv.A = A;
+    inv.lda = lda;
+    inv.n = nt;
+    inv.D = D;
+    inv.unit = unit;
+    rs = trsm_prep_launch(inv, si);
+  }
+  if (rs == TB_SUCCESS) {
+    const int max_chain = (int)(leaf / 32);
+    dim3 grid((unsigned)max_chain, (unsigned)nleaf);
+    trtri_chain_kernel<<<grid, kChainThreads, 0, si>>>(A, lda, dleaves, D, c.wh, c.wl, c.ldw, c.wstride, W64);
+    if (cudaGetLastError() != cudaSuccess) rs = TB_ERROR_CUDA;
+    note_launch();
+  }
+  if (rs == TB_SUCCESS) rs = trsm_prep_launch(conv, st);
+  if (sa && (cudaEventRecord(join, sa) != cudaSuccess || cudaStreamWaitEvent(st, join, 0) != cudaSuccess) &&
+      rs == TB_SUCCESS)
+    rs = TB_ERROR_CUDA;
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+  return rs;
 }
 
 size_t trsm_scratch_bytes(bool right, long m, long n, long nb, Split split) {
@@ -718,7 +761,9 @@ tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float*
   TrsmCtx c;
   std::vector<long> leaf_start;
   TB_TRY(trsm_setup(right, m, n, A, lda, nb, split, st, nullptr, c, leaf_start, false, B, ldb));
-  return trsm_solve_2s(c, leaf_start, B, ldb, m, n);
+  const tb_status rs = trsm_solve_2s(c, leaf_start, B, ldb, m, n);
+  c.r0_ready = false;
+  return rs;
 }
 
 
@@ -849,6 +894,7 @@ tb_status trsm_ex_impl(bool right, bool upper, bool trans, bool unit, long m, lo
   std::vector<long> leaf_start;
   TB_TRY(trsm_setup(right, m, n, Ause, ldause, nb, split, st, ws + copy_bytes, c, leaf_start, unit, B, ldb));
   TB_TRY(trsm_solve_2s(c, leaf_start, B, ldb, m, n));
+  c.r0_ready = false;
   if (rev) TB_TRY(reverse(m, n, B, ldb, right, st));
   return TB_SUCCESS;
 }

@@ -882,7 +882,7 @@ tb_status launch_dag(const DagArgs& a, int grid, cudaStream_t st, double flops) 
                                      kDagSmem));
     attr_set[dev] = true;
   }
-  void* tok = prof_begin(st);
+  void* tok = prof_begin(st, kProfDag);
   trsm_dag_kernel<A_MN, B_MN, NST><<<grid, kDagThreads, kDagSmem, st>>>(a);
   TB_CUDA_TRY(cudaGetLastError());
   prof_end(tok, st, flops);

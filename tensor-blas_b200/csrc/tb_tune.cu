@@ -11,9 +11,12 @@
 // so one file can serve several machines.
 //
 // Knobs: the GEMM engine (1: 256 x 256 tiles on CTA pairs for the large
-// plain launches, 0: single-CTA tiles), and for TRSM the leaf size nb (128,
+// plain launches, 0: single-CTA tiles); for TRSM the leaf size nb (128,
 // 256, 512), which sets the recursion's leaf inverses and the number of
-// update launches. SYRK, SYR2K and TRMM do not use nb.
+// update launches (SYRK, SYR2K and TRMM do not use nb); and for plain 'N'
+// SYRKs whose triangle has fewer 128 x 256 tiles than the GPU has SMs (small
+// n, long k) the split-K count (2 to 16 parts of K in one grouped launch plus
+// a reduction), which fills the SMs the one-pass launch leaves idle.
 #include <unistd.h>
 
 #include <cstdio>
@@ -58,9 +61,13 @@ void load_locked() {
   while (fgets(line, sizeof(line), f)) {
     char key[512];
     TuneChoice c{};
-    if (sscanf(line, " {\"key\": \"%511[^\"]\", \"nb\": %ld, \"engine\": %d, \"ms\": %lf}", key, &c.nb, &c.engine,
-               &c.ms) == 4)
+    if (sscanf(line, " {\"key\": \"%511[^\"]\", \"nb\": %ld, \"engine\": %d, \"splitk\": %d, \"ms\": %lf}", key,
+               &c.nb, &c.engine, &c.splitk, &c.ms) == 5 ||
+        sscanf(line, " {\"key\": \"%511[^\"]\", \"nb\": %ld, \"engine\": %d, \"ms\": %lf}", key, &c.nb, &c.engine,
+               &c.ms) == 4) {
+      if (c.splitk < 1) c.splitk = 1;
       g_cache[key] = c;
+    }
   }
   fclose(f);
 }
@@ -77,8 +84,9 @@ tb_status save_locked() {
   fprintf(f, "{\n \"format\": \"tensorblas-autotune-1\",\n \"entries\": [\n");
   size_t i = 0;
   for (const auto& kv : g_cache)
-    fprintf(f, "  {\"key\": \"%s\", \"nb\": %ld, \"engine\": %d, \"ms\": %.6f}%s\n", kv.first.c_str(), kv.second.nb,
-            kv.second.engine, kv.second.ms, ++i < g_cache.size() ? "," : "");
+    fprintf(f, "  {\"key\": \"%s\", \"nb\": %ld, \"engine\": %d, \"splitk\": %d, \"ms\": %.6f}%s\n",
+            kv.first.c_str(), kv.second.nb, kv.second.engine, kv.second.splitk, kv.second.ms,
+            ++i < g_cache.size() ? "," : "");
   fprintf(f, " ]\n}\n");
   const bool ok = fflush(f) == 0 && fsync(fileno(f)) == 0;
   fclose(f);
@@ -126,6 +134,7 @@ tb_status autotune(const std::string& key, const std::vector<TuneChoice>& candid
   tb_status status = TB_SUCCESS;
   for (const TuneChoice& c : candidates) {
     EngineScope scope(c.engine);
+    SplitKScope sk(c.splitk);
     status = trial(c);  // warm-up: plans, scratch growth, tile uploads
     if (status != TB_SUCCESS) break;
     double ms = 1e30;
@@ -139,7 +148,10 @@ tb_status autotune(const std::string& key, const std::vector<TuneChoice>& candid
       ms = t < ms ? t : ms;
     }
     if (status != TB_SUCCESS) break;
-    if (best.ms < 0 || ms < best.ms) best = TuneChoice{c.nb, c.engine, ms};
+    if (best.ms < 0 || ms < best.ms) {
+      best = c;
+      best.ms = ms;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -182,6 +194,30 @@ extern "C" tb_status tb_autotune_put(const char* routine, const char* flags, lon
   init_file_locked();
   g_cache[key] = TuneChoice{nb, engine, ms};
   return save_locked();
+}
+
+extern "C" tb_status tb_autotune_put_ex(const char* routine, const char* flags, long a, long b, int precision, long nb,
+                                        int engine, int splitk, double ms) {
+  if (!routine || !flags || nb <= 0 || (engine != 0 && engine != 1) || splitk < 1 || splitk > 64)
+    return TB_ERROR_INVALID_VALUE;
+  const std::string key = tune_key(routine, flags, a, b, precision);
+  std::lock_guard<std::mutex> lk(g_mu);
+  init_file_locked();
+  TuneChoice c{nb, engine, ms};
+  c.splitk = splitk;
+  g_cache[key] = c;
+  return save_locked();
+}
+
+extern "C" tb_status tb_autotune_get_ex(const char* routine, const char* flags, long a, long b, int precision,
+                                        long* nb, int* engine, int* splitk) {
+  if (!splitk) return TB_ERROR_INVALID_VALUE;
+  const tb_status s = tb_autotune_get(routine, flags, a, b, precision, nb, engine);
+  if (s != TB_SUCCESS) return s;
+  const std::string key = tune_key(routine, flags, a, b, precision);
+  std::lock_guard<std::mutex> lk(g_mu);
+  *splitk = g_cache[key].splitk;
+  return TB_SUCCESS;
 }
 
 extern "C" tb_status tb_autotune_get(const char* routine, const char* flags, long a, long b, int precision, long* nb,
@@ -235,8 +271,22 @@ tb_status auto_ssyrk(char uplo, char trans, long n, long k, float alpha, const f
   const cudaStream_t st = current_stream();
   TuneScratch s((size_t)ldc * n * sizeof(float));
   const char flags[3] = {uplo, trans, 0};
+  std::vector<TuneChoice> cands = kEngines;
+  const bool tr = trans == 'T' || trans == 't' || trans == 'C' || trans == 'c';
+  const long kb = (k + kGemmBK - 1) / kGemmBK;
+  if (precision == TB_PREC_PLAIN && !tr && n <= kSplitKMaxN && kb > kGemmPfMaxKb) {
+    // split-K candidates while the one-pass triangle leaves SMs idle
+    const bool up = uplo == 'U' || uplo == 'u';
+    const long tiles = (long)(up ? plan_upper((int)n, 256, 0, 1) : plan_lower((int)n, 256, 0, 1)).size();
+    for (int sk : {2, 4, 8, 16})
+      if (tiles < sm_count() && tiles * sk <= 4L * sm_count() && sk <= kb / 4) {
+        TuneChoice c{256, 0, 0};
+        c.splitk = sk;
+        cands.push_back(c);
+      }
+  }
   TuneChoice ch;
-  TB_TRY(autotune(tune_key("ssyrk", flags, n, k, precision), kEngines,
+  TB_TRY(autotune(tune_key("ssyrk", flags, n, k, precision), cands,
                   [&](const TuneChoice& c) {
                     float* Cs = nullptr;
                     TB_TRY(s.get(st, &Cs));
@@ -244,6 +294,7 @@ tb_status auto_ssyrk(char uplo, char trans, long n, long k, float alpha, const f
                   },
                   st, &ch));
   EngineScope scope(ch.engine);
+  SplitKScope sk(ch.splitk);
   return tb_ssyrk(uplo, trans, n, k, alpha, A, lda, beta, C, ldc, ch.nb, precision);
 }
 

@@ -81,6 +81,13 @@ lib.tb_autotune_put.restype = ctypes.c_int
 lib.tb_autotune_get.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _c_long, _c_long, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]
 lib.tb_autotune_get.restype = ctypes.c_int
+lib.tb_autotune_put_ex.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _c_long, _c_long, ctypes.c_int, _c_long,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_double]
+lib.tb_autotune_put_ex.restype = ctypes.c_int
+lib.tb_autotune_get_ex.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _c_long, _c_long, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_int)]
+lib.tb_autotune_get_ex.restype = ctypes.c_int
 lib.tb_strsm_host.restype = ctypes.c_int
 lib.tb_alloc_count.argtypes = []
 lib.tb_alloc_count.restype = ctypes.c_ulonglong
@@ -177,6 +184,14 @@ def autotune_get(routine, flags, a, b, precision=PLAIN):
     nb, eng = ctypes.c_long(), ctypes.c_int()
     st = lib.tb_autotune_get(routine.encode(), flags.encode(), a, b, precision, ctypes.byref(nb), ctypes.byref(eng))
     return (nb.value, eng.value) if st == 0 else None
+
+
+def autotune_get_ex(routine, flags, a, b, precision=PLAIN):
+    """The cached (nb, engine, split-K parts) of a key, or None (see tb_autotune_get_ex)."""
+    nb, eng, sk = ctypes.c_long(), ctypes.c_int(), ctypes.c_int()
+    st = lib.tb_autotune_get_ex(routine.encode(), flags.encode(), a, b, precision, ctypes.byref(nb), ctypes.byref(eng),
+                                ctypes.byref(sk))
+    return (nb.value, eng.value, sk.value) if st == 0 else None
 
 
 def _host_f32(t, name):

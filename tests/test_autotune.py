@@ -44,3 +44,20 @@ def test_put_rejects_bad_entries(cache):
     assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 0, 1, 1.0) == 1   # nb <= 0
     assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 128, 2, 1.0) == 1  # engine not 0 / 1
     assert TB.autotune_entries() == 0
+
+
+def test_splitk_entries_roundtrip_and_old_format(cache):
+    TB._check(TB.lib.tb_autotune_put_ex(b"ssyrk", b"LN", 1024, 16384, TB.PLAIN, 256, 0, 8, 0.05))
+    assert TB.autotune_get_ex("ssyrk", "LN", 1024, 16384, TB.PLAIN) == (256, 0, 8)
+    assert TB.autotune_get("ssyrk", "LN", 1024, 16384, TB.PLAIN) == (256, 0)
+    assert TB.lib.tb_autotune_put_ex(b"ssyrk", b"LN", 8, 8, 0, 256, 0, 0, 1.0) == 1  # split-K count < 1
+    doc = json.load(open(cache))
+    assert [e["splitk"] for e in doc["entries"]] == [8]
+    # a file written before the split-K field existed still loads (one pass)
+    key = doc["entries"][0]["key"].replace("|1024|", "|2048|")
+    with open(cache, "w") as f:
+        f.write('{\n "format": "tensorblas-autotune-1",\n "entries": [\n'
+                f'  {{"key": "{key}", "nb": 256, "engine": 1, "ms": 0.5}}\n ]\n}}\n')
+    TB.lib.tb_autotune_clear()
+    TB.autotune_set_file(cache)
+    assert TB.autotune_get_ex("ssyrk", "LN", 2048, 16384, TB.PLAIN) == (256, 1, 1)

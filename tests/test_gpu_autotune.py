@@ -61,3 +61,60 @@ def test_strsm_auto(fresh):
     TB.synchronize()
     assert TB.autotune_entries() == 1
     assert torch.equal(dB, dB2)
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+def test_ssyrk_splitk_wins_small_n_long_k(fresh, uplo):
+    """n = 768, k = 16384 plain: the one-pass triangle has 12 tiles of
+    128 x 256 for 148 SMs, so a split-K candidate (parts of K in one grouped
+    launch plus a reduction) must beat both one-pass engines. The chosen form
+    is checked against FP64 of the FP16-rounded operands, the other triangle
+    stays untouched, and a second auto call reuses the entry and gives the
+    same bits."""
+    g = np.random.Generator(np.random.PCG64(47))
+    n, k = 768, 16384
+    A = g.uniform(-1, 1, (n, k)).astype(np.float32)
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    C0 = g.uniform(-1, 1, (n, n)).astype(np.float32)
+    dC = torch.from_numpy(np.ascontiguousarray(C0.T)).cuda().reshape(-1)
+    TB._bind_stream(dA)
+    TB._check(TB.lib.tb_ssyrk(uplo.encode(), b"N", n, k, 0.5, dA.data_ptr(), n, 2.0, dC.data_ptr(), n, TB.NB_AUTO,
+                              TB.PLAIN))
+    TB.synchronize()
+    nb, engine, sk = TB.autotune_get_ex("ssyrk", uplo + "N", n, k, TB.PLAIN)
+    assert sk > 1, "a split-K candidate should win at n = 768, k = 16384"
+    got = dC.cpu().numpy().reshape(n, n).T.astype(np.float64)
+    Ah = A.astype(np.float16).astype(np.float64)  # plain: FP16-rounded operands
+    exact = 0.5 * (Ah @ Ah.T) + 2.0 * C0.astype(np.float64)
+    tri = np.tril(np.ones((n, n), dtype=bool)) if uplo == "L" else np.triu(np.ones((n, n), dtype=bool))
+    err = np.linalg.norm((got - exact)[tri]) / np.linalg.norm(exact[tri])
+    assert err <= 1e-6 + 1e-8 * k
+    assert np.array_equal(got[~tri], C0.astype(np.float64)[~tri])  # the other triangle is untouched
+    # a second auto call reuses the entry and gives the same bits
+    dC2 = torch.from_numpy(np.ascontiguousarray(C0.T)).cuda().reshape(-1)
+    TB._check(TB.lib.tb_ssyrk(uplo.encode(), b"N", n, k, 0.5, dA.data_ptr(), n, 2.0, dC2.data_ptr(), n, TB.NB_AUTO,
+                              TB.PLAIN))
+    TB.synchronize()
+    assert torch.equal(dC, dC2)
+
+
+@pytest.mark.parametrize("uplo,n,k,parts", [("L", 500, 3000, 5), ("U", 333, 1100, 3), ("L", 1024, 4096, 16)])
+def test_ssyrk_splitk_forced_entry(fresh, uplo, n, k, parts):
+    """A cached split-K entry (put through tb_autotune_put_ex) drives the
+    NB_AUTO call: ragged n and k, K parts of unequal length, beta = 0."""
+    g = np.random.Generator(np.random.PCG64(53 + n))
+    A = g.uniform(-1, 1, (n, k)).astype(np.float32)
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    TB._check(TB.lib.tb_autotune_put_ex(b"ssyrk", (uplo + "N").encode(), n, k, TB.PLAIN, 256, 0, parts, 0.0))
+    dC = torch.full((n * n,), 7.0, device="cuda")
+    TB._bind_stream(dA)
+    TB._check(TB.lib.tb_ssyrk(uplo.encode(), b"N", n, k, 1.0, dA.data_ptr(), n, 0.0, dC.data_ptr(), n, TB.NB_AUTO,
+                              TB.PLAIN))
+    TB.synchronize()
+    got = dC.cpu().numpy().reshape(n, n).T.astype(np.float64)
+    Ah = A.astype(np.float16).astype(np.float64)
+    exact = Ah @ Ah.T
+    tri = np.tril(np.ones((n, n), dtype=bool)) if uplo == "L" else np.triu(np.ones((n, n), dtype=bool))
+    err = np.linalg.norm((got - exact)[tri]) / np.linalg.norm(exact[tri])
+    assert err <= 1e-6 + 1e-8 * k
+    assert np.all(got[~tri] == 7.0)
