@@ -58,7 +58,8 @@ def parse():
     p.add_argument("--profile-gemm", type=int, default=0, metavar="N",
                    help="run three plain N x N x N SGEMMs and exit (the GEMM-engine ncu captures)")
     p.add_argument("--profile-syrk", type=int, default=0, metavar="N",
-                   help="run two plain SYRKs n = k = N and exit (the SYRK DRAM captures)")
+                   help="run two plain SYRKs n = k = N and exit (the SYRK captures)")
+    p.add_argument("--split", action="store_true", help="--profile-syrk: split precision")
     p.add_argument("--profile-ozaki", type=int, default=0, metavar="N",
                    help="run two FP64 Ozaki DSYRKs n = k = N with 8 slices and exit (the Ozaki-engine ncu captures)")
     return p.parse_args()
@@ -853,15 +854,16 @@ def profile_step(args):
 
 
 def profile_syrk(args):
-    """Two untimed plain SYRKs n = k = args.profile_syrk (lower, 'N', nb 256),
-    nothing timed: the command the SYRK DRAM captures come from."""
+    """Two untimed SYRKs n = k = args.profile_syrk (lower, 'N', nb 256; plain,
+    or split with --split), nothing timed: the command the SYRK captures come
+    from."""
     import TensorBLAS as TB
 
     n = args.profile_syrk
     A, _, _ = make_inputs(n)
     C = torch.zeros(n, n, device="cuda")
     for _ in range(2):
-        TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN)
+        TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.SPLIT if args.split else TB.PLAIN)
     TB.synchronize()
     print("profile syrk done", flush=True)
 

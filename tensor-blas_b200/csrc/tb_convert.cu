@@ -84,13 +84,8 @@ tb_status convert_f32_f16(long long rows, long long cols, const float* src, long
                    (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(hi) % 16 == 0) &&
                    (lo == nullptr || reinterpret_cast<uintptr_t>(lo) % 16 == 0);
   const int threads = 256;
-  const long long units = vec ? rows / 8 : rows;
-  long long gx = (units + threads - 1) / threads;
-  if (gx > 1024) gx = 1024;
-  long long gy = cols < 65535 ? cols : 65535;
-  // whole matrices on the vector path: about 16 blocks per SM, each thread
-  // walking many columns (convert8_body keeps four columns' loads in flight)
-  if (vec && tri == 0) gy = std::max<long long>(1, std::min<long long>(gy, (16LL * sm_count() + gx - 1) / gx));
+  long long gx = 0, gy = 0;
+  conv::convert_grid(rows, cols, tri, vec, sm_count(), threads, &gx, &gy);
   dim3 grid((unsigned)gx, (unsigned)gy);
   if (vec)
     convert8_kernel<<<grid, threads, 0, stream>>>(rows, cols, src, lds, hi, lo, ldd, lo_scale, tri, dup);

@@ -65,6 +65,41 @@ __device__ __forceinline__ void convert8_body(long long bx, long long gx, long l
                                               __half* __restrict__ hi, __half* __restrict__ lo, long long ldd,
                                               float lo_scale, int tri, long long dup) {
   const long long rows8 = rows >> 3;
+  if (tri == 2) {
+    // lower part: row group v (rows 8v .. 8v + 7) has the columns j < 8v + 8.
+    // A thread takes row groups t and rows8 - 1 - t, so every thread has
+    // about the same number of columns, and walks them four at a time.
+    const long long half = (rows8 + 1) >> 1;
+    for (long long t = bx * blockDim.x + threadIdx.x; t < half; t += gx * blockDim.x) {
+      for (int w = 0; w < 2; ++w) {
+        const long long v = w ? rows8 - 1 - t : t;
+        if (w && v == t) break;
+        const long long i = v << 3, jend = min(cols, i + 8);
+        long long j = by;
+        for (; j + 3 * gy < jend; j += 4 * gy) {
+          float4 a[4], b[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float* s = src + i + (j + u * gy) * lds;
+            a[u] = ld_stream(s);
+            b[u] = ld_stream(s + 4);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float f[8] = {a[u].x, a[u].y, a[u].z, a[u].w, b[u].x, b[u].y, b[u].z, b[u].w};
+            store8(f, hi, lo, i + (j + u * gy) * ldd, dup, lo_scale);
+          }
+        }
+        for (; j < jend; j += gy) {
+          const float* s = src + i + j * lds;
+          const float4 a = ld_stream(s), b = ld_stream(s + 4);
+          const float f[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+          store8(f, hi, lo, i + j * ldd, dup, lo_scale);
+        }
+      }
+    }
+    return;
+  }
   if (tri == 0) {
     for (long long v = bx * blockDim.x + threadIdx.x; v < rows8; v += gx * blockDim.x) {
       const long long i = v << 3;
@@ -114,6 +149,26 @@ __device__ __forceinline__ void convert8_body(long long bx, long long gx, long l
       store8(f, hi, lo, i + j * ldd, dup, lo_scale);
     }
   }
+}
+
+// Grid (gx, gy) of convert8_body / convert1_body for a rows x cols operand:
+// whole matrices and lower parts on the vector path take about 16 blocks of
+// 256 threads per SM, each thread walking many columns; the other forms one
+// column per block row.
+inline void convert_grid(long long rows, long long cols, int tri, bool vec, int sms, int threads, long long* gx,
+                         long long* gy) {
+  long long units = vec ? rows / 8 : rows;
+  if (vec && tri == 2) units = (units + 1) / 2;  // two row groups per thread
+  long long x = (units + threads - 1) / threads;
+  if (x > 1024) x = 1024;
+  long long y = cols < 65535 ? cols : 65535;
+  if (vec && (tri == 0 || tri == 2)) {
+    const long long want = (16LL * sms + x - 1) / x;
+    y = want < y ? want : y;
+    if (y < 1) y = 1;
+  }
+  *gx = x;
+  *gy = y;
 }
 
 // Scalar fallback for ragged or unaligned shapes.

@@ -30,8 +30,10 @@ void set_last_error(const char* fmt, ...);
 
 // ------------------------------------------------------------------ streams / pool
 cudaStream_t current_stream();
-// Two more (non-blocking) streams per device (i = 0, 1) for work the library
-// splits; joined back into the caller's stream before a routine returns.
+// More (non-blocking) streams per device (i = 0 .. kAuxStreams - 1) for work
+// the library splits; joined back into the caller's stream before a routine
+// returns.
+constexpr int kAuxStreams = 4;
 cudaStream_t aux_stream(int i = 0);
 // Device scratch owned by the library (grow-only, per device and slot).
 // Slot 0 serves the routines' own scratch; slot 1 the host-memory entry

@@ -862,65 +862,96 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1) oz_pair_kern
 //   L = 2 .. S + 1.
 // One block per 32-column slab of a tile of the GEMM's tile list (tile_rows
 // rows; eight slabs per tile, so even a one-wave GEMM gives every SM several
-// blocks); a thread takes one row and every (256 / tile_rows)-th column of
-// the slab, so a warp's loads and stores cover 32 consecutive rows of a
-// column.
+// blocks); a thread takes one row. The slab's level sums stream through
+// shared memory: per column, S contiguous runs of the tile's rows (one per
+// level) are fetched by bulk copies into a ring of kOzFoldStages stages, so
+// up to kOzFoldStages * S * tile_rows * 4 bytes per block are in flight
+// without holding them in registers, and the threads fold column q while the
+// copies of the next columns land. The workspace's leading dimension is a
+// multiple of 32 rows, so the runs never leave it (rows at or past M are
+// fetched and not used). Every wait is bounded.
 constexpr int kOzFoldSlab = 32;
+constexpr int kOzFoldStages = 4;
+__host__ __device__ constexpr int oz_fold_smem(int S, int tile_rows) { return kOzFoldStages * S * tile_rows * 4; }
+
 __global__ void __launch_bounds__(256) oz_fold_kernel(const int4* __restrict__ tiles, int tile_rows, int M, int N,
                                                       int tri, int S, double alpha, double beta, double* C,
                                                       long long ldc, const int* __restrict__ eA,
                                                       const int* __restrict__ eB, const int* __restrict__ raw,
-                                                      long long ld_raw, long long plane) {
+                                                      long long ld_raw, long long plane, int* err) {
+  extern __shared__ __align__(128) int fold_buf[];
+  __shared__ uint64_t bars[kOzFoldStages];
+  __shared__ int abort_flag;
   const int4 tile = tiles[blockIdx.x / (kOzBN / kOzFoldSlab)];
   const int c0 = (int)(blockIdx.x % (kOzBN / kOzFoldSlab)) * kOzFoldSlab;
   const double b = (tile.z & kOzAccumulate) ? 1.0 : beta;
   const bool empty = tile.w <= (tile.z & (kOzAccumulate - 1));
-  const long long i = (long long)tile.x + (int)(threadIdx.x % tile_rows);
-  if (i >= M) return;
-  const int ei = oz_row_exp(eA, i);
-  const int step = 256 / tile_rows;
+  const int tid = threadIdx.x;
   if (empty) {
-    for (int c = c0 + (int)(threadIdx.x / tile_rows); c < c0 + kOzFoldSlab; c += step) {
-      const long long j = (long long)tile.y + c;
-      if (j >= N || (tri == 1 && j > i)) break;  // columns only grow
-      if (tri == 2 && j < i) continue;
-      double* const cp = C + i + j * ldc;
-      if (b != 1.0) *cp = b == 0.0 ? 0.0 : b * *cp;
+    for (int r = tid; r < tile_rows; r += blockDim.x) {
+      const long long i = (long long)tile.x + r;
+      if (i >= M) break;
+      for (int c = c0; c < c0 + kOzFoldSlab; ++c) {
+        const long long j = (long long)tile.y + c;
+        if (j >= N || (tri == 1 && j > i)) break;  // columns only grow
+        if (tri == 2 && j < i) continue;
+        double* const cp = C + i + j * ldc;
+        if (b != 1.0) *cp = b == 0.0 ? 0.0 : b * *cp;
+      }
     }
     return;
   }
-  // four columns per pass: every level sum and C value of the four is
-  // requested before the first fold, so S + 1 loads per column are in flight
-  // together (the per-element arithmetic and its order are unchanged)
-  constexpr int U = 4;
-  for (int cb = c0 + (int)(threadIdx.x / tile_rows); cb < c0 + kOzFoldSlab; cb += U * step) {
-    bool act[U];
-    long long jj[U];
-    int v[U][kOzMaxSlices];
-    double old[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int c = cb + u * step;
-      jj[u] = (long long)tile.y + c;
-      act[u] = c < c0 + kOzFoldSlab && jj[u] < N && !(tri == 1 && jj[u] > i) && !(tri == 2 && jj[u] < i);
-      old[u] = 0.0;
-      if (act[u]) {
-        const int* const p = raw + i + jj[u] * ld_raw;
-#pragma unroll
-        for (int l = 0; l < kOzMaxSlices; ++l) v[u][l] = l < S ? __ldcs(p + l * plane) : 0;
-        if (b != 0.0) old[u] = C[i + jj[u] * ldc];
-      }
+  // the slab's columns with work: [cb, ce)
+  long long ce = std::min<long long>(c0 + kOzFoldSlab, (long long)N - tile.y);
+  if (tri == 1) ce = std::min<long long>(ce, (long long)tile.x + tile_rows - tile.y);  // some row i >= j
+  long long cb = c0;
+  if (tri == 2) cb = std::max<long long>(cb, (long long)tile.x - tile.y);  // some row i <= j
+  const int ncols = (int)(ce - cb);
+  if (ncols <= 0) return;
+  const int run = (int)std::min<long long>(tile_rows, ld_raw - tile.x);  // rows fetched per level (multiple of 32)
+  const uint32_t run_bytes = (uint32_t)run * 4u;
+  if (tid == 0) {
+    for (int s = 0; s < kOzFoldStages; ++s) mbar_init(&bars[s], 1);
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int q) {  // column cb + q into stage q % kOzFoldStages (thread 0)
+    const int s = q % kOzFoldStages;
+    const long long j = (long long)tile.y + cb + q;
+    mbar_arrive_expect_tx(&bars[s], run_bytes * (uint32_t)S);
+    for (int l = 0; l < S; ++l)
+      bulk_load(fold_buf + (s * S + l) * tile_rows, raw + tile.x + j * ld_raw + l * plane, run_bytes, &bars[s]);
+  };
+  if (tid == 0)
+    for (int q = 0; q < kOzFoldStages && q < ncols; ++q) issue(q);
+  const long long i = (long long)tile.x + tid;
+  const bool row_ok = tid < tile_rows && i < M;
+  const int ei = row_ok ? oz_row_exp(eA, i) : 0;
+  int q = 0;
+  for (; q < ncols; ++q) {
+    const int s = q % kOzFoldStages;
+    const bool ok = mbar_wait(&bars[s], (uint32_t)(q / kOzFoldStages) & 1u, &abort_flag, err, kDevErrTimeoutEpilogue);
+    if (__syncthreads_or(!ok)) break;
+    const long long j = (long long)tile.y + cb + q;
+    if (row_ok && !(tri == 1 && j > i) && !(tri == 2 && j < i)) {
+      const int ej = oz_row_exp(eB, j);
+      double* const cp = C + i + j * ldc;
+      const int* const v = fold_buf + s * S * tile_rows + tid;
+      double acc = b * (b != 0.0 ? *cp : 0.0);
+      for (int l = 0; l < S; ++l) acc = fma(alpha * pow2i(ei + ej - 7 * (l + 2)), (double)v[l * tile_rows], acc);
+      *cp = acc;
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (!act[u]) continue;
-      const int ej = oz_row_exp(eB, jj[u]);
-      double acc = b * old[u];
-#pragma unroll
-      for (int l = 0; l < kOzMaxSlices; ++l)
-        if (l < S) acc = fma(alpha * pow2i(ei + ej - 7 * (l + 2)), (double)v[u][l], acc);
-      C[i + jj[u] * ldc] = acc;
-    }
+    __syncthreads();  // stage s is read
+    if (tid == 0 && q + kOzFoldStages < ncols) issue(q + kOzFoldStages);
+  }
+  if (q < ncols && tid == 0) {
+    // a wait gave up: let the copies already issued land before the block
+    // leaves (bounded)
+    const uint64_t t0 = globaltimer_ns();
+    for (int r = q; r < ncols && r < q + kOzFoldStages; ++r)
+      while (!mbar_try_wait(&bars[r % kOzFoldStages], (uint32_t)(r / kOzFoldStages) & 1u))
+        if (globaltimer_ns() - t0 > 1000000000ull) break;
   }
 }
 
@@ -1180,6 +1211,8 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
   if (dev < 64 && !attr[dev]) {
     TB_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzSmem));
     TB_CUDA_TRY(cudaFuncSetAttribute(oz_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzPairSmem));
+    TB_CUDA_TRY(cudaFuncSetAttribute(oz_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     oz_fold_smem(kOzMaxSlices, 256)));
     attr[dev] = true;
   }
   void* tok = prof_begin(st, kProfOzaki);
@@ -1194,9 +1227,9 @@ tb_status oz_launch(const OzPlanes& a, const OzPlanes& b, int kb_shift, int kb_m
   TB_CUDA_TRY(cudaGetLastError());
   if (levels) {
     note_launch();
-    oz_fold_kernel<<<g.num_tiles * (kOzBN / kOzFoldSlab), 256, 0, st>>>(g.tiles, pair ? 256 : kOzBM, M, N, tri, S,
-                                                                       alpha, beta, C, ldc, g.eA, g.eB, levels, ld_r,
-                                                                       plane);
+    const int tile_rows = pair ? 256 : kOzBM;
+    oz_fold_kernel<<<g.num_tiles * (kOzBN / kOzFoldSlab), 256, oz_fold_smem(S, tile_rows), st>>>(
+        g.tiles, tile_rows, M, N, tri, S, alpha, beta, C, ldc, g.eA, g.eB, levels, ld_r, plane, g.err);
     TB_CUDA_TRY(cudaGetLastError());
   }
   prof_end(tok, st, flops);

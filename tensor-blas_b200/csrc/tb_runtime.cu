@@ -24,7 +24,7 @@ struct DeviceState {
   int* err = nullptr;        // the library's device error block (kErrBlockInts ints)
   int* extra_err = nullptr;  // a second block of this device (the allocation-free entry point's)
   int sms = 0;
-  cudaStream_t aux[2] = {nullptr, nullptr};
+  cudaStream_t aux[kAuxStreams] = {};
 };
 DeviceState g_dev[kMaxDevices];
 std::mutex g_mu;
@@ -112,7 +112,7 @@ cudaStream_t current_stream() { return g_stream; }
 
 cudaStream_t aux_stream(int i) {
   DeviceState* s = state();
-  if (!s || i < 0 || i > 1) return nullptr;
+  if (!s || i < 0 || i >= kAuxStreams) return nullptr;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!s->aux[i] && cudaStreamCreateWithFlags(&s->aux[i], cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();

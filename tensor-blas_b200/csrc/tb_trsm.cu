@@ -438,11 +438,8 @@ tb_status trsm_prep_launch(const PrepJobs& j, cudaStream_t st) {
     const bool vec = (c.rows % 8 == 0) && (c.lds % 4 == 0) && (c.ldd % 8 == 0) &&
                      (reinterpret_cast<uintptr_t>(c.src) % 16 == 0) && (reinterpret_cast<uintptr_t>(c.hi) % 16 == 0) &&
                      (c.lo == nullptr || reinterpret_cast<uintptr_t>(c.lo) % 16 == 0);
-    const long long units = vec ? c.rows / 8 : c.rows;
-    long long gx = (units + kPrepThreads - 1) / kPrepThreads;
-    if (gx > 1024) gx = 1024;
-    long long gy = c.cols < 65535 ? c.cols : 65535;
-    if (vec && c.tri == 0) gy = std::max<long long>(1, std::min<long long>(gy, (16LL * sm_count() + gx - 1) / gx));
+    long long gx = 0, gy = 0;
+    conv::convert_grid(c.rows, c.cols, c.tri, vec, sm_count(), kPrepThreads, &gx, &gy);
     p.conv_vec[k] = vec ? 1 : 0;
     p.conv_gx[k] = gx;
     p.conv_base[k] = next;
@@ -711,45 +708,54 @@ tb_status trsm_solve_launches(TrsmCtx& c, const std::vector<long>& leaf_start, f
 
 tb_status trsm_solve_2s(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols) {
   const long span = c.right ? rows : cols;  // independent systems
+  // TB_TRSM_STREAMS in the environment: how many parts of B's independent
+  // dimension are solved side by side (1 to 4, default 2; read once)
   static const int streams = [] {
     const char* e = getenv("TB_TRSM_STREAMS");
-    return (e && e[0] == '1') ? 1 : 2;
+    const int v = e ? atoi(e) : 0;
+    return (v >= 1 && v <= 4) ? v : 2;
   }();
   // plain products only: the split form's launches carry three products per
   // tile, their tails are short, and halving their tile counts cost more
   // than the overlap gained (measured at 16384: plain 6.36 -> 6.11 ms,
   // split 15.45 -> 15.65 ms)
   if (trsm_dag_eligible(c, B, ldb)) return trsm_solve_dag(c, leaf_start, B, ldb, rows, cols);
-  const cudaStream_t st2 = streams > 1 && span >= 4096 && c.split == Split::kPlain ? aux_stream() : nullptr;
-  if (!st2 || ldb < (rows > 1 ? rows : 1)) return trsm_solve_launches(c, leaf_start, B, ldb, rows, cols);
-  const long half = round_up((span + 1) / 2, 128);
-  // the second half's scratch: X and R are laid out along the split dimension
-  TrsmCtx c2 = c;
-  c2.st = st2;
-  const long long xo = c.right ? half : (long long)half * c.ldx;
-  const long long ro = c.right ? half : (long long)half * c.ldr;
-  c2.xh = c.xh + xo;
-  c2.xl = c.xl ? c.xl + xo : nullptr;
-  c2.rh = c.rh + ro;
-  c2.rl = c.rl + ro;
-  cudaEvent_t fork, join;
+  int parts = (c.split == Split::kPlain && span >= 4096) ? streams : 1;
+  cudaStream_t sq[4] = {c.st, nullptr, nullptr, nullptr};
+  for (int p = 1; p < parts; ++p)
+    if (!(sq[p] = aux_stream(p - 1))) parts = 1;
+  if (parts == 1 || ldb < (rows > 1 ? rows : 1)) return trsm_solve_launches(c, leaf_start, B, ldb, rows, cols);
+  const long w = round_up((span + parts - 1) / parts, 128);
+  cudaEvent_t fork, join[4];
   TB_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-  TB_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
-  tb_status s1 = TB_SUCCESS, s2 = TB_SUCCESS;
-  if (cudaEventRecord(fork, c.st) != cudaSuccess || cudaStreamWaitEvent(st2, fork, 0) != cudaSuccess) {
-    s1 = TB_ERROR_CUDA;
-  } else {
-    s2 = c.right ? trsm_solve_launches(c2, leaf_start, B + half, ldb, rows - half, cols)
-                 : trsm_solve_launches(c2, leaf_start, B + half * ldb, ldb, rows, cols - half);
-    s1 = c.right ? trsm_solve_launches(c, leaf_start, B, ldb, half, cols)
-                 : trsm_solve_launches(c, leaf_start, B, ldb, rows, half);
-    // the caller's stream continues only after both halves
-    if (cudaEventRecord(join, st2) != cudaSuccess || cudaStreamWaitEvent(c.st, join, 0) != cudaSuccess)
-      s1 = TB_ERROR_CUDA;
+  for (auto& e : join) TB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  tb_status rs = TB_SUCCESS;
+  if (cudaEventRecord(fork, c.st) != cudaSuccess) rs = TB_ERROR_CUDA;
+  // the parts after the first on the auxiliary streams, the first on the
+  // caller's stream; X and R scratch are laid out along the split dimension
+  for (int p = parts - 1; p >= 0 && rs == TB_SUCCESS; --p) {
+    const long lo = std::min(span, p * w), hi = std::min(span, (p + 1) * w);
+    if (hi <= lo) continue;
+    TrsmCtx cp = c;
+    cp.st = sq[p];
+    const long long xo = c.right ? lo : (long long)lo * c.ldx;
+    const long long ro = c.right ? lo : (long long)lo * c.ldr;
+    cp.xh = c.xh + xo;
+    cp.xl = c.xl ? c.xl + xo : nullptr;
+    cp.rh = c.rh + ro;
+    cp.rl = c.rl + ro;
+    if (p > 0 && cudaStreamWaitEvent(sq[p], fork, 0) != cudaSuccess) {
+      rs = TB_ERROR_CUDA;
+      break;
+    }
+    rs = c.right ? trsm_solve_launches(cp, leaf_start, B + lo, ldb, hi - lo, cols)
+                 : trsm_solve_launches(cp, leaf_start, B + lo * ldb, ldb, rows, hi - lo);
+    if (p > 0 && (cudaEventRecord(join[p], sq[p]) != cudaSuccess || cudaStreamWaitEvent(c.st, join[p], 0) != cudaSuccess))
+      rs = TB_ERROR_CUDA;
   }
   cudaEventDestroy(fork);
-  cudaEventDestroy(join);
-  return s1 != TB_SUCCESS ? s1 : s2;
+  for (auto& e : join) cudaEventDestroy(e);
+  return rs;
 }
 
 tb_status trsm_impl(bool right, long m, long n, const float* A, long lda, float* B, long ldb, long nb, Split split,

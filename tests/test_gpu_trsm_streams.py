@@ -1,9 +1,9 @@
 """On the launch-per-product path (TB_TRSM_DAG=0), plain TRSMs with at least
-4096 independent columns (left) or rows (right) are solved in two halves on
-two streams; each column's (row's) arithmetic is the same either way, so the
-result must be bit-identical to the one-stream solve. The stream count is
-read once per process (TB_TRSM_STREAMS), so each setting runs in its own
-subprocess."""
+4096 independent columns (left) or rows (right) are solved in parts (two by
+default, up to four) on as many streams; each column's (row's) arithmetic is
+the same either way, so the result must be bit-identical to the one-stream
+solve. The part count is read once per process (TB_TRSM_STREAMS), so each
+setting runs in its own subprocess."""
 import os
 import subprocess
 import sys
@@ -44,3 +44,10 @@ def _digest(streams, side, m, n):
 @pytest.mark.parametrize("side,m,n", [("L", 2048, 4608), ("R", 4608, 2048)])
 def test_two_stream_solve_is_bit_identical(side, m, n):
     assert _digest(1, side, m, n) == _digest(2, side, m, n)
+
+
+@pytest.mark.parametrize("side,m,n", [("L", 1536, 5000), ("R", 5000, 1536)])
+def test_three_and_four_part_solves_are_bit_identical(side, m, n):
+    ref = _digest(1, side, m, n)
+    assert _digest(3, side, m, n) == ref
+    assert _digest(4, side, m, n) == ref
