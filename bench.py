@@ -178,7 +178,8 @@ def measured_peaks():
 
 
 def traffic_summary():
-    """Per-launch DRAM bytes of the GEMM engine from a committed ncu summary."""
+    """DRAM bytes per algorithmic flop of the GEMM kernels, from a committed
+    small-case ncu summary (scaled here to a launch by its flops)."""
     try:
         with open(os.path.join(ROOT, "profiles", "gemm_engine_traffic.json")) as f:
             return json.load(f)
@@ -379,7 +380,8 @@ def run_mine(args, world, rank, local):
             "frac": (ach / burst) if ach and burst else None, "launches_per_step": cnt,
             "ms_per_step": ms, "flops_per_launch": fl / cnt if cnt else None,
             "share_of_step_gemm_time": ms / sum(v[0] for v in kernels.values()),
-            "traffic": t.get("bytes_per_launch"), "traffic_note": t.get("note")}
+            "traffic": t["bytes_per_flop"] * fl / cnt if ("bytes_per_flop" in t and cnt) else None,
+            "traffic_note": t.get("note")}
     dominant = keys[max(kernels, key=lambda k: kernels[k][0])]
     roof = dict(per_kernel[dominant])
     roof.update({"peak_source": f"{peak_src} bf16_tflops (burst: each launch timed alone; sustained {sustained})",
@@ -908,8 +910,9 @@ def profile_ozaki(args):
 
 def profile_aux(args):
     """One plain SYRK and TRSM at n (FP32->FP16 conversions, 32x32 and leaf
-    inverses), one Ozaki DSYRK n=k=n/2 with 10 slices (exponent, slicing and
-    level-fold passes) and one FP8 SYR2K n/2 x n/4 (block quantisation);
+    inverses), one Ozaki DSYRK n=k=n/2 with the slice count chosen by the
+    library (range measurement, exponent, slicing and level-fold passes) and
+    one FP8 SYR2K n/2 x n/4 (block quantisation);
     nothing timed. At n = 8192 the whole run holds about 2 GB on the device
     (the size the ncu captures of these kernels use)."""
     import ctypes
@@ -930,7 +933,7 @@ def profile_aux(args):
     L, P = ctypes.c_long, ctypes.c_void_p
     TB.lib.tb_dsyrk_ozaki.argtypes = [ctypes.c_char, ctypes.c_char, L, L, ctypes.c_double, P, L, ctypes.c_double, P, L,
                                       ctypes.c_int]
-    TB._check(TB.lib.tb_dsyrk_ozaki(b"L", b"N", m, m, 1.0, D.data_ptr(), m, 0.0, E.data_ptr(), m, 10))
+    TB._check(TB.lib.tb_dsyrk_ozaki(b"L", b"N", m, m, 1.0, D.data_ptr(), m, 0.0, E.data_ptr(), m, 0))
     del D, E
     kk = m // 2
     X = torch.randn(kk, m, device="cuda")

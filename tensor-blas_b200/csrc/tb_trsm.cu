@@ -709,16 +709,18 @@ tb_status trsm_solve_launches(TrsmCtx& c, const std::vector<long>& leaf_start, f
 tb_status trsm_solve_2s(TrsmCtx& c, const std::vector<long>& leaf_start, float* B, long ldb, long rows, long cols) {
   const long span = c.right ? rows : cols;  // independent systems
   // TB_TRSM_STREAMS in the environment: how many parts of B's independent
-  // dimension are solved side by side (1 to 4, default 2; read once)
+  // dimension are solved side by side on as many streams (1 to 4; read
+  // once). Default 1: with the setup's preparation launches overlapped
+  // (trsm_setup), plain m = n = 16384 nb 512 took 6.13 / 6.69 / 6.87 / 6.89 ms
+  // with 1 / 2 / 3 / 4 parts on a B200 (6.47 / 7.03 / 7.20 / 7.22 on another):
+  // a part's short launches cost as long as the whole solve's, so splitting
+  // them adds latency. Plain products only: the split form's launches carry
+  // three products per tile and never gained from parts.
   static const int streams = [] {
     const char* e = getenv("TB_TRSM_STREAMS");
     const int v = e ? atoi(e) : 0;
-    return (v >= 1 && v <= 4) ? v : 2;
+    return (v >= 1 && v <= 4) ? v : 1;
   }();
-  // plain products only: the split form's launches carry three products per
-  // tile, their tails are short, and halving their tile counts cost more
-  // than the overlap gained (measured at 16384: plain 6.36 -> 6.11 ms,
-  // split 15.45 -> 15.65 ms)
   if (trsm_dag_eligible(c, B, ldb)) return trsm_solve_dag(c, leaf_start, B, ldb, rows, cols);
   int parts = (c.split == Split::kPlain && span >= 4096) ? streams : 1;
   cudaStream_t sq[4] = {c.st, nullptr, nullptr, nullptr};

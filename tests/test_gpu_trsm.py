@@ -38,8 +38,8 @@ def _run(tblas, side, A, B, nb, precision):
 
 
 # (1024, 4608) / (4608, 1024): the independent dimension (columns for the
-# left side, rows for the right side) reaches 4096, so the solve runs as two
-# halves on two streams
+# left side, rows for the right side) reaches 4096, where TB_TRSM_STREAMS > 1
+# would split the solve into parts
 CASES = [(512, 1024, 256), (300, 700, 128), (1024, 2048, 512), (64, 64, 512), (130, 1, 64), (2048, 1536, 512),
          (4096, 512, 512), (512, 4096, 512), (1024, 4608, 256), (4608, 1024, 256)]
 

@@ -1,8 +1,8 @@
 """On the launch-per-product path (TB_TRSM_DAG=0), plain TRSMs with at least
-4096 independent columns (left) or rows (right) are solved in parts (two by
-default, up to four) on as many streams; each column's (row's) arithmetic is
-the same either way, so the result must be bit-identical to the one-stream
-solve. The part count is read once per process (TB_TRSM_STREAMS), so each
+4096 independent columns (left) or rows (right) can be solved in parts (up
+to four, TB_TRSM_STREAMS; one by default) on as many streams; each column's
+(row's) arithmetic is the same either way, so the result must be
+bit-identical to the one-stream solve. The part count is read once per process (TB_TRSM_STREAMS), so each
 setting runs in its own subprocess."""
 import os
 import subprocess
