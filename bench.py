@@ -67,15 +67,22 @@ def parse():
 
 # ------------------------------------------------------------------ process / ranks
 def dist_setup(args):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): NCCL
+    on GPUs, gloo where no GPU is visible (the CPU tests of this plumbing)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    gpu = torch.cuda.is_available()
+    if gpu:
+        torch.cuda.set_device(local)
     if world > 1:
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if gpu:
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -87,13 +94,22 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest of the ranks' values (device times: the job's time is the
+    slowest rank's)."""
     if world == 1:
         return x
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_tflops(world, steps, flops_step, ms_max):
+    """Whole-job throughput of N replicas: every rank runs `steps` steps of
+    `flops_step`, the job takes the slowest rank's `ms_max`."""
+    return world * steps * flops_step / (ms_max * 1e-3) / 1e12
 
 
 def physical_gpu(local):
@@ -315,8 +331,8 @@ def run_mine(args, world, rank, local):
         if cnt.value:
             kernels[kind] = (ms.value / 5, fl.value / 5, cnt.value / 5)
 
-    value = world * args.steps * flops_step / (ms_plain * 1e-3) / 1e12
-    value_split = world * args.steps * flops_step / (ms_split * 1e-3) / 1e12
+    value = job_tflops(world, args.steps, flops_step, ms_plain)
+    value_split = job_tflops(world, args.steps, flops_step, ms_split)
     agreement = agreement_vs_reference(TB, args, A, C, T, B0, Bw) if rank == 0 else None
 
     # ---- end to end through the public host-memory API (page-locked buffers):
@@ -348,7 +364,7 @@ def run_mine(args, world, rank, local):
             ms_e2e_syrk += e0.elapsed_time(em)
     ms_e2e = max_over_ranks(ms_e2e, world)
     barrier(world)
-    e2e_value = world * args.e2e_steps * flops_step / (ms_e2e * 1e-3) / 1e12
+    e2e_value = job_tflops(world, args.e2e_steps, flops_step, ms_e2e)
     if rank == 0:
         # the host copies must reproduce the device results
         Bw.copy_(B0)
