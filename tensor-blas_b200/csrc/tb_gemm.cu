@@ -181,6 +181,17 @@ int split_kchunk() {
   return k;
 }
 
+// CTA-pair launches that store from registers get a seventh operand stage
+// (TB_GEMM_PAIR_DIRECT in the environment, read once: 0 none, 1 the beta = 0
+// launches without side copies, 2 all).
+static int pair_direct_mode() {
+  static const int mode = [] {
+    const char* e = getenv("TB_GEMM_PAIR_DIRECT");
+    return (e && e[0] >= '0' && e[0] <= '2') ? e[0] - '0' : 1;
+  }();
+  return mode;
+}
+
 int gemm_bn(Split s) { return s == Split::kPlain ? 256 : 128; }
 int gemm_bn(Split s, int kblocks) {
   const bool pf = kblocks > 0 && kblocks <= kGemmPfMaxKb;
@@ -255,6 +266,13 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   if (c.fp8) return launch_variant<GemmCfg<kGemmBNFp8, 1, false, false, false, true>, false>(a, c.num_tiles, stream,
                                                                                             c.flops);
   if (c.pair) {
+    const int direct = pair_direct_mode();
+    if (direct == 2 || (direct == 1 && c.beta == 0.f && !c.out_hi)) {
+      if (amn && bmn) return launch_pair<PairCfg<true, true, true>>(a, c.num_tiles, stream, c.flops);
+      if (amn && !bmn) return launch_pair<PairCfg<true, false, true>>(a, c.num_tiles, stream, c.flops);
+      if (!amn && !bmn) return launch_pair<PairCfg<false, false, true>>(a, c.num_tiles, stream, c.flops);
+      return launch_pair<PairCfg<false, true, true>>(a, c.num_tiles, stream, c.flops);
+    }
     if (amn && bmn) return launch_pair<PairCfg<true, true>>(a, c.num_tiles, stream, c.flops);
     if (amn && !bmn) return launch_pair<PairCfg<true, false>>(a, c.num_tiles, stream, c.flops);
     if (!amn && !bmn) return launch_pair<PairCfg<false, false>>(a, c.num_tiles, stream, c.flops);

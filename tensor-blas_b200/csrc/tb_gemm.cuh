@@ -936,17 +936,22 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
 // Every wait is bounded like the single-CTA kernel's; a cluster barrier
 // before TMEM is freed keeps either CTA from leaving while the pair's MMAs
 // or remote arrivals may still touch it.
-template <bool A_MN_, bool B_MN_>
+// DIRECT: launches that read no C and write no side copies (beta = 0, e.g.
+// SYRK) store each thread's row of a chunk straight from registers (a
+// warp's 32 rows of a column are one 128-byte line), which frees the
+// epilogue's staging buffers for a seventh operand stage.
+template <bool A_MN_, bool B_MN_, bool DIRECT_ = false>
 struct PairCfg {
   static constexpr int BM = 128, BN = 256, BK = 64;  // BM: rows per CTA; BN: the pair tile's columns
   static constexpr bool A_MN = A_MN_, B_MN = B_MN_;
+  static constexpr bool DIRECT = DIRECT_;
   static constexpr int A_BYTES = BM * BK * 2;
   static constexpr int B_BYTES = (BN / 2) * BK * 2;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int STAGES = 6;
+  static constexpr int STAGES = DIRECT ? 7 : 6;
   static constexpr int ACC_COLS = BN;
   static constexpr int TMEM_COLS = 2 * ACC_COLS;
-  static constexpr int EPI_BYTES = 2 * 128 * 32 * 4;
+  static constexpr int EPI_BYTES = DIRECT ? 0 : 2 * 128 * 32 * 4;
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + 256;
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
   static constexpr uint32_t IDESC = idesc_f16(2 * BM, BN, false, A_MN, B_MN);
@@ -1145,7 +1150,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
         }
-        if (args.tma_c && !direct) {
+        if (!Cfg::DIRECT && args.tma_c && !direct) {
           if (tile.y + c0 < args.N && m0 < args.M)
             epilogue_chunk_tma(args, stage_c, cload, es, v, m0, tile.y + c0, row, args.beta != 0.0f || tile_masked,
                                issuer, abort_flag);

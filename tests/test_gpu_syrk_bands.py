@@ -32,8 +32,8 @@ print(hashlib.sha1(C.cpu().numpy().tobytes()).hexdigest())
 """
 
 
-def _digest(parts, trans, n, k, prec, beta):
-    env = dict(os.environ, TB_SYRK_PARTS=parts)
+def _digest(parts, trans, n, k, prec, beta, **extra):
+    env = dict(os.environ, TB_SYRK_PARTS=parts, **extra)
     out = subprocess.run([sys.executable, "-c", SCRIPT, os.path.join(ROOT, "tensor-blas_b200", "python"), trans,
                           str(n), str(k), str(prec), str(beta)], env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
@@ -50,3 +50,10 @@ def test_band_count_does_not_change_the_bits():
     ref = _digest("1", "N", 8448, 1100, 0, 0.5)
     for parts in ("2", "7", "16"):
         assert _digest(parts, "N", 8448, 1100, 0, 0.5) == ref, parts
+
+
+@pytest.mark.parametrize("trans,n,k", [("N", 8448, 1100), ("T", 4096, 3000)])
+def test_direct_store_epilogue_is_bit_identical(trans, n, k):
+    """beta = 0 CTA-pair launches store from registers with a seventh operand
+    stage (TB_GEMM_PAIR_DIRECT=0 keeps the staged TMA epilogue): same bits."""
+    assert _digest("1", trans, n, k, 0, 0.0, TB_GEMM_PAIR_DIRECT="0") == _digest("1", trans, n, k, 0, 0.0)
