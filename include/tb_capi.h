@@ -322,6 +322,10 @@ TB_API tb_status tb_batch_destroy(tb_batch_t batch);
  * Replaces the reference's s2h / s2h_swpipe kernels (util/util.cu:127-136,
  * include/TensorBLAS.h:185-283); ah and al are __half arrays. */
 TB_API tb_status tb_s2h(long m, long n, const float* as, long ldas, void* ah, long ldah, void* al, float lo_scale);
+/* The same plain conversion (no low half) on the host's cores, host buffers
+ * in and out: what tb_ssyrk_host does to A's row panels before they cross
+ * PCIe. Round to nearest, ties to even, as the device conversion. */
+TB_API tb_status tb_host_s2h(long m, long n, const float* as, long ldas, void* ah, long ldah);
 
 /* Mirror lower -> upper of an n x n matrix (util/util.cu:148-157). */
 TB_API tb_status tb_ssymmetrize(long n, float* A, long lda);

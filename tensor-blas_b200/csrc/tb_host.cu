@@ -11,9 +11,12 @@
 // returns only the lower triangle it computes.
 //
 //  SYRK, C = alpha A A^T + beta C (lower): row panel i of A (rows [r0, r1),
-//   all k columns) is copied, converted into the device FP16 copy of A, and
-//   row panel i of C (rows [r0, r1), columns [0, r1)) is computed from it
-//   and the panels before it and copied back while panel i+1 is on its way.
+//   all k columns) reaches the device FP16 copy of A — in plain precision
+//   converted to FP16 on the host's cores first (tb_host_convert.cpp), so
+//   half the bytes cross PCIe; in split precision copied as FP32 and
+//   converted to hi/lo on the device — and row panel i of C (rows [r0, r1),
+//   columns [0, r1)) is computed from it and the panels before it and
+//   copied back while panel i+1 is on its way.
 //  TRSM: A's lower triangle is copied once and prepared (FP16 copy, leaf
 //   inverses); B then flows through a ring of device panels (columns for the
 //   left side, rows for the right side: those are independent systems).
@@ -76,6 +79,35 @@ enum : int {
   kEvTri = 24,  // A triangle staged
 };
 
+// Page-locked host staging for the FP16 row panels of A (plain SYRK), per
+// device, grown on demand and kept until tb_release_scratch.
+struct HostStage {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+HostStage g_stage[kMaxDev];
+
+void* host_stage(size_t bytes) {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDev) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pipe_mu);
+  HostStage& h = g_stage[d];
+  if (h.bytes >= bytes) return h.p;
+  if (h.p) {
+    cudaDeviceSynchronize();  // copies still reading the old buffer must finish
+    cudaFreeHost(h.p);
+    h.p = nullptr;
+    h.bytes = 0;
+  }
+  if (cudaHostAlloc(&h.p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    h.p = nullptr;
+    return nullptr;
+  }
+  h.bytes = bytes;
+  return h.p;
+}
+
 tb_status finish(cudaStream_t cs, HostPipes& p) {
   TB_TRY(join(cs, p.h2d, p.ev[kEvEndH2d]));
   TB_TRY(join(cs, p.d2h, p.ev[kEvEndD2h]));
@@ -105,7 +137,15 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   const size_t half_bytes = (size_t)round_up(ldh * k * 2, 256);
   const size_t stA_bytes = (size_t)round_up((long long)P * k * 4, 256);
   const size_t cb_bytes = (size_t)round_up((long long)P * n * 4, 256);
-  const size_t total = half_bytes * (hilo ? 2 : 1) + kSyrkSlots * (stA_bytes + cb_bytes);
+  // plain: A's row panels are converted to FP16 on the host's cores into
+  // page-locked slots and copied straight into the device FP16 copy (half
+  // the bytes of FP32 across PCIe, no device conversion); split keeps the
+  // FP32 upload and the device conversion (hi and lo are as many bytes as
+  // FP32). Without the page-locked slots, plain falls back to the latter.
+  uint16_t* h16 = nullptr;
+  const size_t h16_slot = (size_t)P * (size_t)k * 2;
+  if (!hilo) h16 = static_cast<uint16_t*>(host_stage(kSyrkSlots * h16_slot));
+  const size_t total = half_bytes * (hilo ? 2 : 1) + kSyrkSlots * ((h16 ? 0 : stA_bytes) + cb_bytes);
   char* ws = static_cast<char*>(pool_get(total, 1));
   if (!ws) {
     set_last_error("tb_ssyrk_host: cannot allocate %zu bytes of staging", total);
@@ -118,9 +158,10 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   // have come back, so a long download does not hold up the uploads behind it
   float* stA[kSyrkSlots];
   float* cb[kSyrkSlots];
+  const size_t stA_used = h16 ? 0 : stA_bytes;
   for (int q = 0; q < kSyrkSlots; ++q) {
-    stA[q] = reinterpret_cast<float*>(w2 + q * stA_bytes);
-    cb[q] = reinterpret_cast<float*>(w2 + kSyrkSlots * stA_bytes + q * cb_bytes);
+    stA[q] = reinterpret_cast<float*>(w2 + q * stA_used);
+    cb[q] = reinterpret_cast<float*>(w2 + kSyrkSlots * stA_used + q * cb_bytes);
   }
 
   // everything starts after the work already queued on the caller's stream
@@ -141,10 +182,20 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   for (long i = 0; i < npan; ++i) {
     const long r0 = i * P, r1 = std::min(n, r0 + P), pr = r1 - r0;
     const int s = (int)(i % kSyrkSlots);
-    // A rows [r0, r1) -> staging slot s (reused once panel i-3 was converted)
-    if (i >= kSyrkSlots) TB_CUDA_TRY(cudaStreamWaitEvent(p.h2d, p.ev[kEvConv + s], 0));
-    TB_CUDA_TRY(cudaMemcpy2DAsync(stA[s], P * 4, hA + r0, (size_t)lda * 4, (size_t)pr * 4, (size_t)k,
-                                  cudaMemcpyHostToDevice, p.h2d));
+    if (h16) {
+      // A rows [r0, r1) -> FP16 on the host into page-locked slot s (free
+      // once panel i-3's copy out of it has completed) -> the device copy
+      uint16_t* slot = h16 + (size_t)s * (h16_slot / 2);
+      if (i >= kSyrkSlots) TB_CUDA_TRY(cudaEventSynchronize(p.ev[kEvA + s]));
+      host_f32_to_f16(hA + r0, lda, pr, k, slot, P);
+      TB_CUDA_TRY(cudaMemcpy2DAsync(hi + r0, (size_t)ldh * 2, slot, (size_t)P * 2, (size_t)pr * 2, (size_t)k,
+                                    cudaMemcpyHostToDevice, p.h2d));
+    } else {
+      // A rows [r0, r1) -> staging slot s (reused once panel i-3 was converted)
+      if (i >= kSyrkSlots) TB_CUDA_TRY(cudaStreamWaitEvent(p.h2d, p.ev[kEvConv + s], 0));
+      TB_CUDA_TRY(cudaMemcpy2DAsync(stA[s], P * 4, hA + r0, (size_t)lda * 4, (size_t)pr * 4, (size_t)k,
+                                    cudaMemcpyHostToDevice, p.h2d));
+    }
     TB_CUDA_TRY(cudaEventRecord(p.ev[kEvA + s], p.h2d));
     // C rows [r0, r1): the diagonal block (its strict upper part must come
     // back unchanged), or all columns [0, r1) when beta != 0
@@ -153,10 +204,13 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
     TB_CUDA_TRY(cudaMemcpy2DAsync(cb[s] + c0 * P, P * 4, hC + r0 + (size_t)c0 * ldc, (size_t)ldc * 4, (size_t)pr * 4,
                                   (size_t)(r1 - c0), cudaMemcpyHostToDevice, p.h2d));
     TB_CUDA_TRY(cudaEventRecord(p.ev[kEvC + s], p.h2d));
-    // convert into the FP16 copy of A, then the panel's lower tiles
+    // convert into the FP16 copy of A (unless the host did), then the
+    // panel's lower tiles
     TB_CUDA_TRY(cudaStreamWaitEvent(cs, p.ev[kEvA + s], 0));
-    TB_TRY(convert_f32_f16(pr, k, stA[s], P, hi + r0, lo ? lo + r0 : nullptr, ldh, 2048.f, 0, cs));
-    TB_CUDA_TRY(cudaEventRecord(p.ev[kEvConv + s], cs));
+    if (!h16) {
+      TB_TRY(convert_f32_f16(pr, k, stA[s], P, hi + r0, lo ? lo + r0 : nullptr, ldh, 2048.f, 0, cs));
+      TB_CUDA_TRY(cudaEventRecord(p.ev[kEvConv + s], cs));
+    }
     TB_CUDA_TRY(cudaStreamWaitEvent(cs, p.ev[kEvC + s], 0));
     std::vector<int4> plan;
     for (int g = 0; g < (int)((r1 + bn - 1) / bn); g += 8)
@@ -262,6 +316,15 @@ tb_status trsm_host(bool right, long m, long n, const float* hA, long lda, float
     TB_CUDA_TRY(cudaEventRecord(p.ev[kEvOut + s], p.d2h));
   }
   return finish(cs, p);
+}
+
+void release_host_staging() {
+  std::lock_guard<std::mutex> lk(g_pipe_mu);
+  for (HostStage& h : g_stage) {
+    if (h.p) cudaFreeHost(h.p);
+    h.p = nullptr;
+    h.bytes = 0;
+  }
 }
 
 }  // namespace tb

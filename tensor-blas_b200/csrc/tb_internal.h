@@ -170,6 +170,11 @@ std::vector<int4> plan_upper(int n, int bn, int kb0, int kb1);
 const int4* upload_tiles(const std::vector<int4>& tiles, cudaStream_t stream);
 
 // ------------------------------------------------------------------ conversion
+// rows x cols column-major FP32 -> FP16 (bits) on the host's cores
+// (tb_host_convert.cpp); round to nearest even, as __float2half_rn.
+void host_f32_to_f16(const float* src, long lds, long rows, long cols, uint16_t* dst, long ldd);
+// Frees the host-memory forms' page-locked staging (tb_release_scratch).
+void release_host_staging();
 // fp32 (rows x cols, column-major, lds) -> fp16 hi [and lo] with the same
 // orientation (ldd). lo = fp16((x - hi) * lo_scale).
 //   tri == 0: whole matrix; tri == 1: zero the strict upper triangle;

@@ -268,6 +268,7 @@ tb_status tb_release_scratch(void) {
   if (e != cudaSuccess) return tb::cuda_status(e);
   tb::release_pool();
   tb::release_tile_cache();
+  tb::release_host_staging();
   return TB_SUCCESS;
 }
 
