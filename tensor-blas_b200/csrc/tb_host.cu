@@ -11,18 +11,19 @@
 // returns only the lower triangle it computes.
 //
 //  SYRK, C = alpha A A^T + beta C (lower): row panel i of A (rows [r0, r1),
-//   all k columns) reaches the device FP16 copy of A — in plain precision
-//   converted to FP16 on the host's cores first (tb_host_convert.cpp), so
-//   half the bytes cross PCIe; in split precision copied as FP32 and
-//   converted to hi/lo on the device — and row panel i of C (rows [r0, r1),
-//   columns [0, r1)) is computed from it and the panels before it and
-//   copied back while panel i+1 is on its way.
+//   all k columns) is copied as FP32 and converted on the device into the
+//   FP16 copy of A (optionally, in plain precision, converted to FP16 on the
+//   host's cores first, tb_host_convert.cpp, so half the bytes cross PCIe),
+//   and row panel i of C (rows [r0, r1), columns [0, r1)) is computed from
+//   it and the panels before it and copied back while panel i+1 is on its
+//   way.
 //  TRSM: A's lower triangle is copied once and prepared (FP16 copy, leaf
 //   inverses); B then flows through a ring of device panels (columns for the
 //   left side, rows for the right side: those are independent systems).
 //
 // Calls are synchronous: they return when the results are in host memory.
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -108,6 +109,22 @@ void* host_stage(size_t bytes) {
   return h.p;
 }
 
+// Which of SYRK's A panels the host converts (plain precision): every
+// n-th (TB_HOST_F16_EVERY in the environment, read once). Default 0, none:
+// on the B200 boxes measured, 16 host cores converted a 64 MB panel more
+// slowly than PCIe moved it as FP32 (SYRK n = k = 16384 from host memory:
+// 24.7-25.5 ms with the device converting, 28.8-29.1 ms with the host
+// converting every panel), so the option pays only on hosts with more
+// memory bandwidth per PCIe link.
+int host_convert_every() {
+  static const int v = [] {
+    const char* e = getenv("TB_HOST_F16_EVERY");
+    const int x = e ? atoi(e) : 0;
+    return x >= 0 ? x : 0;
+  }();
+  return v;
+}
+
 tb_status finish(cudaStream_t cs, HostPipes& p) {
   TB_TRY(join(cs, p.h2d, p.ev[kEvEndH2d]));
   TB_TRY(join(cs, p.d2h, p.ev[kEvEndD2h]));
@@ -144,8 +161,10 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   // FP32). Without the page-locked slots, plain falls back to the latter.
   uint16_t* h16 = nullptr;
   const size_t h16_slot = (size_t)P * (size_t)k * 2;
-  if (!hilo) h16 = static_cast<uint16_t*>(host_stage(kSyrkSlots * h16_slot));
-  const size_t total = half_bytes * (hilo ? 2 : 1) + kSyrkSlots * ((h16 ? 0 : stA_bytes) + cb_bytes);
+  const int every = host_convert_every();
+  if (!hilo && every > 0) h16 = static_cast<uint16_t*>(host_stage(kSyrkSlots * h16_slot));
+  const bool all_host = h16 && every == 1;
+  const size_t total = half_bytes * (hilo ? 2 : 1) + kSyrkSlots * ((all_host ? 0 : stA_bytes) + cb_bytes);
   char* ws = static_cast<char*>(pool_get(total, 1));
   if (!ws) {
     set_last_error("tb_ssyrk_host: cannot allocate %zu bytes of staging", total);
@@ -158,7 +177,7 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   // have come back, so a long download does not hold up the uploads behind it
   float* stA[kSyrkSlots];
   float* cb[kSyrkSlots];
-  const size_t stA_used = h16 ? 0 : stA_bytes;
+  const size_t stA_used = all_host ? 0 : stA_bytes;
   for (int q = 0; q < kSyrkSlots; ++q) {
     stA[q] = reinterpret_cast<float*>(w2 + q * stA_used);
     cb[q] = reinterpret_cast<float*>(w2 + kSyrkSlots * stA_used + q * cb_bytes);
@@ -182,7 +201,8 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
   for (long i = 0; i < npan; ++i) {
     const long r0 = i * P, r1 = std::min(n, r0 + P), pr = r1 - r0;
     const int s = (int)(i % kSyrkSlots);
-    if (h16) {
+    const bool on_host = h16 && i % every == 0;
+    if (on_host) {
       // A rows [r0, r1) -> FP16 on the host into page-locked slot s (free
       // once panel i-3's copy out of it has completed) -> the device copy
       uint16_t* slot = h16 + (size_t)s * (h16_slot / 2);
@@ -207,7 +227,7 @@ tb_status syrk_host(long n, long k, float alpha, const float* hA, long lda, floa
     // convert into the FP16 copy of A (unless the host did), then the
     // panel's lower tiles
     TB_CUDA_TRY(cudaStreamWaitEvent(cs, p.ev[kEvA + s], 0));
-    if (!h16) {
+    if (!on_host) {
       TB_TRY(convert_f32_f16(pr, k, stA[s], P, hi + r0, lo ? lo + r0 : nullptr, ldh, 2048.f, 0, cs));
       TB_CUDA_TRY(cudaEventRecord(p.ev[kEvConv + s], cs));
     }

@@ -1,7 +1,8 @@
-// FP32 -> FP16 conversion on the host cores, for the host-memory SYRK
-// (tb_host.cu): converting A's row panels before they cross PCIe halves the
-// bytes the plain SYRK moves host -> device, and the device then reads the
-// FP16 copy directly. The result is the IEEE-754 binary16 value nearest to
+// FP32 -> FP16 conversion on the host cores (tb_host_s2h, and the
+// host-memory SYRK's optional host-side conversion, TB_HOST_F16_EVERY):
+// converting A's row panels before they cross PCIe halves the bytes the
+// plain SYRK moves host -> device, and the device then reads the FP16 copy
+// directly. The result is the IEEE-754 binary16 value nearest to
 // each input, ties to even (the same as the device conversion kernels'
 // __float2half_rn for every finite input, and for infinities).
 //

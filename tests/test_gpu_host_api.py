@@ -55,3 +55,38 @@ def test_host_api_rejects_device_tensors(tblas):
     d = torch.zeros(4, 4, device="cuda")
     with pytest.raises(TypeError):
         tblas.ssyrk_host(d, d, 4, 4, 4, 4)
+
+
+HOST_CONVERT = r"""
+import hashlib, sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+import TensorBLAS as TB
+n, k, beta = int(sys.argv[2]), int(sys.argv[3]), float(sys.argv[4])
+g = np.random.Generator(np.random.PCG64(n + k))
+A = g.uniform(-1, 1, (k, n)).astype(np.float32)
+C0 = g.uniform(-1, 1, (n, n)).astype(np.float32)
+hA, hC = torch.from_numpy(A).pin_memory(), torch.from_numpy(C0).pin_memory()
+TB.ssyrk_host(hA, hC, n, k, n, n, 1.25, beta, 256, TB.PLAIN)
+dA, dC = torch.from_numpy(A).cuda(), torch.from_numpy(C0).cuda()
+TB.ssyrk(dA, dC, n, k, n, n, 1.25, beta, "N", 256, TB.PLAIN)
+TB.synchronize()
+print(int(np.array_equal(hC.numpy(), dC.cpu().numpy())))
+"""
+
+
+@pytest.mark.parametrize("every", ["1", "2"])
+@pytest.mark.parametrize("n,k,beta", [(3100, 700, 0.0), (2048, 1000, 0.5)])
+def test_ssyrk_host_with_host_side_conversion(every, n, k, beta):
+    """TB_HOST_F16_EVERY converts every (or every second) A panel to FP16 on
+    the host's cores before it crosses PCIe: the result must still equal the
+    device routine's bit for bit (read once per process: a subprocess)."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, TB_HOST_F16_EVERY=every)
+    r = subprocess.run([sys.executable, "-c", HOST_CONVERT, os.path.join(root, "tensor-blas_b200", "python"), str(n),
+                        str(k), str(beta)], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "1"
