@@ -57,3 +57,10 @@ def test_direct_store_epilogue_is_bit_identical(trans, n, k):
     """beta = 0 CTA-pair launches store from registers with a seventh operand
     stage (TB_GEMM_PAIR_DIRECT=0 keeps the staged TMA epilogue): same bits."""
     assert _digest("1", trans, n, k, 0, 0.0, TB_GEMM_PAIR_DIRECT="0") == _digest("1", trans, n, k, 0, 0.0)
+
+
+def test_pair_and_single_cta_engines_give_the_same_bits():
+    """Large plain launches on CTA pairs (256 x 256 tiles, the default) or on
+    single CTAs (128 x 256, TB_GEMM_PAIR=0): each element is the same
+    K-ordered FP32 accumulation of the same FP16 products."""
+    assert _digest("1", "N", 4096, 3000, 0, 0.5, TB_GEMM_PAIR="0") == _digest("1", "N", 4096, 3000, 0, 0.5)
