@@ -193,6 +193,15 @@ def measured_peaks():
         return 1590.0, 1400.0, "fallback"
 
 
+def measured_hbm():
+    """HBM copy bandwidth (GB/s) and its source."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError, TypeError):
+        return 6650.0, "fallback"
+
+
 def traffic_summary():
     """DRAM bytes per algorithmic flop of the GEMM kernels, from a committed
     small-case ncu summary (scaled here to a launch by its flops)."""
@@ -316,7 +325,8 @@ def run_mine(args, world, rank, local):
     ms_syrk = _median_ms(lambda: TB.ssyrk(A, C, n, n, n, n, 1.0, 0.0, "N", args.nb_syrk, TB.PLAIN), 5)
     # per-kernel rooflines: 5 plain steps (SYRK + TRSM) with every GEMM-engine
     # launch event-timed on its own stream (tb_profile_begin / end), split by
-    # kernel (tb_profile_kernel): launch durations, algorithmic flops, launches
+    # kernel (tb_profile_kernel): launch durations, algorithmic flops and
+    # DRAM bytes, launches
     TB.lib.tb_profile_begin()
     for _ in range(5):
         Bw.copy_(B0)
@@ -325,11 +335,14 @@ def run_mine(args, world, rank, local):
     ms, fl, cnt = TB.ctypes.c_double(), TB.ctypes.c_double(), TB.ctypes.c_long()
     TB.lib.tb_profile_end(TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
     prof = (ms.value / 5, fl.value / 5, cnt.value / 5)
-    kernels = {}
+    kernels, kernel_bytes = {}, {}
+    by = TB.ctypes.c_double()
     for kind in range(4):
-        TB.lib.tb_profile_kernel(kind, TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(cnt))
+        TB.lib.tb_profile_kernel(kind, TB.ctypes.byref(ms), TB.ctypes.byref(fl), TB.ctypes.byref(by),
+                                 TB.ctypes.byref(cnt))
         if cnt.value:
             kernels[kind] = (ms.value / 5, fl.value / 5, cnt.value / 5)
+            kernel_bytes[kind] = by.value / 5
 
     value = job_tflops(world, args.steps, flops_step, ms_plain)
     value_split = job_tflops(world, args.steps, flops_step, ms_split)
@@ -398,6 +411,15 @@ def run_mine(args, world, rank, local):
             "share_of_step_gemm_time": ms / sum(v[0] for v in kernels.values()),
             "traffic": t["bytes_per_flop"] * fl / cnt if ("bytes_per_flop" in t and cnt) else None,
             "traffic_note": t.get("note")}
+        if kind == 0 and ms > 0:
+            # the short launches move more bytes than their MMAs take time:
+            # their bound is HBM (algorithmic bytes: operands once, C read
+            # and written, FP16 side copies)
+            hbm, hbm_src = measured_hbm()
+            gbs = kernel_bytes[kind] / (ms * 1e-3) / 1e9
+            per_kernel[keys[kind]]["hbm"] = {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                                             "frac": gbs / hbm, "bytes_per_launch": kernel_bytes[kind] / cnt,
+                                             "peak_source": f"{hbm_src} hbm_gbs"}
     dominant = keys[max(kernels, key=lambda k: kernels[k][0])]
     roof = dict(per_kernel[dominant])
     roof.update({"peak_source": f"{peak_src} bf16_tflops (burst: each launch timed alone; sustained {sustained})",

@@ -89,9 +89,10 @@ TB_API tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_
 /* The launches of the last begin/end window by kernel: kind 0 the single-CTA
  * GEMM kernel, 1 the CTA-pair GEMM kernel, 2 the persistent TRSM kernel, 3
  * the Ozaki INT8 kernels. Device ms during which at least one launch of that
- * kernel ran (the union of their intervals), their algorithmic flops and
- * their number. */
-TB_API tb_status tb_profile_kernel(int kind, double* ms, double* flops, long* launches);
+ * kernel ran (the union of their intervals), their algorithmic flops, their
+ * algorithmic DRAM bytes (GEMM kernels: operands once, C read when beta != 0
+ * and written, FP16 side copies; 0 for the others) and their number. */
+TB_API tb_status tb_profile_kernel(int kind, double* ms, double* flops, double* bytes, long* launches);
 
 /*
  * GEMM: C = alpha * op(A) * op(B) + beta * C, op(A) m x k, op(B) k x n, all

@@ -127,7 +127,7 @@ bool make_half_out_map(CUtensorMap* map, __half* p, long long rows, long long co
 }
 
 template <class Cfg>
-tb_status launch_pair(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops) {
+tb_status launch_pair(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops, double bytes = 0) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -141,13 +141,13 @@ tb_status launch_pair(const GemmArgs& args, int num_tiles, cudaStream_t stream, 
   void* tok = prof_begin(stream, kProfPair);
   gemm_pair_kernel<Cfg><<<2 * pairs, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(args);
   TB_CUDA_TRY(cudaGetLastError());
-  prof_end(tok, stream, flops);
+  prof_end(tok, stream, flops, bytes);
   note_launch();
   return TB_SUCCESS;
 }
 
 template <class Cfg, bool GROUPED>
-tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops) {
+tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t stream, double flops, double bytes = 0) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -160,7 +160,7 @@ tb_status launch_variant(const GemmArgs& args, int num_tiles, cudaStream_t strea
   void* tok = prof_begin(stream, kProfGemm);
   gemm_kernel<Cfg, GROUPED><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(args);
   TB_CUDA_TRY(cudaGetLastError());
-  prof_end(tok, stream, flops);
+  prof_end(tok, stream, flops, bytes);
   note_launch();
   return TB_SUCCESS;
 }
@@ -257,50 +257,68 @@ tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
   return TB_SUCCESS;
 }
 
+// Algorithmic DRAM bytes of a launch (profiling only): the operands once
+// (hi and lo in split mode), C read when beta != 0 and written (half of the
+// rectangle for triangle launches), and the FP16 side copies.
+static double gemm_algorithmic_bytes(const GemmCall& c) {
+  const double elem = c.fp8 ? 1.0 : 2.0, nops = (c.split == Split::kHiLo && !c.fp8) ? 2.0 : 1.0;
+  const double K = (double)c.kblocks * kGemmBK;
+  const double ops = ((double)c.M + (double)c.N) * K * elem * nops;
+  const double cbytes = (double)c.M * c.N * 4.0 * (c.beta != 0.f ? 2.0 : 1.0) * (c.tri ? 0.5 : 1.0);
+  double side = 0;
+  if (c.out_hi) {
+    const double om = c.out_m >= 0 ? std::min<double>(c.out_m, c.M) : c.M;
+    const double on = c.out_n >= 0 ? std::min<double>(c.out_n, c.N) : c.N;
+    side = om * on * 2.0 * (c.out_lo ? 2.0 : 1.0);
+  }
+  return ops + cbytes + side;
+}
+
 tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   if (c.num_tiles <= 0) return TB_SUCCESS;
   GemmArgs a;
   TB_TRY(gemm_build_args(c, &a));
+  const double bytes = gemm_algorithmic_bytes(c);
   const bool split = c.split == Split::kHiLo;
   const bool amn = c.a_hi.mn_major, bmn = c.b_hi.mn_major;
   if (c.fp8) return launch_variant<GemmCfg<kGemmBNFp8, 1, false, false, false, true>, false>(a, c.num_tiles, stream,
-                                                                                            c.flops);
+                                                                                            c.flops, bytes);
   if (c.pair) {
     const int direct = pair_direct_mode();
     if (direct == 2 || (direct == 1 && c.beta == 0.f && !c.out_hi)) {
-      if (amn && bmn) return launch_pair<PairCfg<true, true, true>>(a, c.num_tiles, stream, c.flops);
-      if (amn && !bmn) return launch_pair<PairCfg<true, false, true>>(a, c.num_tiles, stream, c.flops);
-      if (!amn && !bmn) return launch_pair<PairCfg<false, false, true>>(a, c.num_tiles, stream, c.flops);
-      return launch_pair<PairCfg<false, true, true>>(a, c.num_tiles, stream, c.flops);
+      if (amn && bmn) return launch_pair<PairCfg<true, true, true>>(a, c.num_tiles, stream, c.flops, bytes);
+      if (amn && !bmn) return launch_pair<PairCfg<true, false, true>>(a, c.num_tiles, stream, c.flops, bytes);
+      if (!amn && !bmn) return launch_pair<PairCfg<false, false, true>>(a, c.num_tiles, stream, c.flops, bytes);
+      return launch_pair<PairCfg<false, true, true>>(a, c.num_tiles, stream, c.flops, bytes);
     }
-    if (amn && bmn) return launch_pair<PairCfg<true, true>>(a, c.num_tiles, stream, c.flops);
-    if (amn && !bmn) return launch_pair<PairCfg<true, false>>(a, c.num_tiles, stream, c.flops);
-    if (!amn && !bmn) return launch_pair<PairCfg<false, false>>(a, c.num_tiles, stream, c.flops);
-    return launch_pair<PairCfg<false, true>>(a, c.num_tiles, stream, c.flops);
+    if (amn && bmn) return launch_pair<PairCfg<true, true>>(a, c.num_tiles, stream, c.flops, bytes);
+    if (amn && !bmn) return launch_pair<PairCfg<true, false>>(a, c.num_tiles, stream, c.flops, bytes);
+    if (!amn && !bmn) return launch_pair<PairCfg<false, false>>(a, c.num_tiles, stream, c.flops, bytes);
+    return launch_pair<PairCfg<false, true>>(a, c.num_tiles, stream, c.flops, bytes);
   }
   if (c.kblocks > 0 && c.kblocks <= kGemmPfMaxKb) {
     if (!split) {
-      if (amn && bmn) return launch_variant<GemmCfg<128, 1, true, true, true>, false>(a, c.num_tiles, stream, c.flops);
-      if (amn && !bmn) return launch_variant<GemmCfg<128, 1, true, false, true>, false>(a, c.num_tiles, stream, c.flops);
+      if (amn && bmn) return launch_variant<GemmCfg<128, 1, true, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+      if (amn && !bmn) return launch_variant<GemmCfg<128, 1, true, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
       if (!amn && !bmn)
-        return launch_variant<GemmCfg<128, 1, false, false, true>, false>(a, c.num_tiles, stream, c.flops);
-      return launch_variant<GemmCfg<128, 1, false, true, true>, false>(a, c.num_tiles, stream, c.flops);
+        return launch_variant<GemmCfg<128, 1, false, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+      return launch_variant<GemmCfg<128, 1, false, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
     }
-    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true, true>, false>(a, c.num_tiles, stream, c.flops);
-    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false, true>, false>(a, c.num_tiles, stream, c.flops);
-    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false, true>, false>(a, c.num_tiles, stream, c.flops);
-    return launch_variant<GemmCfg<128, 3, false, true, true>, false>(a, c.num_tiles, stream, c.flops);
+    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    return launch_variant<GemmCfg<128, 3, false, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
   }
   if (!split) {
-    if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>, false>(a, c.num_tiles, stream, c.flops);
-    if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>, false>(a, c.num_tiles, stream, c.flops);
-    if (!amn && !bmn) return launch_variant<GemmCfg<256, 1, false, false>, false>(a, c.num_tiles, stream, c.flops);
-    return launch_variant<GemmCfg<256, 1, false, true>, false>(a, c.num_tiles, stream, c.flops);
+    if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (amn && !bmn) return launch_variant<GemmCfg<256, 1, true, false>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (!amn && !bmn) return launch_variant<GemmCfg<256, 1, false, false>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    return launch_variant<GemmCfg<256, 1, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
   } else {
-    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true>, false>(a, c.num_tiles, stream, c.flops);
-    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false>, false>(a, c.num_tiles, stream, c.flops);
-    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>, false>(a, c.num_tiles, stream, c.flops);
-    return launch_variant<GemmCfg<128, 3, false, true>, false>(a, c.num_tiles, stream, c.flops);
+    if (amn && bmn) return launch_variant<GemmCfg<128, 3, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    return launch_variant<GemmCfg<128, 3, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
   }
 }
 

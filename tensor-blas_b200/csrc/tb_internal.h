@@ -72,7 +72,7 @@ void note_launch(int n = 1);
 enum ProfKind { kProfGemm = 0, kProfPair = 1, kProfDag = 2, kProfOzaki = 3, kProfKinds = 4 };
 bool profiling();
 void* prof_begin(cudaStream_t st, ProfKind kind);
-void prof_end(void* token, cudaStream_t st, double flops);
+void prof_end(void* token, cudaStream_t st, double flops, double bytes = 0);
 
 inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 

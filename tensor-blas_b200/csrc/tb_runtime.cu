@@ -41,12 +41,12 @@ namespace {
 std::atomic<unsigned long long> g_launches{0};
 struct ProfRec {
   cudaEvent_t a, b;
-  double flops;
+  double flops, bytes;
   int kind;  // ProfKind
 };
 // Per kind, for the last tb_profile_end: the union of the launches'
 // intervals (ms), their flops and their number.
-double g_prof_kind_ms[kProfKinds], g_prof_kind_flops[kProfKinds];
+double g_prof_kind_ms[kProfKinds], g_prof_kind_flops[kProfKinds], g_prof_kind_bytes[kProfKinds];
 long g_prof_kind_n[kProfKinds];
 bool g_prof_on = false;
 std::vector<ProfRec> g_prof_live;     // recorded since tb_profile_begin
@@ -82,17 +82,19 @@ void* prof_begin(cudaStream_t st, ProfKind kind) {
   r.a = ev_get();
   r.b = ev_get();
   r.flops = 0;
+  r.bytes = 0;
   r.kind = (int)kind;
   cudaEventRecord(r.a, st);
   g_prof_live.push_back(r);
   return reinterpret_cast<void*>(g_prof_live.size());
 }
 
-void prof_end(void* token, cudaStream_t st, double flops) {
+void prof_end(void* token, cudaStream_t st, double flops, double bytes) {
   if (!token) return;
   ProfRec& r = g_prof_live[reinterpret_cast<size_t>(token) - 1];
   cudaEventRecord(r.b, st);
   r.flops = flops;
+  r.bytes = bytes;
 }
 
 void set_last_error(const char* fmt, ...) {
@@ -329,7 +331,7 @@ tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launche
   for (auto& r : tb::g_prof_live)
     if (cudaEventSynchronize(r.b) != cudaSuccess) st = TB_ERROR_CUDA;
   for (int k = 0; k < tb::kProfKinds; ++k) {
-    tb::g_prof_kind_ms[k] = tb::g_prof_kind_flops[k] = 0;
+    tb::g_prof_kind_ms[k] = tb::g_prof_kind_flops[k] = tb::g_prof_kind_bytes[k] = 0;
     tb::g_prof_kind_n[k] = 0;
   }
   std::vector<std::pair<double, double>> kind_iv[tb::kProfKinds];
@@ -341,6 +343,7 @@ tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launche
       fl += r.flops;
       ++cnt;
       tb::g_prof_kind_flops[r.kind] += r.flops;
+      tb::g_prof_kind_bytes[r.kind] += r.bytes;
       ++tb::g_prof_kind_n[r.kind];
     }
   }
@@ -357,13 +360,14 @@ tb_status tb_profile_end(double* gemm_ms, double* gemm_flops, long* gemm_launche
   return st;
 }
 
-tb_status tb_profile_kernel(int kind, double* ms, double* flops, long* launches) {
+tb_status tb_profile_kernel(int kind, double* ms, double* flops, double* bytes, long* launches) {
   if (kind < 0 || kind >= tb::kProfKinds) {
     tb::set_last_error("tb_profile_kernel: kind %d out of range", kind);
     return TB_ERROR_INVALID_VALUE;
   }
   if (ms) *ms = tb::g_prof_kind_ms[kind];
   if (flops) *flops = tb::g_prof_kind_flops[kind];
+  if (bytes) *bytes = tb::g_prof_kind_bytes[kind];
   if (launches) *launches = tb::g_prof_kind_n[kind];
   return TB_SUCCESS;
 }
