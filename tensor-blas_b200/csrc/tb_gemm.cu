@@ -181,6 +181,16 @@ int split_kchunk() {
   return k;
 }
 
+// CTA-pair epilogues load C one chunk ahead; TB_GEMM_C_AHEAD=0 in the
+// environment turns it off (read once).
+static bool c_ahead_enabled() {
+  static const int on = [] {
+    const char* e = getenv("TB_GEMM_C_AHEAD");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return on == 1;
+}
+
 // CTA-pair launches that store from registers get a seventh operand stage
 // (TB_GEMM_PAIR_DIRECT in the environment, read once: 0 none, 1 the beta = 0
 // launches without side copies, 2 all).
@@ -246,6 +256,7 @@ tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
   a.out_m = c.out_m >= 0 ? (c.out_m < c.M ? c.out_m : c.M) : c.M;
   a.out_n = c.out_n >= 0 ? (c.out_n < c.N ? c.out_n : c.N) : c.N;
   a.tma_out = 0;
+  a.c_ahead = c_ahead_enabled() ? 1 : 0;
   if (c.out_hi && a.tma_c && c.tri == 0 && make_half_out_map(&a.mapOut[0], c.out_hi, a.out_m, a.out_n, c.ld_out) &&
       (!c.out_lo || make_half_out_map(&a.mapOut[1], c.out_lo, a.out_m, a.out_n, c.ld_out)))
     a.tma_out = 1;

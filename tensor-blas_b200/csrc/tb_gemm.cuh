@@ -73,6 +73,7 @@ struct GemmArgs {
   float out_lo_scale;
   int out_m, out_n;  // side copies only for rows < out_m and columns < out_n
   int tma_out;       // 1: side copies through mapOut (requires tma_c and tri == 0)
+  int c_ahead;       // CTA-pair kernel: C chunks loaded one ahead where no side copies are staged
   int* err;
   // FP8: per-(128-row block, 128-deep K block) scales of the A and B
   // operands, row-block-major with scale_ld K blocks per row block.
@@ -385,6 +386,43 @@ __device__ __forceinline__ void epilogue_chunk_tma(const GemmArgs& args, float* 
   if (copies) store_fp16_copies(StoreK(args), r, gi, gj0);
   ++es.chunk;
   es.last_side = side_mode;
+}
+
+// Pipelined form of the TMA path for tiles that load C and stage no side
+// copies: the C chunk for chunk c + 1 is requested (into the other buffer)
+// before chunk c is combined, so a tile pays one load latency instead of one
+// per chunk. c_issue_load requests chunk (m0, gj0) into buffer es.chunk + ahead
+// once every earlier store has read its buffer; epilogue_chunk_loaded then
+// combines and stores the chunk whose load was requested. Same arithmetic as
+// epilogue_chunk_tma.
+__device__ __forceinline__ void c_issue_load(const GemmArgs& args, float* stage, uint64_t* cload,
+                                             const EpiState& es, int ahead, int m0, int gj0) {
+  const int b = (es.chunk + ahead) & 1;
+  bulk_wait_read<0>();  // the store that last used buffer b (and every earlier one) has read it
+  mbar_arrive_expect_tx(&cload[b], 128 * 32 * 4);
+  tma_load_2d(stage + b * (128 * 32), &args.mapC, &cload[b], m0, gj0);
+}
+
+__device__ __forceinline__ void epilogue_chunk_loaded(const GemmArgs& args, float* stage, uint64_t* cload,
+                                                      EpiState& es, const float* v, int m0, int gj0, int row,
+                                                      bool issuer, volatile int* abort_flag) {
+  const EpiK k(args);
+  const int b = es.chunk & 1;
+  float* S = stage + b * (128 * 32);
+  const long long gi = (long long)m0 + row;
+  float r[32];
+  mbar_wait(&cload[b], (es.lphase >> b) & 1u, abort_flag, args.err, kDevErrTimeoutEpilogue);
+  es.lphase ^= 1u << b;
+  combine32(k, S, row, v, gi, gj0, k.chunk_masked(m0, gj0), r);
+  fence_proxy_async_smem();
+  named_bar_sync(1, 128);
+  if (issuer) {
+    tma_store_2d(&args.mapC, S, m0, gj0);
+    bulk_commit();
+  }
+  if (!args.tma_out && args.out_hi && gi < args.out_m) store_fp16_copies(StoreK(args), r, gi, gj0);
+  ++es.chunk;
+  es.last_side = false;
 }
 
 // PF epilogue, one 128 x 32 chunk (columns gj0..gj0+31) staged in the next
@@ -1126,6 +1164,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const bool issuer = (warp == 2 && lane == 0);
+    const bool c_prefetch = args.c_ahead != 0;
     EpiState es{0, 0u, false};
     int it = 0;
     for (int t = static_first(args, pair); t >= 0; t = static_next(args, pair, npairs, t), ++it) {
@@ -1138,7 +1177,24 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       const StoreK sk(args);
       const int buf = it & 1;
       const uint32_t tph = (uint32_t)(it >> 1) & 1u;
-      if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) break;
+      // C loads one chunk ahead (the first before the accumulator wait) for
+      // tiles that read C and stage no side copies in shared memory
+      const long long nrem = ((long long)args.N - tile.y + 31) / 32;
+      const int nval = nrem < BN / 32 ? (int)nrem : BN / 32;
+      const bool ahead = !Cfg::DIRECT && c_prefetch && args.tma_c && !direct && m0 < args.M &&
+                         (args.beta != 0.0f || tile_masked) &&
+                         !(args.tma_out && m0 < args.out_m && tile.y < args.out_n);
+      const int b0 = es.chunk & 1;
+      const uint32_t ph0 = (es.lphase >> b0) & 1u;
+      if (ahead && issuer) c_issue_load(args, stage_c, cload, es, 0, m0, tile.y);
+      if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) {
+        if (ahead && issuer) {  // the chunk-0 load in flight lands before the CTA leaves (bounded)
+          const uint64_t t0 = globaltimer_ns();
+          while (!mbar_try_wait(&cload[b0], ph0))
+            if (globaltimer_ns() - t0 > 1000000000ull) break;
+        }
+        break;
+      }
       tc_fence_after();
       const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
 #pragma unroll 1
@@ -1150,7 +1206,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
         }
-        if (!Cfg::DIRECT && args.tma_c && !direct) {
+        if (ahead) {
+          if (c0 / 32 < nval) {
+            if (issuer && c0 / 32 + 1 < nval) c_issue_load(args, stage_c, cload, es, 1, m0, tile.y + c0 + 32);
+            epilogue_chunk_loaded(args, stage_c, cload, es, v, m0, tile.y + c0, row, issuer, abort_flag);
+          }
+        } else if (!Cfg::DIRECT && args.tma_c && !direct) {
           if (tile.y + c0 < args.N && m0 < args.M)
             epilogue_chunk_tma(args, stage_c, cload, es, v, m0, tile.y + c0, row, args.beta != 0.0f || tile_masked,
                                issuer, abort_flag);
