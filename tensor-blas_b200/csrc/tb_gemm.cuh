@@ -562,6 +562,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  // the set-up above touches no global memory and may overlap the previous
+  // launch's last tiles (programmatic dependent launch)
+  grid_dep_wait();
+  grid_dep_launch();
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
@@ -1057,6 +1061,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
   cluster_sync_all();  // the peer's barriers exist before any remote arrival
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  grid_dep_wait();  // as in gemm_kernel
+  grid_dep_launch();
   const uint32_t full_leader = mapa_shared(smem_u32(full), 0);
   const uint32_t tempty_leader = mapa_shared(smem_u32(tempty), 0);
 

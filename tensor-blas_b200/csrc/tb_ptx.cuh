@@ -43,6 +43,20 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   return t;
 }
 
+// ------------------------------------------- programmatic dependent launch
+// grid_dep_wait: returns once the grids this launch was made dependent on
+// (the previous kernel on the stream, for a launch with programmatic stream
+// serialization) have completed and their memory operations are visible;
+// it returns at once for an ordinary launch. Every thread calls it before
+// its first access to global memory.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// grid_dep_launch: the dependent launch after this one may be scheduled once
+// every CTA of this grid has issued it (or exited). Its CTAs take SMs as
+// this grid's CTAs exit and block in grid_dep_wait until this grid is done.
+__device__ __forceinline__ void grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---------------------------------------------------------------- mbarrier
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
