@@ -246,8 +246,9 @@ int gemm_bn(Split s, int kblocks) {
 
 tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
   const bool split = c.split == Split::kHiLo && !c.fp8;
-  // pair launches: each CTA loads 128 of the tile's 256 B rows
-  const int bn = c.fp8 ? kGemmBNFp8 : (c.pair ? 128 : gemm_bn(c.split, c.kblocks));
+  // pair launches: each CTA loads half of the tile's B rows (128 of 256;
+  // split: 64 of 128)
+  const int bn = c.fp8 ? kGemmBNFp8 : (c.pair ? (split ? 64 : 128) : gemm_bn(c.split, c.kblocks));
   GemmArgs& a = *out;
   memset(&a, 0, sizeof(a));
   if (c.fp8) {
@@ -330,6 +331,12 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
   const bool amn = c.a_hi.mn_major, bmn = c.b_hi.mn_major;
   if (c.fp8) return launch_variant<GemmCfg<kGemmBNFp8, 1, false, false, false, true>, false>(a, c.num_tiles, stream,
                                                                                             c.flops, bytes);
+  if (c.pair && split) {
+    if (amn && bmn) return launch_pair<PairCfg<true, true, false, 3>>(a, c.num_tiles, stream, c.flops, bytes);
+    if (amn && !bmn) return launch_pair<PairCfg<true, false, false, 3>>(a, c.num_tiles, stream, c.flops, bytes);
+    if (!amn && !bmn) return launch_pair<PairCfg<false, false, false, 3>>(a, c.num_tiles, stream, c.flops, bytes);
+    return launch_pair<PairCfg<false, true, false, 3>>(a, c.num_tiles, stream, c.flops, bytes);
+  }
   if (c.pair) {
     const int direct = pair_direct_mode();
     if (direct == 2 || (direct == 1 && c.beta == 0.f && !c.out_hi)) {
@@ -375,6 +382,23 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
 static thread_local int t_engine_override = -1;
 void set_engine_override(int engine) { t_engine_override = engine; }
 int engine_override() { return t_engine_override; }
+
+// Long split launches (hi/lo operands, three products) that write no FP16
+// side copies run on CTA pairs too (256 x 128 tiles); TB_GEMM_PAIR_SPLIT=0
+// in the environment keeps them on single-CTA 128 x 128 tiles (read once).
+// On a B200: split SYRK n = k = 16384 11.62-11.67 ms on pairs against
+// 12.22-12.37 ms, results bit-identical; the split TRSM's long updates
+// (which stage the next leaf's hi/lo copies) took 1 % longer on pairs and
+// stay on single CTAs. Per SM a 256 x 128 pair MMA runs as long as the
+// single-CTA 128 x 128 one, so the pair saves shared-memory and L2 traffic
+// only; a 256-column split tile would need 256 fold registers per thread.
+static bool pair_split_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("TB_GEMM_PAIR_SPLIT");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 
 bool pair_engine_enabled() {
   if (t_engine_override >= 0) return t_engine_override == 1;
@@ -441,7 +465,8 @@ static tb_status set_tiles(GemmCall& c, const std::vector<int4>& tiles, int work
 
 tb_status gemm_launch_plan(GemmCall& c, const std::vector<int4>& plan, cudaStream_t stream) {
   const bool pf = c.kblocks > 0 && c.kblocks <= kGemmPfMaxKb;
-  c.pair = !c.fp8 && c.split == Split::kPlain && !pf && c.M >= 512 && c.N >= 512 && pair_engine_enabled();
+  c.pair = !c.fp8 && (c.split == Split::kPlain || (pair_split_enabled() && !c.out_hi)) && !pf && c.M >= 512 &&
+           c.N >= 512 && pair_engine_enabled();
   if (!c.pair) {
     TB_TRY(set_tiles(c, plan, std::min<int>((int)plan.size(), sm_count()), stream));
     return gemm_launch(c, stream);

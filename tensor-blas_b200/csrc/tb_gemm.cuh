@@ -982,17 +982,32 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_kernel(const __grid_cons
 // SYRK) store each thread's row of a chunk straight from registers (a
 // warp's 32 rows of a column are one 128-byte line), which frees the
 // epilogue's staging buffers for a seventh operand stage.
-template <bool A_MN_, bool B_MN_, bool DIRECT_ = false>
+// NSPLIT = 3 (split precision): 256 x 128 pair tiles with hi/lo operands
+// (each CTA loads 128 rows of A hi and lo and 64 rows of B hi and lo per K
+// block) and two accumulators per TMEM buffer, hi*hi and hi*lo + lo*hi;
+// the MMA issuer runs a tile's K range in rounds of kchunk K-blocks, one
+// TMEM buffer per round, and the epilogue folds each round into FP32
+// registers (acc += corr_scale * corr + main), as the single-CTA split
+// kernel does. Per SM and 16-deep K step the three MMAs read 6 KB of shared
+// memory each, against 8 KB for the single-CTA 128 x 128 split tile, which
+// is bound by shared-memory bandwidth.
+template <bool A_MN_, bool B_MN_, bool DIRECT_ = false, int NSPLIT_ = 1>
 struct PairCfg {
-  static constexpr int BM = 128, BN = 256, BK = 64;  // BM: rows per CTA; BN: the pair tile's columns
+  static constexpr int NSPLIT = NSPLIT_;
+  static constexpr bool FOLD = NSPLIT > 1;
+  static constexpr int NOPS = FOLD ? 2 : 1;  // copies per operand (hi[, lo])
+  static constexpr int NACC = FOLD ? 2 : 1;  // accumulators per TMEM buffer
+  static constexpr int BM = 128, BN = FOLD ? 128 : 256, BK = 64;  // BM: rows per CTA; BN: the pair tile's columns
   static constexpr bool A_MN = A_MN_, B_MN = B_MN_;
   static constexpr bool DIRECT = DIRECT_;
+  static_assert(!(FOLD && DIRECT), "the split pair tile stages its epilogue");
   static constexpr int A_BYTES = BM * BK * 2;
   static constexpr int B_BYTES = (BN / 2) * BK * 2;
-  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int STAGES = DIRECT ? 7 : 6;
-  static constexpr int ACC_COLS = BN;
+  static constexpr int STAGE_BYTES = NOPS * (A_BYTES + B_BYTES);
+  static constexpr int STAGES = FOLD ? 4 : (DIRECT ? 7 : 6);
+  static constexpr int ACC_COLS = NACC * BN;
   static constexpr int TMEM_COLS = 2 * ACC_COLS;
+  static_assert(TMEM_COLS <= 512, "TMEM budget");
   static constexpr int EPI_BYTES = DIRECT ? 0 : 2 * 128 * 32 * 4;
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + 256;
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
@@ -1085,9 +1100,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
           uint8_t* st = smem + s * Cfg::STAGE_BYTES;
           const int k = args.k_off + kb * BK;
           const uint32_t bar = full_leader + 8u * (uint32_t)s;
-          load_operand_pair<Cfg::A_MN, 128>(st, &args.mapA[0], bar, args.a_off + tile.x + 128 * (int)rank, k);
-          load_operand_pair<Cfg::B_MN, 128>(st + Cfg::A_BYTES, &args.mapB[0], bar, args.b_off + tile.y + 128 * (int)rank,
-                                            k);
+#pragma unroll
+          for (int h = 0; h < Cfg::NOPS; ++h) {
+            load_operand_pair<Cfg::A_MN, 128>(st + h * Cfg::A_BYTES, &args.mapA[h], bar,
+                                              args.a_off + tile.x + 128 * (int)rank, k);
+            load_operand_pair<Cfg::B_MN, BN / 2>(st + Cfg::NOPS * Cfg::A_BYTES + h * Cfg::B_BYTES, &args.mapB[h], bar,
+                                                 args.b_off + tile.y + (BN / 2) * (int)rank, k);
+          }
           issued_mask |= 1u << s;
           phase_mask = (phase_mask & ~(1u << s)) | (ph << s);
           if (++s == STAGES) {
@@ -1121,36 +1140,47 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       uint32_t ph = 0;
       int it = 0;
       bool ok = true, any = false;
-      for (int t = static_first(args, pair); t >= 0 && ok; t = static_next(args, pair, npairs, t), ++it) {
+      // a tile's K range in rounds of kchunk K-blocks (split) or one round
+      const int kc = Cfg::FOLD ? args.kchunk : (1 << 30);
+      for (int t = static_first(args, pair); t >= 0 && ok; t = static_next(args, pair, npairs, t)) {
         const int4 tile = args.tiles[t];
-        const int buf = it & 1;
-        const uint32_t tph = (uint32_t)(it >> 1) & 1u;
-        if (!mbar_wait(&tempty[buf], tph ^ 1u, abort_flag, args.err, kDevErrTimeoutMma)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t d0 = tmem_base + (uint32_t)(buf * Cfg::ACC_COLS);
-        for (int kb = tile.z; kb < tile.w; ++kb) {
-          if (!mbar_wait(&full[s], ph, abort_flag, args.err, kDevErrTimeoutMma)) {
+        for (int c0 = tile.z; c0 < tile.w && ok; c0 += kc, ++it) {
+          const int c1 = (tile.w - c0 > kc) ? c0 + kc : tile.w;
+          const int buf = it & 1;
+          const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+          if (!mbar_wait(&tempty[buf], tph ^ 1u, abort_flag, args.err, kDevErrTimeoutMma)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t a = smem_u32(smem + s * Cfg::STAGE_BYTES), b = a + Cfg::A_BYTES;
+          const uint32_t d0 = tmem_base + (uint32_t)(buf * Cfg::ACC_COLS);
+          for (int kb = c0; kb < c1; ++kb) {
+            if (!mbar_wait(&full[s], ph, abort_flag, args.err, kDevErrTimeoutMma)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a = smem_u32(smem + s * Cfg::STAGE_BYTES), b = a + Cfg::NOPS * Cfg::A_BYTES;
 #pragma unroll
-          for (int kk = 0; kk < BK / 16; ++kk)
-            umma_f16_pair(d0, operand_desc<Cfg::A_MN>(a, kk), operand_desc<Cfg::B_MN>(b, kk), Cfg::IDESC,
-                          (kb > tile.z || kk > 0) ? 1u : 0u);
-          any = true;
-          tc_commit_pair(&empty[s], 3);
-          if (++s == STAGES) {
-            s = 0;
-            ph ^= 1u;
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint32_t acc = (kb > c0 || kk > 0) ? 1u : 0u;
+              const uint64_t da = operand_desc<Cfg::A_MN>(a, kk), db = operand_desc<Cfg::B_MN>(b, kk);
+              umma_f16_pair(d0, da, db, Cfg::IDESC, acc);
+              if constexpr (Cfg::FOLD) {
+                umma_f16_pair(d0 + BN, da, operand_desc<Cfg::B_MN>(b + Cfg::B_BYTES, kk), Cfg::IDESC, acc);
+                umma_f16_pair(d0 + BN, operand_desc<Cfg::A_MN>(a + Cfg::A_BYTES, kk), db, Cfg::IDESC, 1u);
+              }
+            }
+            any = true;
+            tc_commit_pair(&empty[s], 3);
+            if (++s == STAGES) {
+              s = 0;
+              ph ^= 1u;
+            }
           }
+          if (!ok) break;
+          tc_commit_pair(&tfull[buf], 3);
         }
-        if (!ok) break;
-        tc_commit_pair(&tfull[buf], 3);
       }
       if (!ok && any) {
         tc_commit_pair(drain, 1);
@@ -1173,7 +1203,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     const bool c_prefetch = args.c_ahead != 0;
     EpiState es{0, 0u, false};
     int it = 0;
-    for (int t = static_first(args, pair); t >= 0; t = static_next(args, pair, npairs, t), ++it) {
+    for (int t = static_first(args, pair); t >= 0; t = static_next(args, pair, npairs, t)) {
       const int4 tile = args.tiles[t];
       const int m0 = tile.x + 128 * (int)rank;
       const long long gi = (long long)m0 + row;
@@ -1181,8 +1211,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       const bool tile_masked = tile_reaches_mask(args, m0, tile.y, 128, BN);
       const bool direct = tile_masked && args.beta == 0.0f;  // as in the single-CTA kernel
       const StoreK sk(args);
-      const int buf = it & 1;
-      const uint32_t tph = (uint32_t)(it >> 1) & 1u;
       // C loads one chunk ahead (the first before the accumulator wait) for
       // tiles that read C and stage no side copies in shared memory
       const long long nrem = ((long long)args.N - tile.y + 31) / 32;
@@ -1192,26 +1220,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
                          !(args.tma_out && m0 < args.out_m && tile.y < args.out_n);
       const int b0 = es.chunk & 1;
       const uint32_t ph0 = (es.lphase >> b0) & 1u;
-      if (ahead && issuer) c_issue_load(args, stage_c, cload, es, 0, m0, tile.y);
-      if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) {
-        if (ahead && issuer) {  // the chunk-0 load in flight lands before the CTA leaves (bounded)
-          const uint64_t t0 = globaltimer_ns();
-          while (!mbar_try_wait(&cload[b0], ph0))
-            if (globaltimer_ns() - t0 > 1000000000ull) break;
-        }
-        break;
-      }
-      tc_fence_after();
-      const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
-#pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 32) {
-        float v[32];
-        tmem_ld32(tacc + c0, v);
-        if (c0 == BN - 32) {  // this CTA's half of the accumulator is read: tell the leader
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
-        }
+      // one 128 x 32 chunk of this CTA's output rows: alpha * v (+ beta * C)
+      auto store_chunk = [&](const float* v, int c0) {
         if (ahead) {
           if (c0 / 32 < nval) {
             if (issuer && c0 / 32 + 1 < nval) c_issue_load(args, stage_c, cload, es, 1, m0, tile.y + c0 + 32);
@@ -1223,6 +1233,68 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
                                issuer, abort_flag);
         } else if (row_ok) {
           epilogue_store32(sk, v, gi, (long long)tile.y + c0);
+        }
+      };
+      // the chunk-0 load in flight lands before the CTA leaves (bounded)
+      auto drain_ahead = [&]() {
+        if (ahead && issuer) {
+          const uint64_t t0 = globaltimer_ns();
+          while (!mbar_try_wait(&cload[b0], ph0))
+            if (globaltimer_ns() - t0 > 1000000000ull) break;
+        }
+      };
+      if (ahead && issuer) c_issue_load(args, stage_c, cload, es, 0, m0, tile.y);
+      if constexpr (Cfg::FOLD) {
+        float acc[BN];
+#pragma unroll
+        for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+        bool bad = false;
+        for (int c0k = tile.z; c0k < tile.w; c0k += args.kchunk, ++it) {
+          const int buf = it & 1;
+          const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+          if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) {
+            bad = true;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+#pragma unroll
+          for (int c0 = 0; c0 < BN; c0 += 32) {
+            float v[32], w[32];
+            tmem_ld32x2(tacc + c0, tacc + BN + c0, v, w);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc[c0 + j] += fmaf(args.corr_scale, w[j], v[j]);
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
+        }
+        if (bad) {
+          drain_ahead();
+          break;
+        }
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 32) store_chunk(acc + c0, c0);
+      } else {
+        const int buf = it & 1;
+        const uint32_t tph = (uint32_t)(it >> 1) & 1u;
+        ++it;
+        if (named_bar_any(1, 128, !mbar_wait(&tfull[buf], tph, abort_flag, args.err, kDevErrTimeoutEpilogue))) {
+          drain_ahead();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tacc = tmem_base + lane_addr + (uint32_t)(buf * Cfg::ACC_COLS);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+          float v[32];
+          tmem_ld32(tacc + c0, v);
+          if (c0 == BN - 32) {  // this CTA's half of the accumulator is read: tell the leader
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(tempty_leader + 8u * (uint32_t)buf);
+          }
+          store_chunk(v, c0);
         }
       }
     }
