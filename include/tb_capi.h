@@ -119,8 +119,10 @@ TB_API tb_status tb_ssyrk(char uplo, char trans, long n, long k, float alpha, co
 /*
  * nb = TB_NB_AUTO in tb_ssyrk, tb_strsm, tb_ssyr2k and tb_strmm: the
  * library's autotuner picks nb (the TRSM leaf size: 128, 256 or 512) and the
- * GEMM engine (256 x 256 tiles on CTA pairs, or single-CTA tiles) for this
- * (routine, flags, sizes, precision). The first call with a new key times
+ * GEMM engine, i.e. the tile shape and cluster size of the large plain
+ * launches (engine 1: 256 x 256 tiles on CTA pairs; 0: single-CTA 128 x 256
+ * tiles; 2: single-CTA 128 x 128 tiles, a candidate in plain precision only)
+ * for this (routine, flags, sizes, precision). The first call with a new key times
  * each candidate once on zero-filled scratch outputs of the same shape, on
  * the library's current stream, and caches the fastest per device; the call
  * then runs with it. The cache lives in memory and, when a file is set

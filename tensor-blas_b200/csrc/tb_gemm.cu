@@ -241,7 +241,8 @@ static int pair_direct_mode() {
 int gemm_bn(Split s) { return s == Split::kPlain ? 256 : 128; }
 int gemm_bn(Split s, int kblocks) {
   const bool pf = kblocks > 0 && kblocks <= kGemmPfMaxKb;
-  return (s == Split::kPlain && !pf) ? 256 : 128;
+  if (s != Split::kPlain || pf) return 128;
+  return engine_override() == kEngineNarrow ? 128 : 256;  // the narrow engine's plain tiles
 }
 
 tb_status gemm_build_args(const GemmCall& c, GemmArgs* out) {
@@ -362,6 +363,12 @@ tb_status gemm_launch(const GemmCall& c, cudaStream_t stream) {
     if (amn && !bmn) return launch_variant<GemmCfg<128, 3, true, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
     if (!amn && !bmn) return launch_variant<GemmCfg<128, 3, false, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
     return launch_variant<GemmCfg<128, 3, false, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+  }
+  if (!split && engine_override() == kEngineNarrow) {  // plans built with gemm_bn() = 128
+    if (amn && bmn) return launch_variant<GemmCfg<128, 1, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (amn && !bmn) return launch_variant<GemmCfg<128, 1, true, false>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    if (!amn && !bmn) return launch_variant<GemmCfg<128, 1, false, false>, false>(a, c.num_tiles, stream, c.flops, bytes);
+    return launch_variant<GemmCfg<128, 1, false, true>, false>(a, c.num_tiles, stream, c.flops, bytes);
   }
   if (!split) {
     if (amn && bmn) return launch_variant<GemmCfg<256, 1, true, true>, false>(a, c.num_tiles, stream, c.flops, bytes);

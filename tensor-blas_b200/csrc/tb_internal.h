@@ -140,7 +140,12 @@ int gemm_bn(Split s, int kblocks);
 
 tb_status gemm_launch(const GemmCall& call, cudaStream_t stream);
 // GEMM engine for the large plain launches of this thread: -1 the default
-// (CTA pairs unless TB_GEMM_PAIR=0), 0 single-CTA tiles, 1 CTA pairs.
+// (CTA pairs unless TB_GEMM_PAIR=0), 0 single-CTA 128 x 256 tiles, 1 CTA
+// pairs (256 x 256), 2 single-CTA 128 x 128 tiles (kEngineNarrow: twice the
+// tiles of engine 0, for launches whose 128 x 256 tiles leave SMs idle).
+// The override also sets the tile width that gemm_bn(split, kblocks) gives
+// the plans of plain long-K launches, so plan and kernel agree.
+constexpr int kEngineNarrow = 2;
 void set_engine_override(int engine);
 int engine_override();
 struct EngineScope {
@@ -327,7 +332,7 @@ tb_status gemm_fp8(bool ta, bool tb_, long m, long n, long k, float alpha, const
 // ------------------------------------------------------------------ autotuner (tb_tune.cu)
 struct TuneChoice {
   long nb;
-  int engine;  // 0 single-CTA tiles, 1 CTA pairs
+  int engine;  // 0 single-CTA 128 x 256 tiles, 1 CTA pairs, 2 single-CTA 128 x 128 tiles
   double ms;
   int splitk = 1;  // SYRK: K parts of a split-K launch (1: one pass)
 };

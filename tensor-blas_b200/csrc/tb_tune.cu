@@ -10,8 +10,12 @@
 // Keys start with the device name, compute capability and driver version,
 // so one file can serve several machines.
 //
-// Knobs: the GEMM engine (1: 256 x 256 tiles on CTA pairs for the large
-// plain launches, 0: single-CTA tiles); for TRSM the leaf size nb (128,
+// Knobs: the GEMM engine, i.e. the tile shape and cluster size of the large
+// plain launches (1: 256 x 256 tiles on CTA pairs, 0: single-CTA 128 x 256
+// tiles, 2: single-CTA 128 x 128 tiles, twice as many tiles as 0 for
+// problems whose wider tiles leave SMs idle; split launches use 128-wide
+// tiles either way, so 2 is a candidate for plain precision only); for TRSM
+// the leaf size nb (128,
 // 256, 512), which sets the recursion's leaf inverses and the number of
 // update launches (SYRK, SYR2K and TRMM do not use nb); and for plain 'N'
 // SYRKs whose triangle has fewer 128 x 256 tiles than the GPU has SMs (small
@@ -37,10 +41,25 @@ std::map<std::string, TuneChoice> g_cache;
 std::string g_file;
 bool g_file_init = false;
 
+// The key prefix of the current device, built once per device: the device
+// properties query takes milliseconds of host time, and every NB_AUTO call
+// builds a key.
 std::string device_tag() {
-  int dev = 0, drv = 0;
+  static std::mutex mu;
+  static std::map<int, std::string> tags;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return "nodevice";
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = tags.find(dev);
+    if (it != tags.end()) return it->second;
+  }
+  int drv = 0;
   cudaDeviceProp p;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
     cudaGetLastError();
     return "nodevice";
   }
@@ -49,6 +68,8 @@ std::string device_tag() {
   snprintf(buf, sizeof(buf), "%s/sm_%d%d/drv%d", p.name, p.major, p.minor, drv);
   for (char* c = buf; *c; ++c)
     if (*c == '"' || *c == '\\' || *c == '|') *c = '_';
+  std::lock_guard<std::mutex> lk(mu);
+  tags[dev] = buf;
   return buf;
 }
 
@@ -188,7 +209,7 @@ extern "C" int tb_autotune_entries(void) {
 
 extern "C" tb_status tb_autotune_put(const char* routine, const char* flags, long a, long b, int precision, long nb,
                                      int engine, double ms) {
-  if (!routine || !flags || nb <= 0 || (engine != 0 && engine != 1)) return TB_ERROR_INVALID_VALUE;
+  if (!routine || !flags || nb <= 0 || engine < 0 || engine > kEngineNarrow) return TB_ERROR_INVALID_VALUE;
   const std::string key = tune_key(routine, flags, a, b, precision);
   std::lock_guard<std::mutex> lk(g_mu);
   init_file_locked();
@@ -198,7 +219,7 @@ extern "C" tb_status tb_autotune_put(const char* routine, const char* flags, lon
 
 extern "C" tb_status tb_autotune_put_ex(const char* routine, const char* flags, long a, long b, int precision, long nb,
                                         int engine, int splitk, double ms) {
-  if (!routine || !flags || nb <= 0 || (engine != 0 && engine != 1) || splitk < 1 || splitk > 64)
+  if (!routine || !flags || nb <= 0 || engine < 0 || engine > kEngineNarrow || splitk < 1 || splitk > 64)
     return TB_ERROR_INVALID_VALUE;
   const std::string key = tune_key(routine, flags, a, b, precision);
   std::lock_guard<std::mutex> lk(g_mu);
@@ -260,7 +281,13 @@ struct TuneScratch {
   }
 };
 
-const std::vector<TuneChoice> kEngines = {{256, 1, 0}, {256, 0, 0}};
+// Engine candidates of a routine without nb: the pair and single-CTA
+// engines, and for plain precision the narrow single-CTA tiles.
+std::vector<TuneChoice> engines(int precision) {
+  std::vector<TuneChoice> c = {{256, 1, 0}, {256, 0, 0}};
+  if (precision == TB_PREC_PLAIN) c.push_back(TuneChoice{256, kEngineNarrow, 0});
+  return c;
+}
 
 }  // namespace
 
@@ -271,7 +298,7 @@ tb_status auto_ssyrk(char uplo, char trans, long n, long k, float alpha, const f
   const cudaStream_t st = current_stream();
   TuneScratch s((size_t)ldc * n * sizeof(float));
   const char flags[3] = {uplo, trans, 0};
-  std::vector<TuneChoice> cands = kEngines;
+  std::vector<TuneChoice> cands = engines(precision);
   const bool tr = trans == 'T' || trans == 't' || trans == 'C' || trans == 'c';
   const long kb = (k + kGemmBK - 1) / kGemmBK;
   if (precision == TB_PREC_PLAIN && !tr && n <= kSplitKMaxN && kb > kGemmPfMaxKb) {
@@ -305,7 +332,8 @@ tb_status auto_strsm(char side, long m, long n, const float* A, long lda, float*
   const char flags[2] = {side, 0};
   std::vector<TuneChoice> cands;
   for (long nb : {512L, 256L, 128L})
-    for (int e : {1, 0}) cands.push_back(TuneChoice{nb, e, 0});
+    for (int e : {1, 0, kEngineNarrow})
+      if (e != kEngineNarrow || precision == TB_PREC_PLAIN) cands.push_back(TuneChoice{nb, e, 0});
   TuneChoice ch;
   TB_TRY(autotune(tune_key("strsm", flags, m, n, precision), cands,
                   [&](const TuneChoice& c) {
@@ -326,7 +354,7 @@ tb_status auto_ssyr2k(char uplo, char trans, long n, long k, float alpha, const 
   TuneScratch s((size_t)ldc * n * sizeof(float));
   const char flags[3] = {uplo, trans, 0};
   TuneChoice ch;
-  TB_TRY(autotune(tune_key("ssyr2k", flags, n, k, precision), kEngines,
+  TB_TRY(autotune(tune_key("ssyr2k", flags, n, k, precision), engines(precision),
                   [&](const TuneChoice& c) {
                     float* Cs = nullptr;
                     TB_TRY(s.get(st, &Cs));
@@ -345,7 +373,7 @@ tb_status auto_strmm(char uplo, long m, long n, float alpha, const float* A, lon
   TuneScratch s((size_t)ldc * n * sizeof(float));
   const char flags[2] = {uplo, 0};
   TuneChoice ch;
-  TB_TRY(autotune(tune_key("strmm", flags, m, n, precision), kEngines,
+  TB_TRY(autotune(tune_key("strmm", flags, m, n, precision), engines(precision),
                   [&](const TuneChoice& c) {
                     float* Cs = nullptr;
                     TB_TRY(s.get(st, &Cs));

@@ -26,6 +26,7 @@ SPLIT = 1  # FP16 hi + scaled-lo, 3 products, FP32-level accuracy
 FP8 = 2    # e4m3 scaled per 128x128 block (SYRK/SYR2K/TRMM/SYMM/GEMM), ~1e-2 accuracy
 REFINE = 3  # TRSM: plain solve + one refinement sweep, FP32-level accuracy
 NB_AUTO = -1  # nb for ssyrk / strsm / ssyr2k / strmm: the library's autotuner picks nb and the GEMM engine
+# (engine 1: 256 x 256 tiles on CTA pairs, 0: single-CTA 128 x 256, 2: single-CTA 128 x 128, plain only)
 
 _c_long = ctypes.c_long
 _fp = ctypes.c_void_p

@@ -42,8 +42,20 @@ def test_put_get_file_roundtrip(cache):
 
 def test_put_rejects_bad_entries(cache):
     assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 0, 1, 1.0) == 1   # nb <= 0
-    assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 128, 2, 1.0) == 1  # engine not 0 / 1
+    assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 128, 3, 1.0) == 1  # engine not 0 / 1 / 2
+    assert TB.lib.tb_autotune_put(b"strsm", b"L", 8, 8, 0, 128, -1, 1.0) == 1
     assert TB.autotune_entries() == 0
+
+
+def test_narrow_engine_entries_roundtrip(cache):
+    """Engine 2 (single-CTA 128 x 128 tiles for the plain launches) is a
+    valid entry and survives the file round trip."""
+    TB._check(TB.lib.tb_autotune_put(b"ssyr2k", b"LN", 1024, 8192, TB.PLAIN, 256, 2, 0.08))
+    TB._check(TB.lib.tb_autotune_put_ex(b"strmm", b"U", 4096, 256, TB.PLAIN, 256, 2, 1, 0.05))
+    TB.lib.tb_autotune_clear()
+    TB.autotune_set_file(cache)  # reload
+    assert TB.autotune_get("ssyr2k", "LN", 1024, 8192, TB.PLAIN) == (256, 2)
+    assert TB.autotune_get_ex("strmm", "U", 4096, 256, TB.PLAIN) == (256, 2, 1)
 
 
 def test_splitk_entries_roundtrip_and_old_format(cache):

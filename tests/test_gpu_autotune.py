@@ -31,7 +31,7 @@ def test_ssyrk_auto(fresh):
         TB.synchronize()
         assert TB.autotune_entries() == 1
     choice = TB.autotune_get("ssyrk", "LN", n, k, TB.SPLIT)
-    assert choice is not None and choice[1] in (0, 1)
+    assert choice is not None and choice[1] in (0, 1)  # split precision: no narrow-engine candidate
     got = dC.cpu().numpy().reshape(n, n).T.astype(np.float64)
     exact = A.astype(np.float64) @ A.astype(np.float64).T
     low = np.tril(np.ones((n, n), dtype=bool))
@@ -118,3 +118,69 @@ def test_ssyrk_splitk_forced_entry(fresh, uplo, n, k, parts):
     err = np.linalg.norm((got - exact)[tri]) / np.linalg.norm(exact[tri])
     assert err <= 1e-6 + 1e-8 * k
     assert np.all(got[~tri] == 7.0)
+
+
+def _run_auto(routine, dA, dB, n1, n2):
+    """One NB_AUTO call of tb_ssyr2k ('L', 'N': n = n1, k = n2) or tb_strmm
+    ('U': m = n1, n = n2) in plain precision on fresh zero outputs."""
+    size = n1 * n1 if routine == "ssyr2k" else n1 * n2
+    dC = torch.zeros(size, device="cuda")
+    TB._bind_stream(dA)
+    if routine == "ssyr2k":
+        TB._check(TB.lib.tb_ssyr2k(b"L", b"N", n1, n2, 1.0, dA.data_ptr(), n1, dB.data_ptr(), n1, 0.0, dC.data_ptr(),
+                                   n1, TB.NB_AUTO, TB.PLAIN))
+    else:
+        TB._check(TB.lib.tb_strmm(b"U", n1, n2, 1.0, dA.data_ptr(), n1, dB.data_ptr(), n1, dC.data_ptr(), n1,
+                                  TB.NB_AUTO, TB.PLAIN))
+    TB.synchronize()
+    return dC
+
+
+@pytest.mark.parametrize("routine,n1,n2", [("ssyr2k", 1024, 8192), ("strmm", 4096, 256), ("ssyr2k", 1000, 3000)])
+def test_engines_give_the_same_bits_and_tuner_picks_one(fresh, routine, n1, n2):
+    """Plain long-K launches on CTA pairs (engine 1, 256 x 256), single-CTA
+    128 x 256 tiles (0) or single-CTA 128 x 128 tiles (2, the narrow engine,
+    twice the tiles of 0 where the wider tiles leave SMs idle): each element
+    is the same K-ordered FP32 sum of the same FP16 products, so a cached
+    entry naming any of them gives the same bits; the tuner's own choice is
+    one of the three and gives those bits too; the result matches FP64 of
+    the FP16-rounded operands."""
+    g = np.random.Generator(np.random.PCG64(59 + n1))
+    if routine == "ssyr2k":
+        n, k = n1, n2
+        A = g.uniform(-1, 1, (n, k)).astype(np.float32)
+        B = g.uniform(-1, 1, (n, k)).astype(np.float32)
+        flags = "LN"
+    else:
+        m, n = n1, n2
+        A = np.triu(g.uniform(-1, 1, (m, m))).astype(np.float32)
+        B = g.uniform(-1, 1, (m, n)).astype(np.float32)
+        flags = "U"
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()
+    outs = {}
+    for e in (0, 1, 2):
+        TB.lib.tb_autotune_clear()
+        TB._check(TB.lib.tb_autotune_put(routine.encode(), flags.encode(), n1, n2, TB.PLAIN, 256, e, 0.0))
+        outs[e] = _run_auto(routine, dA, dB, n1, n2)
+    assert torch.equal(outs[0], outs[2]) and torch.equal(outs[1], outs[2])
+    TB.lib.tb_autotune_clear()
+    tuned = _run_auto(routine, dA, dB, n1, n2)
+    nb, engine = TB.autotune_get(routine, flags, n1, n2, TB.PLAIN)
+    assert engine in (0, 1, 2)
+    assert torch.equal(tuned, outs[2])
+    Ah = A.astype(np.float16).astype(np.float64)
+    Bh = B.astype(np.float16).astype(np.float64)
+    if routine == "ssyr2k":
+        got = tuned.cpu().numpy().reshape(n1, n1).T.astype(np.float64)
+        exact = Ah @ Bh.T + Bh @ Ah.T
+        sel = np.tril(np.ones((n1, n1), dtype=bool))
+        K = 2 * n2
+    else:
+        got = tuned.cpu().numpy().reshape(n2, n1).T.astype(np.float64)
+        exact = Ah @ Bh
+        sel = np.ones_like(exact, dtype=bool)
+        K = n1
+    err = np.linalg.norm((got - exact)[sel]) / np.linalg.norm(exact[sel])
+    assert err <= 1e-6 + 1e-8 * K
+
