@@ -1,8 +1,8 @@
 """CPU oracle for the TensorBLAS hot path — TEST INFRASTRUCTURE ONLY.
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg (and the
-reference arm of bench.py) may import this module, and only as the checker or
-the timed CPU baseline; the library never calls it.
+reference arm of bench.py) may import this module, and only to check results
+or as the timed CPU baseline; the library never calls it.
 
 It restates, in NumPy, the arithmetic model of the reference's tc_* routines
 (Orgline/Tensor-BLAS; paths relative to that project):
