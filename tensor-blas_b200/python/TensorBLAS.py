@@ -120,12 +120,35 @@ def _dev_f32(t, name):
         raise TypeError(f"{name} must be a float32 CUDA tensor")
 
 
+def _shape(t, name, rows=None, cols=None):
+    """A logical matrix argument: 2-D, of the given shape where one is
+    required (None: any). A wrong shape would make the kernels read or write
+    outside the tensor, so it is an error here, before any device work; the
+    callers check every shape first and then every device and dtype
+    (`_devs`)."""
+    if t.dim() != 2:
+        raise ValueError(f"{name} must be a 2-D matrix, got shape {tuple(t.shape)}")
+    if (rows is not None and t.shape[0] != rows) or (cols is not None and t.shape[1] != cols):
+        want = f"{'*' if rows is None else rows} x {'*' if cols is None else cols}"
+        raise ValueError(f"{name} must be {want}, got {t.shape[0]} x {t.shape[1]}")
+
+
+def _devs(**tensors):
+    """Every given tensor (None: an omitted optional argument) is float32 on
+    a CUDA device."""
+    for name, t in tensors.items():
+        if t is not None:
+            _dev_f32(t, name)
+
+
 # ---------------------------------------------------------------- reference API
 def tc_syrk(A, transpose=False, nb=256):
     """C = A @ A.T (full symmetric n x n) for a row-major torch A (n x k).
 
     With transpose=True computes A.T @ A, as python/TensorBLAS.py:11-34.
     """
+    _shape(A, "A")
+    _devs(A=A)
     if transpose:
         A = torch.clone(A.T).contiguous()
     n = A.size(0)
@@ -139,7 +162,11 @@ def tc_syrk(A, transpose=False, nb=256):
 
 def tc_trsm(A, B, nb=256):
     """X with X @ A.T = B for lower-triangular A, as python/TensorBLAS.py:43-68."""
+    _shape(A, "A")
     n = A.size(0)
+    _shape(A, "A", n, n)
+    _shape(B, "B", None, n)
+    _devs(A=A, B=B)
     m = B.size(0)
     A = torch.clone(A.T).contiguous()
     B_inout = torch.clone(B.T).contiguous()
@@ -155,18 +182,25 @@ def tc_trsm(A, B, nb=256):
 # T.T. Helpers below take the logical matrix and handle that.
 def sgemm(transa, transb, m, n, k, alpha, A_cm, lda, B_cm, ldb, beta, C_cm, ldc, precision=PLAIN):
     """Raw column-major SGEMM on device buffers (tensor-core products at `precision`)."""
+    _dev_f32(A_cm, "A")
+    _dev_f32(B_cm, "B")
+    _dev_f32(C_cm, "C")
     _check(lib.tb_sgemm(transa.encode(), transb.encode(), m, n, k, alpha, A_cm.data_ptr(), lda, B_cm.data_ptr(), ldb,
                         beta, C_cm.data_ptr(), ldc, precision))
 
 
 def ssyrk(A_cm, C_cm, n, k, lda, ldc, alpha=1.0, beta=0.0, trans="N", nb=256, precision=PLAIN):
     """Raw column-major SSYRK on device buffers (lower triangle)."""
+    _dev_f32(A_cm, "A")
+    _dev_f32(C_cm, "C")
     _check(lib.tb_ssyrk(b"L", trans.encode(), n, k, alpha, A_cm.data_ptr(), lda, beta, C_cm.data_ptr(), ldc, nb,
                         precision))
 
 
 def strsm(side, A_cm, B_cm, m, n, lda, ldb, nb=512, precision=PLAIN):
     """Raw column-major STRSM (lower, non-unit); side 'R': X A^T = B, 'L': A X = B."""
+    _dev_f32(A_cm, "A")
+    _dev_f32(B_cm, "B")
     _check(lib.tb_strsm(side.encode(), m, n, A_cm.data_ptr(), lda, B_cm.data_ptr(), ldb, nb, precision))
 
 
@@ -225,8 +259,11 @@ def syrk(A, alpha=1.0, beta=0.0, C=None, nb=256, precision=PLAIN):
 
     Returns an n x n tensor whose strict upper triangle is C's (or zero).
     """
-    _dev_f32(A, "A")
+    _shape(A, "A")
     n, k = A.shape
+    if C is not None:
+        _shape(C, "C", n, n)
+    _devs(A=A, C=C)
     Acm = A.t().contiguous()  # storage = column-major n x k
     if C is None:
         Ccm = torch.zeros(n, n, device=A.device, dtype=torch.float32)
@@ -239,9 +276,11 @@ def syrk(A, alpha=1.0, beta=0.0, C=None, nb=256, precision=PLAIN):
 
 def trsm(A, B, side="L", nb=512, precision=PLAIN):
     """Solve A X = B (side 'L') or X A^T = B (side 'R') for lower-triangular A."""
-    _dev_f32(A, "A")
-    _dev_f32(B, "B")
+    _shape(B, "B")
     m, n = B.shape
+    nt = n if side in ("R", "r") else m
+    _shape(A, "A", nt, nt)
+    _devs(A=A, B=B)
     Acm = A.t().contiguous()
     Bcm = B.t().contiguous()
     _bind_stream(B)
@@ -251,9 +290,12 @@ def trsm(A, B, side="L", nb=512, precision=PLAIN):
 
 def syr2k(A, B, alpha=1.0, beta=0.0, C=None, nb=256, precision=PLAIN):
     """Lower triangle of alpha (A B^T + B A^T) + beta C (logical n x k torch matrices)."""
-    _dev_f32(A, "A")
-    _dev_f32(B, "B")
+    _shape(A, "A")
     n, k = A.shape
+    _shape(B, "B", n, k)
+    if C is not None:
+        _shape(C, "C", n, n)
+    _devs(A=A, B=B, C=C)
     Acm, Bcm = A.t().contiguous(), B.t().contiguous()
     Ccm = torch.zeros(n, n, device=A.device, dtype=torch.float32) if C is None else C.t().contiguous()
     _bind_stream(A)
@@ -264,9 +306,10 @@ def syr2k(A, B, alpha=1.0, beta=0.0, C=None, nb=256, precision=PLAIN):
 
 def trmm(A, B, alpha=1.0, uplo="L", nb=256, precision=PLAIN):
     """alpha op(A) B for triangular A ('L' lower / 'U' upper), left side, out of place."""
-    _dev_f32(A, "A")
-    _dev_f32(B, "B")
+    _shape(B, "B")
     m, n = B.shape
+    _shape(A, "A", m, m)
+    _devs(A=A, B=B)
     Acm, Bcm = A.t().contiguous(), B.t().contiguous()
     Ccm = torch.empty(n, m, device=B.device, dtype=torch.float32)
     _bind_stream(B)
@@ -277,9 +320,12 @@ def trmm(A, B, alpha=1.0, uplo="L", nb=256, precision=PLAIN):
 
 def symm(A, B, alpha=1.0, beta=0.0, C=None, uplo="L", precision=PLAIN):
     """alpha A B + beta C for symmetric A stored in triangle `uplo` (left side)."""
-    _dev_f32(A, "A")
-    _dev_f32(B, "B")
+    _shape(B, "B")
     m, n = B.shape
+    _shape(A, "A", m, m)
+    if C is not None:
+        _shape(C, "C", m, n)
+    _devs(A=A, B=B, C=C)
     Acm, Bcm = A.t().contiguous(), B.t().contiguous()
     Ccm = torch.zeros(n, m, device=B.device, dtype=torch.float32) if C is None else C.t().contiguous()
     _bind_stream(B)
