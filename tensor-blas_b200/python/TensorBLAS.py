@@ -374,6 +374,16 @@ class Batch:
 
     def __init__(self, kinds, A, BC, nb=0, precision=SPLIT):
         count = len(kinds)
+        if len(A) != count or len(BC) != count:
+            raise ValueError("kinds, A and BC need one entry per instance")
+        for i, (kind, a, bc) in enumerate(zip(kinds, A, BC)):
+            if kind not in (SYRK_KIND, TRSM_KIND):
+                raise ValueError(f"kinds[{i}] must be SYRK_KIND or TRSM_KIND")
+            side = int(round(a.numel() ** 0.5))
+            if side * side != a.numel() or bc.numel() != a.numel():
+                raise ValueError(f"A[{i}] and BC[{i}] must both hold one n x n matrix")
+        for i, (a, bc) in enumerate(zip(A, BC)):
+            _devs(**{f"A[{i}]": a, f"BC[{i}]": bc})
         self._keep = (list(A), list(BC))
         n = [int(round(a.numel() ** 0.5)) for a in A]
         k_arr = (ctypes.c_int * count)(*kinds)

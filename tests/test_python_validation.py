@@ -30,6 +30,10 @@ def cpu(*shape, dtype=torch.float32):
     lambda: TB.tc_syrk(cpu(2, 3, 4)),                           # A not 2-D
     lambda: TB.tc_trsm(cpu(6, 5), cpu(4, 6)),                   # A not square
     lambda: TB.tc_trsm(cpu(6, 6), cpu(4, 5)),                   # B not m x n
+    lambda: TB.Batch([0, 1], [cpu(4, 4), cpu(5, 5)], [cpu(4, 4)]),          # one BC missing
+    lambda: TB.Batch([0, 2], [cpu(4, 4), cpu(5, 5)], [cpu(4, 4), cpu(5, 5)]),  # unknown kind
+    lambda: TB.Batch([0], [cpu(4, 5)], [cpu(4, 5)]),                         # not square
+    lambda: TB.Batch([1], [cpu(4, 4)], [cpu(5, 5)]),                         # BC of another size
 ])
 def test_wrong_shapes_are_rejected(call):
     with pytest.raises(ValueError):
@@ -49,6 +53,7 @@ def test_wrong_shapes_are_rejected(call):
     lambda: TB.ssyrk(cpu(32), cpu(64), 8, 4, 8, 8),
     lambda: TB.strsm("L", cpu(64), cpu(24), 8, 3, 8, 8),
     lambda: TB.sgemm("N", "N", 8, 8, 8, 1.0, cpu(64), 8, cpu(64), 8, 0.0, cpu(64), 8),
+    lambda: TB.Batch([0, 1], [cpu(4, 4), cpu(25)], [cpu(4, 4), cpu(5, 5)]),
 ])
 def test_host_tensors_are_rejected_before_device_work(call):
     with pytest.raises(TypeError, match="CUDA"):
