@@ -172,7 +172,8 @@ def workload(n, nb_syrk, nb_trsm):
     """The config both arms report: the same matrices, shapes and flops."""
     return {"workload": f"plain SYRK n=k={n} nb={nb_syrk} + plain TRSM m=n={n} nb={nb_trsm} (lower, non-unit, "
                         f"{n} right-hand sides) per step", "n": n, "precision": "plain",
-            "l2": "inputs larger than L2 (1 GiB per matrix)", "parallelism": "replicas x1"}
+            "l2": "inputs larger than L2 (1 GiB per matrix)",
+            "parallelism": "replicas: one process per GPU, each running this step (n_gpus gives the count)"}
 
 
 def sample_indices(n):
@@ -435,7 +436,7 @@ def run_mine(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_plain / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f16 operands, f32 accumulate", "data": "synthetic (seeded)",
-        "config": dict(workload(n, args.nb_syrk, args.nb_trsm), parallelism=f"replicas x{world}"),
+        "config": workload(n, args.nb_syrk, args.nb_trsm),
         "detail": {"syrk_ms": ms_syrk, "trsm_ms": trsm_only["plain"]["ms"],
                    "timing": "median per call, CUDA events, device-resident", "trsm_side": "left (A X = B)"},
         "errors_vs_fp64": err_plain,
