@@ -136,6 +136,8 @@ TB_API tb_status tb_autotune_clear(void);                /* forget every entry (
 TB_API int tb_autotune_entries(void);
 /* routine: "ssyrk" (flags uplo+trans, a = n, b = k), "strsm" (flags side,
  * a = m, b = n), "ssyr2k" (uplo+trans, n, k), "strmm" (uplo, m, n).
+ * engine: 0, 1 or 2 as above (others: TB_ERROR_INVALID_VALUE); an entry put
+ * here drives later TB_NB_AUTO calls of that key.
  * tb_autotune_get returns TB_ERROR_NOT_SUPPORTED when there is no entry. */
 TB_API tb_status tb_autotune_put(const char* routine, const char* flags, long a, long b, int precision, long nb,
                                  int engine, double ms);
